@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""bench.py - element-steps/s of DynELA's explicit hot path on B200.
+
+Workload: 3-D Taylor impact of a copper bar (R 3.2 mm, L 32.4 mm) meshed as an
+O-grid cylinder of 960 x 160 = 153,600 ElHex8N3D elements (158,585 nodes,
+1,228,800 Gauss points), 227 m/s onto a rigid wall, Courant time step every 10
+increments.  A step is one explicit increment of the whole mesh (element pass,
+nodal gather + Chung-Hulbert update, time-step pass), run from t = 0 (the
+impact phase, where the radial return works hardest).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+    python bench.py --impl reference ...   # the DynELA reference on the host cores
+
+Several GPUs (torchrun, one process per GPU): every rank runs its own replica
+of the mesh (a single mesh does not shard without a halo exchange), value is
+the sum over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dynela-v.-4.0_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "elem-steps/s (3-D copper Taylor impact, 153,600 ElHex8N3D)"
+UNIT = "elem-steps/s"
+WORKLOAD = "taylor3d-copper-ogrid-153600-hex8"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--axial", type=int, default=160,
+                   help="axial element layers (160 = the measured workload; fewer for profiling captures)")
+    return p.parse_args()
+
+
+AXIAL = 160
+
+
+def workload(precision):
+    from dnlPython import _abi, meshes
+    prec = _abi.PREC_MIXED if precision == "mixed" else _abi.PREC_FP64
+    return meshes.taylor_3d(n_axial=AXIAL, length=32.4 * AXIAL / 160, precision=prec)
+
+
+# ----------------------------------------------------------------- roofline
+
+def alg_bytes(desc, word):
+    """Algorithmic bytes of one increment, counted once per persistent array:
+    per Gauss point 28 state words read+written + detJ0 read (57 word accesses),
+    per element 8 int32 of connectivity, per node x, disp, du (FP64, read+write),
+    v, a (FP64, read+write) and the mass (FP64, read).  Transients (F, R, J,
+    dN/dx, strain increment, element force slots) count 0.  Returns
+    (element kernel bytes, whole increment bytes)."""
+    nE, nN = desc.n_elems, desc.n_nodes
+    ip = nE * 8 * 57 * word
+    conn = nE * 8 * 4
+    elem = ip + conn + nN * (3 * 8 + 3 * 8)        # element pass reads x and du once per node
+    step = ip + conn + nN * (3 * 3 * 8 * 2 + 2 * 3 * 8 * 2 + 8)
+    return elem, step
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram read+write bytes per element-kernel launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "element_kernel_taylor3d.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch_mixed:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="clk_", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# -------------------------------------------------------------- CPU baseline
+
+def reference_rate(desc, steps, warmup, threads):
+    """The DynELA reference (oracle/_ref) on the host cores: elem-steps/s of
+    `steps` increments after `warmup` ones, from its own solver-loop clock.
+    Returns (value, kind, cores, sample) or None when it is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available():
+        return None
+    r = ref.RefModel(desc.copy(precision=0), threads=threads)
+    try:
+        r.init()
+        if warmup:
+            r.run(max_incs=warmup)
+        s0 = r.solver_seconds()
+        n = r.run(max_incs=steps)
+        sec = r.solver_seconds() - s0
+    finally:
+        r.close()
+    return desc.n_elems * n / sec, "reference", threads, \
+        f"{n} increments of the full {desc.n_elems}-element mesh from t=0 after {warmup} warm-up increments, " \
+        f"FP64, OpenMP {threads} threads (model build and start of the solve excluded)"
+
+
+def port_rate(desc, steps):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    o = oracle.OracleModel(desc.copy(precision=0))
+    o.init()
+    t0 = time.perf_counter()
+    n = o.run(max_incs=steps)
+    sec = time.perf_counter() - t0
+    o.close()
+    return desc.n_elems * n / sec, "port", 1, f"{n} increments of the full mesh on the C restatement, 1 thread"
+
+
+def cpu_baseline(desc):
+    threads = os.cpu_count() or 1
+    got = reference_rate(desc, steps=3, warmup=0, threads=threads)
+    if got is None:
+        got = port_rate(desc, steps=1)
+    v, kind, cores, sample = got
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+
+# ------------------------------------------------------------------ arms
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    desc = workload("fp64")
+    threads = os.cpu_count() or 1
+    steps, warmup = max(1, min(args.steps, 10)), min(args.warmup, 2)
+    got = reference_rate(desc, steps=steps, warmup=warmup, threads=threads)
+    if got is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libdnlref.so is not built"}))
+        return
+    v, kind, cores, sample = got
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": warmup, "ms_per_step": desc.n_elems / v * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": desc.n_elems, "nodes": desc.n_nodes, "precision": "fp64",
+                   "parallelism": f"openmp{cores}"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_engine_arm(args, rank, world, dist):
+    import numpy as np
+    from dnlPython import _abi
+    from dnlPython.engine import Engine
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    desc = workload(args.precision)
+    word = 4 if args.precision == "mixed" else 8
+    eng = Engine(desc).init()
+    if args.warmup:
+        eng.run(max_incs=args.warmup)
+
+    # ---- timed region: K increments, device time on the engine stream
+    barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0)
+    sampler.start()
+    done = eng.run(max_incs=args.steps)
+    run_ms = eng.timings()["run_ms"]
+    launches = eng.launch_count()
+    clocks = sampler.stop()
+    barrier()
+    assert done == args.steps, f"ran {done} of {args.steps} increments"
+    ms = max_over_ranks(run_ms)
+    value = world * desc.n_elems * args.steps / (ms / 1e3)
+    ctl = eng.control()
+
+    # ---- roofline of the element kernel (per-kernel CUDA events on the engine stream)
+    eng.set_timing(True)
+    kt = min(args.steps, 200)
+    eng.run(max_incs=kt)
+    tim = eng.timings()
+    eng.set_timing(False)
+    elem_ms = tim["element_ms"] / kt
+    eb, sb = alg_bytes(desc, word)
+    peak, peak_kind = measured_peak()
+    achieved = eb / (elem_ms / 1e3) / 1e9
+    traffic = profiled_traffic() if args.precision == "mixed" else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_element", "peak_source": peak_kind,
+                "alg_bytes_per_launch": eb, "ms_per_launch": elem_ms}
+    step_roofline = {"achieved": sb / (ms / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": sb / (ms / args.steps / 1e3) / 1e9 / peak, "alg_bytes_per_step": sb,
+                     "phase_ms_per_step": {"element": elem_ms, "nodal": tim["nodal_ms"] / kt,
+                                           "timestep_and_control": tim["timestep_ms"] / kt}}
+    eng.close()
+
+    # ---- the FP64 path on the same workload (the mixed/FP64 ratio of the metric)
+    fp64 = None
+    if args.precision == "mixed" and not args.no_fp64:
+        d64 = workload("fp64")
+        e64 = Engine(d64).init()
+        if args.warmup:
+            e64.run(max_incs=args.warmup)
+        k64 = min(args.steps, 500)
+        e64.run(max_incs=k64)
+        ms64 = e64.timings()["run_ms"]
+        e64.close()
+        fp64 = {"value": d64.n_elems * k64 / (ms64 / 1e3), "steps": k64, "ms_per_step": ms64 / k64}
+
+    # ---- end to end through the public API, host buffers in and out
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        e = Engine(desc)
+        e.init()
+        e.run(max_incs=args.steps)
+        coords = e.nodes(_abi.NODE_COORDS)
+        ips = e.ips()
+        t1 = time.perf_counter()
+        e.close()
+        wall = max_over_ranks(t1 - t0)
+        h2d = desc.coords.nbytes + desc.conn.nbytes + desc.v_init.nbytes + desc.bc_code.nbytes
+        d2h = coords.nbytes + ips.nbytes
+        e2e = {"value": world * desc.n_elems * args.steps / wall, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "what": "model upload + start of the solve + K increments + coordinates and point state read back"}
+
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": desc.n_elems, "nodes": desc.n_nodes,
+                   "gauss_points": desc.n_ips, "precision": args.precision, "time_step": "courant every 10",
+                   "increments_from_t0": [args.warmup, args.warmup + args.steps],
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": f"inputs larger than L2 (point state {desc.n_ips * 29 * word / 1e6:.0f} MB > 126 MB)"},
+        "roofline": roofline,
+        "step_roofline": step_roofline,
+        "gpu_launches": launches,
+        "fp64_resolves": ctl["fp64_resolves"],
+    }
+    if fp64:
+        out["fp64_path"] = fp64
+        out["mixed_over_fp64"] = (desc.n_elems * args.steps / (run_ms / 1e3)) / fp64["value"]
+    if clocks:
+        out["clocks"] = clocks
+    if e2e:
+        out["e2e"] = e2e
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(desc)
+    print(json.dumps(out))
+
+
+def main():
+    global AXIAL, WORKLOAD
+    args = parse()
+    AXIAL = args.axial
+    if AXIAL != 160:
+        WORKLOAD = f"taylor3d-copper-ogrid-{960 * AXIAL}-hex8"
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    dist = None
+    if world > 1:
+        # one process per GPU: this rank sees only its own device
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(0)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        run_engine_arm(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,886 @@
+// dnl_kernels.cuh - sm_100a kernels of one explicit increment.
+//
+// Per increment (one CUDA-graph replay):
+//   [k_bc_prep]   imposed-speed nodes: field0 values of the predictor BC
+//   k_element     strains, pressure, radial return, rotation, density, element forces
+//   k_nodal       CSR gather of element forces, Chung-Hulbert predictor+corrector, BCs
+//   k_courant     critical time step (only when due), warp-shuffle min + atomicMin
+//   k_control     end of step / start of the next one (time, dt, increment, swap)
+//
+// Data layout in HBM (all instances concatenated):
+//   nodes        double4 AoS (x, y, z, pad): coords, disp, u[2], v[2], a[2]; double mass
+//   elements     int32 conn[nE*npe]; int32 material
+//   points       Real ip[29][nIPpad] component-major (coalesced per component)
+//   force slots  Real4 slot[nE*npe]: one per (element, local node), written by the
+//                element pass, gathered per node in element order through a CSR list
+#pragma once
+
+#include "dnl_math.cuh"
+#include "dnlgpu.h"
+
+namespace dnl
+{
+
+// Per-instance solver state, resident on the device.
+struct __align__(128) Ctl
+{
+  double t, dt, t_end, t_stop;  // Model::currentTime, Solver::timeStep, end of solve, pause time
+  double dt_eff, t_new;         // time step and end time of the prepared increment
+  unsigned long long min_bits;  // atomicMin accumulator of l/c (positive double bits)
+  long long inc, inc_stop;      // Solver::currentIncrement, stop increment
+  int active, prepared, due, f0; // prepared increment runs / begin evaluated / dt recompute / field0 buffer
+  int status, bad, resolves, ts_freq;
+  double safety, omegaS, alphaM, beta, gammaN;
+  int elem_begin, elem_end, node_begin, node_end;
+  int ts_method, fun_time_base, pad0, pad1;
+};
+
+static constexpr unsigned long long INF_BITS = 0x7ff0000000000000ull;
+
+template <typename R> struct V4;
+template <> struct V4<double> { using type = double4; };
+template <> struct V4<float> { using type = float4; };
+
+struct DevModel
+{
+  int nInst, nN, nE, nIP, nIPpad, nSpeed, nFunc, pad;
+  const int *inst_elem_begin; // [nInst+1]
+  const int *inst_node_begin; // [nInst+1]
+  Ctl *ctl;
+  double4 *x, *disp;
+  double4 *u[2], *v[2], *a[2];
+  double *mass;
+  const int *conn;
+  const int *emat;
+  const MatDev *mat;
+  void *ip;
+  void *slot;
+  const int *csr_off, *csr_idx;
+  const uint8_t *bc;       // per node: 2 bits per component (DNL_BC_*)
+  const double4 *bcval;    // per node imposed speed (only read where the code is DNL_BC_SPEED)
+  const int4 *bcfun;       // per node function index per component (-1 none)
+  const int *speed_nodes;  // nodes carrying an imposed speed
+  const double *fx, *fy;   // packed function points
+  const int *foff;         // [nFunc+1]
+  double4 *fout;           // assembled forces (kernel-level entry point)
+};
+
+__device__ __forceinline__ int find_segment(const int *begin, int n, int v)
+{
+  int lo = 0, hi = n - 1;
+  while (lo < hi)
+  {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(begin + mid) <= v)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ double func_value(const DevModel &M, int f, double t)
+{
+  int b = M.foff[f], e = M.foff[f + 1];
+  const double *X = M.fx, *Y = M.fy;
+  if (t <= X[b])
+    return Y[b];
+  for (int i = b + 1; i < e; i++)
+    if (X[i] >= t)
+    {
+      if (X[i] == t)
+        return Y[i];
+      return ((t - X[i - 1]) / (X[i] - X[i - 1])) * (Y[i] - Y[i - 1]) + Y[i - 1];
+    }
+  return Y[e - 1];
+}
+
+__host__ __device__ __forceinline__ double &comp(double4 &v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// --------------------------------------------------------------- helpers
+
+// Sum v[] over the NPE lanes of an element group and leave in lane g the DIM
+// values of node g (a butterfly reduce-scatter: NPE/2, NPE/4, ... lanes apart).
+template <typename R, int NPE, int DIM>
+__device__ __forceinline__ void reduce_scatter(unsigned mask, int g, R (&w)[NPE * DIM])
+{
+#pragma unroll
+  for (int half = NPE / 2; half >= 1; half >>= 1)
+  {
+    const bool upper = (g & half) != 0;
+#pragma unroll
+    for (int k = 0; k < half * DIM; k++)
+    {
+      R send = upper ? w[k] : w[k + half * DIM];
+      R keep = upper ? w[k + half * DIM] : w[k];
+      w[k] = keep + __shfl_xor_sync(mask, send, half);
+    }
+  }
+}
+
+template <int NPE> __device__ __forceinline__ float group_sum(unsigned mask, float v)
+{
+#pragma unroll
+  for (int h = 1; h < NPE; h <<= 1)
+    v += __shfl_xor_sync(mask, v, h);
+  return v;
+}
+template <int NPE> __device__ __forceinline__ double group_sum(unsigned mask, double v)
+{
+#pragma unroll
+  for (int h = 1; h < NPE; h <<= 1)
+    v += __shfl_xor_sync(mask, v, h);
+  return v;
+}
+
+// local coordinate sign of node / Gauss point n along axis k (ElHex8N3D.C:33-90,
+// ElQua4NAx.C:28-60): (-,-,-) (+,-,-) (+,+,-) (-,+,-) (-,-,+) (+,-,+) (+,+,+) (-,+,+)
+__host__ __device__ constexpr int node_sign(int n, int k)
+{
+  return k == 0 ? ((n & 3) == 1 || (n & 3) == 2 ? 1 : -1) : (k == 1 ? ((n & 3) >= 2 ? 1 : -1) : (n >= 4 ? 1 : -1));
+}
+
+template <typename R> __device__ __forceinline__ R ipv(const DevModel &M, int c, int q)
+{
+  return reinterpret_cast<const R *>(M.ip)[(size_t)c * M.nIPpad + q];
+}
+template <typename R> __device__ __forceinline__ void ipw(const DevModel &M, int c, int q, R v)
+{
+  reinterpret_cast<R *>(M.ip)[(size_t)c * M.nIPpad + q] = v;
+}
+
+__device__ __forceinline__ void raise_status(Ctl *c, int code, int index)
+{
+  if (atomicCAS(&c->status, 0, code) == 0)
+    c->bad = index;
+}
+
+// FP64 re-solve of a point whose FP32 return failed its tests.
+__device__ __noinline__ bool resolve_fp64(const MatDev &mp, const float dE[6], double dt, ReturnState<float> &st,
+                                          const ReturnState<float> &st0)
+{
+  JC<double> jc;
+  jc.load(mp);
+  ReturnState<double> d;
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+  {
+    d.s[c] = st0.s[c];
+    d.ep[c] = st0.ep[c];
+  }
+  d.epsp = st0.epsp;
+  d.depsp = st0.depsp;
+  d.gamma = st0.gamma;
+  d.gcum = st0.gcum;
+  d.yield = st0.yield;
+  d.T = st0.T;
+  d.pressure = st0.pressure;
+  d.eint = st0.eint;
+  d.einel = st0.einel;
+  double de[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    de[c] = dE[c];
+  bool ok;
+  radial_return<double>(jc, mp.twoG, mp.heatFrac, 1.0 / mp.rho0, de, dt, d, ok);
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+  {
+    st.s[c] = (float)d.s[c];
+    st.ep[c] = (float)d.ep[c];
+  }
+  st.epsp = (float)d.epsp;
+  st.depsp = (float)d.depsp;
+  st.gamma = (float)d.gamma;
+  st.gcum = (float)d.gcum;
+  st.yield = (float)d.yield;
+  st.T = (float)d.T;
+  st.pressure = (float)d.pressure;
+  st.eint = (float)d.eint;
+  st.einel = (float)d.einel;
+  return ok;
+}
+
+// ---------------------------------------------------------- element pass
+
+// One thread per integration point; the NPE points of an element are NPE
+// consecutive lanes, and lane g also loads node g of the element.
+// MODE 0: one increment's element work (Explicit.C:204-226 + computeDensity,
+//         Element.C:1103-1256, with the Jacobian of ElementPlane.C:46-102 /
+//         Element3D.C:64-115 computed from the current coordinates).
+// MODE 1: start of the solve: reference Jacobian detJ0, initial point state
+//         (Element::initializeData, Element.C:258-301) and the element lumped
+//         masses (Element::computeMassMatrix, Element.C:304-339) into the slots.
+template <typename R, int NPE, int MODE>
+__global__ void __launch_bounds__(128) k_element(DevModel M)
+{
+  constexpr int DIM = (NPE == 8) ? 3 : 2;
+  constexpr bool AXI = (NPE == 4);
+  using R4 = typename V4<R>::type;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int g = lane & (NPE - 1);
+  const int base = lane & ~(NPE - 1);
+  const int e = q / NPE;
+  const bool valid = e < M.nE;
+  const int ec = valid ? e : M.nE - 1;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
+  Ctl *C = M.ctl + inst;
+  const bool act = valid && (MODE == 1 || C->active);
+  const unsigned amask = __ballot_sync(0xffffffffu, act);
+  if (!act)
+    return;
+  const int f0 = C->f0;
+  const MatDev &mp = M.mat[M.emat[e]];
+
+  // ---- gather the element's nodes (lane g <- node g)
+  const int node = M.conn[q];
+  const double4 X = M.x[node];
+  const double4 U = M.u[f0][node];
+  const double x0 = __shfl_sync(amask, X.x, base), y0 = __shfl_sync(amask, X.y, base),
+               z0 = __shfl_sync(amask, X.z, base);
+  const double ux0 = __shfl_sync(amask, U.x, base), uy0 = __shfl_sync(amask, U.y, base),
+               uz0 = __shfl_sync(amask, U.z, base);
+  // element-local offsets keep the FP32 path free of large-coordinate cancellation
+  const R rx = R(X.x - x0), ry = R(X.y - y0), rz = R(X.z - z0);
+  const R urx = R(U.x - ux0), ury = R(U.y - uy0), urz = R(U.z - uz0);
+
+  // ---- Jacobian J = sum x_n dN_n/dxi and G = sum du_n dN_n/dxi at this Gauss point
+  const R a = R(0.57735026918962576451); // 1/sqrt(3)
+  const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
+  R J[3][3], G[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      J[i][j] = G[i][j] = R(0);
+  R Nr = R(0), Vr = R(0);
+  R dN[NPE][DIM], Nv[NPE];
+#pragma unroll
+  for (int n = 0; n < NPE; n++)
+  {
+    const R s0 = R(node_sign(n, 0)), s1 = R(node_sign(n, 1)), s2 = R(node_sign(n, 2));
+    if constexpr (NPE == 8)
+    {
+      const R f0_ = R(1) + s0 * xi0, f1_ = R(1) + s1 * xi1, f2_ = R(1) + s2 * xi2;
+      dN[n][0] = s0 * f1_ * f2_ / R(8);
+      dN[n][1] = s1 * f0_ * f2_ / R(8);
+      dN[n][2] = s2 * f0_ * f1_ / R(8);
+      Nv[n] = f0_ * f1_ * f2_ / R(8);
+    }
+    else
+    {
+      const R f0_ = R(1) + s0 * xi0, f1_ = R(1) + s1 * xi1;
+      dN[n][0] = s0 * f1_ / R(4);
+      dN[n][1] = s1 * f0_ / R(4);
+      Nv[n] = f0_ * f1_ / R(4);
+    }
+    const R xn[3] = {__shfl_sync(amask, rx, base + n), __shfl_sync(amask, ry, base + n),
+                     DIM == 3 ? __shfl_sync(amask, rz, base + n) : R(0)};
+    const R un[3] = {__shfl_sync(amask, urx, base + n), __shfl_sync(amask, ury, base + n),
+                     DIM == 3 ? __shfl_sync(amask, urz, base + n) : R(0)};
+#pragma unroll
+    for (int i = 0; i < DIM; i++)
+#pragma unroll
+      for (int j = 0; j < DIM; j++)
+      {
+        J[i][j] += dN[n][j] * xn[i];
+        G[i][j] += dN[n][j] * un[i];
+      }
+    if (AXI)
+    {
+      Nr += Nv[n] * xn[0];
+      Vr += Nv[n] * un[0];
+    }
+  }
+  // axisymmetric radius r = sum N_n x_n (ElementAxi.C:46-59) and the radial
+  // displacement increment sum N_n du_n (ElementAxi.C:88-99), from the offsets
+  R radius = R(1);
+  if (AXI)
+  {
+    radius = R(x0 + (double)Nr);
+    Vr += R(ux0);
+  }
+  R detJ, inv[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      inv[i][j] = R(0);
+  if constexpr (DIM == 2)
+  {
+    detJ = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+    const R id = R(1) / detJ;
+    inv[0][0] = J[1][1] * id;
+    inv[0][1] = -J[0][1] * id;
+    inv[1][0] = -J[1][0] * id;
+    inv[1][1] = J[0][0] * id;
+  }
+  else
+  {
+    const R c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const R c01 = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+    const R c02 = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    detJ = J[0][0] * c00 + J[1][0] * c01 + J[2][0] * c02;
+    const R id = R(1) / detJ;
+    inv[0][0] = c00 * id;
+    inv[0][1] = c01 * id;
+    inv[0][2] = c02 * id;
+    inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) * id;
+    inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+    inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
+    inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+    inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  }
+  if (detJ < R(0))
+    raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
+
+  const R TWO_PI = R(6.28318530717958647692);
+  R WxdJ = detJ; // Gauss weight 1
+  if (AXI)
+    WxdJ *= TWO_PI * radius;
+
+  if constexpr (MODE == 1)
+  {
+    // reference Jacobian (ElementPlane.C:96-100), initial state, element masses
+    const R rho0 = R(mp.rho0);
+    ipw<R>(M, DNL_IP_DETJ0, q, AXI ? detJ * radius : detJ);
+#pragma unroll
+    for (int c = 0; c < DNL_IP_DETJ0; c++)
+      ipw<R>(M, c, q, R(0));
+    ipw<R>(M, DNL_IP_T, q, R(mp.T0));
+    ipw<R>(M, DNL_IP_DENSITY, q, rho0);
+    R me[NPE];
+#pragma unroll
+    for (int n = 0; n < NPE; n++)
+      me[n] = rho0 * Nv[n] * WxdJ;
+    reduce_scatter<R, NPE, 1>(amask, g, me);
+    R4 s;
+    s.x = me[0];
+    s.y = s.z = s.w = R(0);
+    reinterpret_cast<R4 *>(M.slot)[q] = s;
+    return;
+  }
+
+  const double dt = C->dt_eff;
+  // ---- F - I = G J^-1 (+ axisymmetric hoop term), polar decomposition
+  R H[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+    {
+      R s = R(0);
+#pragma unroll
+      for (int k = 0; k < DIM; k++)
+        s += G[i][k] * inv[k][j];
+      H[3 * i + j] = (i < DIM && j < DIM) ? s : R(0);
+    }
+  if (AXI)
+    H[8] = Vr / radius;
+  R dE[6], Rot[9];
+  polar_lnU<R>(H, dE, Rot);
+
+  // ---- element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
+  const R trSum = group_sum<NPE>(amask, dE[0] + dE[3] + dE[5]);
+
+  // ---- point state
+  ReturnState<R> st;
+  R strain[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+  {
+    st.s[c] = ipv<R>(M, DNL_IP_STRESS + c, q);
+    strain[c] = ipv<R>(M, DNL_IP_STRAIN + c, q);
+    st.ep[c] = ipv<R>(M, DNL_IP_PLASTIC_STRAIN + c, q);
+  }
+  st.epsp = ipv<R>(M, DNL_IP_EPSP, q);
+  st.depsp = ipv<R>(M, DNL_IP_DEPSP, q);
+  st.gamma = ipv<R>(M, DNL_IP_GAMMA, q);
+  st.gcum = ipv<R>(M, DNL_IP_GAMMA_CUM, q);
+  st.yield = ipv<R>(M, DNL_IP_YIELD, q);
+  st.T = ipv<R>(M, DNL_IP_T, q);
+  st.eint = ipv<R>(M, DNL_IP_EINT, q);
+  st.einel = ipv<R>(M, DNL_IP_EINEL, q);
+  const R detJ0 = ipv<R>(M, DNL_IP_DETJ0, q);
+  st.pressure = (st.s[0] + st.s[3] + st.s[5]) / R(3) + R(mp.K) * (trSum / R(NPE));
+
+  // ---- J2 radial return with Johnson-Cook hardening (Element.C:407-622)
+  {
+    JC<R> jc;
+    jc.load(mp);
+    ReturnState<R> st0 = st;
+    bool ok;
+    radial_return<R>(jc, R(mp.twoG), R(mp.heatFrac), R(1.0 / mp.rho0), dE, R(dt), st, ok);
+    if (!ok)
+    {
+      if constexpr (sizeof(R) == 4)
+      {
+        atomicAdd(&C->resolves, 1);
+        bool ok64 = resolve_fp64(mp, reinterpret_cast<const float *>(dE), dt,
+                                 reinterpret_cast<ReturnState<float> &>(st),
+                                 reinterpret_cast<const ReturnState<float> &>(st0));
+        if (!ok64)
+          raise_status(C, DNL_ERR_NEWTON, q);
+      }
+      else
+        raise_status(C, DNL_ERR_NEWTON, q);
+    }
+  }
+
+  // ---- total strain, final rotation for objectivity (Element.C:1116-1161)
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    strain[c] += dE[c];
+  rotate_sym<R>(Rot, st.s);
+  rotate_sym<R>(Rot, strain);
+  rotate_sym<R>(Rot, st.ep);
+  R rho = R(mp.rho0) * detJ0 / detJ; // Element::computeDensity (Element.C:1243-1256)
+  if (AXI)
+    rho /= radius;
+
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+  {
+    ipw<R>(M, DNL_IP_STRESS + c, q, st.s[c]);
+    ipw<R>(M, DNL_IP_STRAIN + c, q, strain[c]);
+    ipw<R>(M, DNL_IP_PLASTIC_STRAIN + c, q, st.ep[c]);
+  }
+  ipw<R>(M, DNL_IP_EPSP, q, st.epsp);
+  ipw<R>(M, DNL_IP_DEPSP, q, st.depsp);
+  ipw<R>(M, DNL_IP_GAMMA, q, st.gamma);
+  ipw<R>(M, DNL_IP_GAMMA_CUM, q, st.gcum);
+  ipw<R>(M, DNL_IP_YIELD, q, st.yield);
+  ipw<R>(M, DNL_IP_T, q, st.T);
+  ipw<R>(M, DNL_IP_PRESSURE, q, st.pressure);
+  ipw<R>(M, DNL_IP_EINT, q, st.eint);
+  ipw<R>(M, DNL_IP_EINEL, q, st.einel);
+  ipw<R>(M, DNL_IP_DENSITY, q, rho);
+
+  // ---- internal forces f_n = -sum_g dN_n/dx . sigma w detJ (Element.C:362-404):
+  // with P = -w detJ J^-1 sigma, f_n,i = sum_k dN_n/dxi_k P_ki
+  R P[DIM][DIM];
+#pragma unroll
+  for (int k = 0; k < DIM; k++)
+#pragma unroll
+    for (int i = 0; i < DIM; i++)
+    {
+      R s = R(0);
+#pragma unroll
+      for (int j = 0; j < DIM; j++)
+        s += inv[k][j] * st.s[sym_index(j, i)];
+      P[k][i] = -WxdJ * s;
+    }
+  R f[NPE * DIM];
+  const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
+#pragma unroll
+  for (int n = 0; n < NPE; n++)
+#pragma unroll
+    for (int i = 0; i < DIM; i++)
+    {
+      R s = R(0);
+#pragma unroll
+      for (int k = 0; k < DIM; k++)
+        s += dN[n][k] * P[k][i];
+      if (AXI && i == 0)
+        s -= Nv[n] * hoop;
+      f[n * DIM + i] = s;
+    }
+  reduce_scatter<R, NPE, DIM>(amask, g, f);
+  R4 fs;
+  fs.x = f[0];
+  fs.y = f[1];
+  fs.z = (DIM == 3) ? f[DIM - 1] : R(0);
+  fs.w = R(0);
+  reinterpret_cast<R4 *>(M.slot)[q] = fs;
+}
+
+// ------------------------------------------------------------ nodal update
+
+// Explicit::computePredictions (Explicit.C:438-482) fused with
+// Explicit::explicitSolve (Explicit.C:489-536): the nodal force is gathered
+// from the element slots in element order (the order of the scatter-add of
+// Model::computeInternalForces, Model.C:881-898), then the Chung-Hulbert
+// corrector and the boundary conditions, then disp += du, coords += du.
+template <typename R, int DIM>
+__global__ void __launch_bounds__(256) k_nodal(DevModel M)
+{
+  using R4 = typename V4<R>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nN)
+    return;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
+  const Ctl *C = M.ctl + inst;
+  if (!C->active)
+    return;
+  const double dt = C->dt_eff, t = C->t;
+  const double beta = C->beta, gam = C->gammaN, alphaM = C->alphaM;
+  const int f0 = C->f0, f1 = 1 - f0;
+  double4 f = make_double4(0, 0, 0, 0);
+  const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
+  const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
+  for (int k = kb; k < ke; k++)
+  {
+    const R4 s = slot[M.csr_idx[k]];
+    f.x += (double)s.x;
+    f.y += (double)s.y;
+    f.z += (double)s.z;
+  }
+  const double m = M.mass[i];
+  double4 v0 = M.v[f0][i], a0 = M.a[f0][i];
+  const unsigned code = M.bc[i];
+  double4 du, v1, a1;
+  du.w = v1.w = a1.w = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+  {
+    const double vc = comp(v0, c), ac = comp(a0, c);
+    double u_ = dt * (vc + (0.5 - beta) * dt * ac);
+    double v_ = vc + (1.0 - gam) * dt * ac;
+    double a_ = (c < DIM) ? comp(f, c) / m : 0.0;
+    a_ = (a_ - alphaM * ac) / (1.0 - alphaM);
+    v_ += gam * dt * a_;
+    u_ += beta * (dt * dt) * a_;
+    comp(du, c) = u_;
+    comp(v1, c) = v_;
+    comp(a1, c) = a_;
+  }
+  if (code)
+  {
+    // BoundaryRestrain.C:98-128, BoundarySpeed.C:139-206 (both fields)
+    double4 u0 = M.u[f0][i];
+    for (int c = 0; c < 3; c++)
+    {
+      const unsigned cc = (code >> (2 * c)) & 3u;
+      if (cc == DNL_BC_RESTRAIN)
+      {
+        comp(du, c) = comp(v1, c) = comp(a1, c) = 0.0;
+        comp(u0, c) = comp(v0, c) = comp(a0, c) = 0.0;
+      }
+      else if (cc == DNL_BC_SPEED)
+      {
+        double4 sv = M.bcval[i];
+        int4 sf = M.bcfun[i];
+        const double s = comp(sv, c);
+        const int fn = c == 0 ? sf.x : (c == 1 ? sf.y : sf.z);
+        double va = s, vb = s, acc = 0.0;
+        if (fn >= 0)
+        {
+          const double fa = func_value(M, fn, t), fb = func_value(M, fn, t + dt);
+          acc = (fb - fa) * s / dt;
+          va = fa * s;
+          vb = fb * s;
+        }
+        comp(a0, c) = comp(a1, c) = acc;
+        comp(v0, c) = va;
+        comp(v1, c) = vb;
+        comp(u0, c) = va * dt;
+        comp(du, c) = vb * dt;
+      }
+    }
+    M.u[f0][i] = u0;
+    M.v[f0][i] = v0;
+    M.a[f0][i] = a0;
+  }
+  double4 X = M.x[i], D = M.disp[i];
+  X.x += du.x;
+  X.y += du.y;
+  X.z += du.z;
+  D.x += du.x;
+  D.y += du.y;
+  D.z += du.z;
+  M.x[i] = X;
+  M.disp[i] = D;
+  M.u[f1][i] = du;
+  M.v[f1][i] = v1;
+  M.a[f1][i] = a1;
+}
+
+// Predictor boundary conditions on field0 of the imposed-speed nodes before the
+// element pass (the element pass reads field0->u, Element.C:1114).
+__global__ void k_bc_prep(DevModel M)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= M.nSpeed)
+    return;
+  const int i = M.speed_nodes[k];
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
+  const Ctl *C = M.ctl + inst;
+  if (!C->active)
+    return;
+  const double dt = C->dt_eff, t = C->t;
+  const int f0 = C->f0;
+  const unsigned code = M.bc[i];
+  double4 u0 = M.u[f0][i], v0 = M.v[f0][i], a0 = M.a[f0][i];
+  const double4 sv = M.bcval[i];
+  const int4 sf = M.bcfun[i];
+  for (int c = 0; c < 3; c++)
+  {
+    if (((code >> (2 * c)) & 3u) != DNL_BC_SPEED)
+      continue;
+    double4 svc = sv;
+    const double s = comp(svc, c);
+    const int fn = c == 0 ? sf.x : (c == 1 ? sf.y : sf.z);
+    double va = s, acc = 0.0;
+    if (fn >= 0)
+    {
+      const double fa = func_value(M, fn, t), fb = func_value(M, fn, t + dt);
+      acc = (fb - fa) * s / dt;
+      va = fa * s;
+    }
+    comp(a0, c) = acc;
+    comp(v0, c) = va;
+    comp(u0, c) = va * dt;
+  }
+  M.u[f0][i] = u0;
+  M.v[f0][i] = v0;
+  M.a[f0][i] = a0;
+}
+
+// Sum the element slots of every node (lumped mass at the start, or the
+// internal forces for the kernel-level entry point).
+template <typename R>
+__global__ void k_gather(DevModel M, int what)
+{
+  using R4 = typename V4<R>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nN)
+    return;
+  const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
+  double4 f = make_double4(0, 0, 0, 0);
+  for (int k = M.csr_off[i]; k < M.csr_off[i + 1]; k++)
+  {
+    const R4 s = slot[M.csr_idx[k]];
+    f.x += (double)s.x;
+    f.y += (double)s.y;
+    f.z += (double)s.z;
+  }
+  if (what == 0)
+    M.mass[i] = f.x;
+  else
+    M.fout[i] = f;
+}
+
+// ------------------------------------------------------------- time step
+
+__device__ __forceinline__ double3 d3(const double4 &v) { return make_double3(v.x, v.y, v.z); }
+__device__ __forceinline__ double3 sub(double3 a, double3 b) { return make_double3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double3 cross(double3 a, double3 b)
+{
+  return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double norm(double3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ double dot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// ElHex8N3D::getCharacteristicLength (ElHex8N3D.C:634-649): volume
+// (ElHex8N3D::getVolume, three pyramids with apex at node 7, ElHex8N3D.C:651-686)
+// over the largest face area (half the cross product of the face diagonals).
+__device__ __forceinline__ double charlen_hex(const double3 P[8])
+{
+  const int faces[6][4] = {{0, 1, 2, 3}, {0, 1, 5, 4}, {1, 2, 6, 5}, {3, 2, 6, 7}, {0, 3, 7, 4}, {4, 5, 6, 7}};
+  double amax = 0.0;
+#pragma unroll
+  for (int f = 0; f < 6; f++)
+  {
+    const double a = 0.5 * norm(cross(sub(P[faces[f][0]], P[faces[f][2]]), sub(P[faces[f][1]], P[faces[f][3]])));
+    amax = fmax(amax, a);
+  }
+  double vol = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+  {
+    const double3 A = P[faces[k][0]], B = P[faces[k][1]], Cc = P[faces[k][2]], D = P[faces[k][3]];
+    const double3 ab = sub(B, A), ac = sub(Cc, A), ad = sub(D, A);
+    const double area = (norm(cross(ab, ac)) + norm(cross(ad, ac))) / 2.0;
+    double3 nr = cross(ab, ad);
+    const double nn = norm(nr);
+    nr = make_double3(nr.x / nn, nr.y / nn, nr.z / nn);
+    const double h = fabs(dot(nr, sub(P[7], A)));
+    vol += area * h / 3.0;
+  }
+  return vol / amax;
+}
+
+// ElQua4NAx::getCharacteristicLength (ElQua4NAx.C:312-321).
+__device__ __forceinline__ double charlen_q4(const double3 P[4])
+{
+  const double x31 = P[2].x - P[0].x, x24 = P[1].x - P[3].x, y42 = P[3].y - P[1].y, y31 = P[2].y - P[0].y;
+  return (x31 * y42 + x24 * y31) / sqrt(2.0 * (x24 * x24 + y42 * y42 + x31 * x31 + y31 * y31));
+}
+
+// Model::computeCourantTimeStep (Model.C:636-669): min over elements of l_e/c_e
+// with the elongation wave speed of the mean point density (Element.C:343-359).
+// One thread per element, a segmented warp-shuffle min over the lanes of one
+// instance, then one atomicMin per instance and warp.
+template <typename R, int NPE>
+__global__ void __launch_bounds__(256) k_courant(DevModel M, int force)
+{
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool valid = e < M.nE;
+  const int ec = valid ? e : M.nE - 1;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
+  Ctl *C = M.ctl + inst;
+  const bool act = valid && (force || (C->active && C->due));
+  if (__ballot_sync(0xffffffffu, act) == 0)
+    return;
+  double ratio = 1e300;
+  if (act)
+  {
+    double3 P[NPE];
+#pragma unroll
+    for (int n = 0; n < NPE; n++)
+      P[n] = d3(M.x[M.conn[e * NPE + n]]);
+    double len;
+    if constexpr (NPE == 8)
+      len = charlen_hex(P);
+    else
+      len = charlen_q4(P);
+    double rho = 0.0;
+#pragma unroll
+    for (int g = 0; g < NPE; g++)
+      rho += (double)ipv<R>(M, DNL_IP_DENSITY, e * NPE + g);
+    rho /= NPE;
+    const MatDev &mp = M.mat[M.emat[e]];
+    ratio = len / sqrt(mp.wave2 / rho);
+  }
+  // segmented min: lanes of one instance form a contiguous run
+  const int key = act ? inst : -1;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1)
+  {
+    const double o = __shfl_down_sync(0xffffffffu, ratio, off);
+    const int ok = __shfl_down_sync(0xffffffffu, key, off);
+    if (lane + off < 32 && ok == key)
+      ratio = fmin(ratio, o);
+  }
+  const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  if (act && (lane == 0 || prev != key))
+    atomicMin(&C->min_bits, (unsigned long long)__double_as_longlong(ratio));
+}
+
+// ---------------------------------------------------------------- control
+
+enum
+{
+  CTL_FINISH = 0,   // end of the increment that ran, then begin the next one
+  CTL_LIMITS = 1,   // new pause time / increment budget, then begin
+  CTL_INIT_DT = 2,  // after the forced Courant pass of the start: dt, then arm the first element pass
+  CTL_POST_INIT = 3 // after the first element pass
+};
+
+__device__ __forceinline__ void begin_increment(Ctl &c)
+{
+  // Explicit::updateTimes (Explicit.C:414-427) for the increment to come
+  const bool go = c.status == 0 && c.t < c.t_end && c.t < c.t_stop && c.inc < c.inc_stop;
+  if (go)
+  {
+    if (c.t + c.dt > c.t_end)
+      c.dt = c.t_end - c.t;
+    c.inc += 1;
+    c.dt_eff = c.dt;
+    c.t_new = c.t + c.dt;
+    // Solver::computeTimeStep runs after the Jacobian when the solve goes on (Explicit.C:239-254, Solver.C:200)
+    c.due = (c.t_new < c.t_end) && (c.inc % c.ts_freq == 0);
+  }
+  else
+    c.due = 0;
+  c.active = go;
+  c.prepared = 1;
+}
+
+__device__ __forceinline__ void apply_courant(Ctl &c)
+{
+  // Solver::computeTimeStep (Solver.C:205-226): omega_max = 2 / dt_crit
+  const double crit = __longlong_as_double((long long)c.min_bits);
+  c.dt = c.safety * c.omegaS / (2.0 / crit);
+  c.min_bits = INF_BITS;
+}
+
+__global__ void k_control(DevModel M, int phase, double t_stop, long long max_incs)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nInst)
+    return;
+  Ctl &c = M.ctl[i];
+  if (phase == CTL_FINISH)
+  {
+    if (c.prepared && c.active && c.status == 0)
+    {
+      // Explicit::endStep (Explicit.C:539-552): time, then the nodal field swap
+      c.t = c.t_new;
+      c.f0 ^= 1;
+      if (c.due)
+        apply_courant(c);
+    }
+    c.prepared = 0;
+    c.active = 0;
+    begin_increment(c);
+  }
+  else if (phase == CTL_LIMITS)
+  {
+    const long long committed = c.inc - ((c.prepared && c.active) ? 1 : 0);
+    c.inc = committed;
+    c.t_stop = t_stop;
+    c.inc_stop = (max_incs > 0) ? committed + max_incs : 0x7fffffffffffffffll;
+    c.prepared = 0;
+    c.active = 0;
+    begin_increment(c);
+  }
+  else if (phase == CTL_INIT_DT)
+  {
+    apply_courant(c);
+    c.dt_eff = c.dt;
+    c.active = (c.status == 0);
+    c.prepared = 0;
+    c.due = 0;
+  }
+  else
+  {
+    c.active = 0;
+    c.prepared = 0;
+  }
+}
+
+// -------------------------------------------------------------- energies
+
+// One block per instance, fixed-order tree sums (deterministic).
+template <typename R, int NPE>
+__global__ void k_energies(DevModel M, double *out /* [nInst*3] */, int speed_field)
+{
+  const int inst = blockIdx.x;
+  const Ctl &c = M.ctl[inst];
+  __shared__ double sh[3][256];
+  double ke = 0.0, ei = 0.0, ep = 0.0;
+  const int fsel = speed_field ? (1 - c.f0) : c.f0;
+  for (int i = c.node_begin + threadIdx.x; i < c.node_end; i += blockDim.x)
+  {
+    const double4 v = M.v[fsel][i];
+    ke += M.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0;
+  }
+  const double wfac = (NPE == 4) ? 6.28318530717958647692 : 1.0;
+  for (int q = c.elem_begin * NPE + threadIdx.x; q < c.elem_end * NPE; q += blockDim.x)
+  {
+    const MatDev &mp = M.mat[M.emat[q / NPE]];
+    const double w = mp.rho0 * (double)ipv<R>(M, DNL_IP_DETJ0, q) * wfac;
+    ei += w * (double)ipv<R>(M, DNL_IP_EINT, q);
+    ep += w * (double)ipv<R>(M, DNL_IP_EINEL, q);
+  }
+  sh[0][threadIdx.x] = ke;
+  sh[1][threadIdx.x] = ei;
+  sh[2][threadIdx.x] = ep;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1)
+  {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 3; k++)
+        sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++)
+      out[3 * inst + k] = sh[k][0];
+}
+
+} // namespace dnl

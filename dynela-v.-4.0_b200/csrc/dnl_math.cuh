@@ -1,0 +1,391 @@
+// dnl_math.cuh - device tensor algebra, polar decomposition and the
+// Johnson-Cook J2 radial return of the DynELA hot path, templated on the
+// arithmetic type (double for the FP64 path, float for the mixed path).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dnl
+{
+
+template <typename R> struct Num;
+template <> struct Num<double>
+{
+  static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+  static __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
+  static __device__ __forceinline__ double log_(double x) { return log(x); }
+  static __device__ __forceinline__ double log1p_(double x) { return log1p(x); }
+  static __device__ __forceinline__ double pow_(double x, double y) { return pow(x, y); }
+  static __device__ __forceinline__ double abs_(double x) { return fabs(x); }
+  static __device__ __forceinline__ double div_(double a, double b) { return a / b; }
+  static constexpr double eps = 2.220446049250313e-16;
+};
+template <> struct Num<float>
+{
+  static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+  static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+  static __device__ __forceinline__ float log_(float x) { return __logf(x); }
+  static __device__ __forceinline__ float log1p_(float x) { return log1pf(x); }
+  // x^y for x > 0 through the fast base-2 exponential and logarithm
+  static __device__ __forceinline__ float pow_(float x, float y) { return exp2f(y * __log2f(x)); }
+  static __device__ __forceinline__ float abs_(float x) { return fabsf(x); }
+  static __device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+  static constexpr float eps = 1.1920929e-7f;
+};
+
+// symmetric storage xx, xy, xz, yy, yz, zz (SymTensor2 _data order)
+__host__ __device__ constexpr int sym_index(int i, int j)
+{
+  return (i == j) ? (i == 0 ? 0 : (i == 1 ? 3 : 5)) : ((i + j) == 1 ? 1 : ((i + j) == 2 ? 2 : 4));
+}
+
+template <typename R> struct Sym
+{
+  R v[6];
+};
+
+template <typename R> __device__ __forceinline__ R sym_norm(const R s[6])
+{
+  return Num<R>::sqrt_(s[0] * s[0] + s[3] * s[3] + s[5] * s[5] + R(2) * (s[1] * s[1] + s[2] * s[2] + s[4] * s[4]));
+}
+
+template <typename R> __device__ __forceinline__ R sym_ddot(const R a[6], const R b[6])
+{
+  return a[0] * b[0] + a[3] * b[3] + a[5] * b[5] + R(2) * (a[1] * b[1] + a[2] * b[2] + a[4] * b[4]);
+}
+
+// S <- Q S Q^T for a full 3x3 Q (row-major) and symmetric S (SymTensor2::dotRxRT).
+template <typename R> __device__ __forceinline__ void rotate_sym(const R Q[9], R S[6])
+{
+  R T[9]; // T = Q S
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      T[3 * i + j] = Q[3 * i] * S[sym_index(0, j)] + Q[3 * i + 1] * S[sym_index(1, j)] + Q[3 * i + 2] * S[sym_index(2, j)];
+  R out[6];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++)
+      out[sym_index(i, j)] = T[3 * i] * Q[3 * j] + T[3 * i + 1] * Q[3 * j + 1] + T[3 * i + 2] * Q[3 * j + 2];
+#pragma unroll
+  for (int k = 0; k < 6; k++)
+    S[k] = out[k];
+}
+
+// One Jacobi rotation zeroing A(p, q) of the symmetric matrix held in A6,
+// accumulated into the eigenvector matrix V (columns).
+template <typename R, int P, int Q>
+__device__ __forceinline__ void jacobi_rotate(R A[3][3], R V[3][3])
+{
+  R apq = A[P][Q];
+  if (apq == R(0))
+    return;
+  R theta = (A[Q][Q] - A[P][P]) / (R(2) * apq);
+  R at = Num<R>::abs_(theta);
+  R t;
+  if (at > R(1e18))
+    t = R(0.5) / theta;
+  else
+    t = (theta >= R(0) ? R(1) : R(-1)) / (at + Num<R>::sqrt_(theta * theta + R(1)));
+  R c = Num<R>::rsqrt_(t * t + R(1));
+  R s = t * c;
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+  {
+    R arp = A[r][P], arq = A[r][Q];
+    A[r][P] = c * arp - s * arq;
+    A[r][Q] = s * arp + c * arq;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+  {
+    R apr = A[P][r], aqr = A[Q][r];
+    A[P][r] = c * apr - s * aqr;
+    A[Q][r] = s * apr + c * aqr;
+  }
+  A[P][Q] = A[Q][P] = R(0);
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+  {
+    R vrp = V[r][P], vrq = V[r][Q];
+    V[r][P] = c * vrp - s * vrq;
+    V[r][Q] = s * vrp + c * vrq;
+  }
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix (Golub & Van
+// Loan, Matrix Computations, sec. 8.5).  mu receives the eigenvalues, the
+// columns of V the eigenvectors.
+template <typename R> __device__ __forceinline__ void sym_eigen3(const R a6[6], R mu[3], R V[3][3])
+{
+  R A[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+    {
+      A[i][j] = a6[sym_index(i, j)];
+      V[i][j] = (i == j) ? R(1) : R(0);
+    }
+  const R tol = Num<R>::eps * R(1e-2);
+  for (int sweep = 0; sweep < 12; sweep++)
+  {
+    R off = Num<R>::abs_(A[0][1]) + Num<R>::abs_(A[0][2]) + Num<R>::abs_(A[1][2]);
+    R scale = Num<R>::abs_(A[0][0]) + Num<R>::abs_(A[1][1]) + Num<R>::abs_(A[2][2]) + off;
+    if (off <= tol * scale)
+      break;
+    jacobi_rotate<R, 0, 1>(A, V);
+    jacobi_rotate<R, 0, 2>(A, V);
+    jacobi_rotate<R, 1, 2>(A, V);
+  }
+  mu[0] = A[0][0];
+  mu[1] = A[1][1];
+  mu[2] = A[2][2];
+}
+
+// Polar decomposition F = R U of F = I + H and the logarithmic strain
+// increment ln U (Tensor2::polarCuppenLnU, Tensor2.C:1237-1457, restated):
+// with A = F^T F - I = H + H^T + H^T H and its eigenpairs (mu_k, n_k),
+// ln U = sum log1p(mu_k)/2 n_k n_k and R = F U^-1, U^-1 = sum (1+mu_k)^-1/2 n_k n_k.
+// Working on F^T F - I keeps the relative precision of the small increments.
+template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R lnU[6], R Rot[9])
+{
+  R A[6];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++)
+      A[sym_index(i, j)] = H[3 * i + j] + H[3 * j + i] + H[i] * H[j] + H[3 + i] * H[3 + j] + H[6 + i] * H[6 + j];
+  R mu[3], V[3][3];
+  sym_eigen3<R>(A, mu, V);
+  R hl[3], g[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+  {
+    hl[k] = R(0.5) * Num<R>::log1p_(mu[k]);
+    g[k] = Num<R>::rsqrt_(R(1) + mu[k]) - R(1); // (1+mu)^-1/2 - 1
+  }
+  R Wm[6]; // U^-1 - I
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++)
+    {
+      R a = R(0), b = R(0);
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+      {
+        R p = V[i][k] * V[j][k];
+        a += hl[k] * p;
+        b += g[k] * p;
+      }
+      lnU[sym_index(i, j)] = a;
+      Wm[sym_index(i, j)] = b;
+    }
+  // R = (I + H)(I + Wm) = I + H + Wm + H Wm
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+    {
+      R s = H[3 * i + j] + Wm[sym_index(i, j)];
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        s += H[3 * i + k] * Wm[sym_index(k, j)];
+      Rot[3 * i + j] = s + ((i == j) ? R(1) : R(0));
+    }
+}
+
+// Johnson-Cook parameters of one material, with the constants the return uses.
+struct MatDev
+{
+  double young, poisson, rho0, cp, tq, T0;
+  double A, B, C, n, m, depsp0, Tm, Tref;
+  double twoG, K, heatFrac, wave2; // E/(1+nu), E/(3(1-2nu)), tq/(rho0 Cp), E(1-nu)/((1+nu)(1-2nu))
+};
+
+template <typename R> struct JC
+{
+  R A, B, C, n, m, depsp0, Tm, Tref, invTmT, thermal; // thermal = tq/(rho0 Cp)
+  __device__ __forceinline__ void load(const MatDev &p)
+  {
+    A = R(p.A); B = R(p.B); C = R(p.C); n = R(p.n); m = R(p.m); depsp0 = R(p.depsp0);
+    Tm = R(p.Tm); Tref = R(p.Tref); invTmT = R(1.0 / (p.Tm - p.Tref)); thermal = R(p.heatFrac);
+  }
+  // JohnsonCookLaw::getYieldStress (JohnsonCookLaw.C:146-170) and the analytic
+  // total derivative getDerivateYieldStress (JohnsonCookLaw.C:298-339), in one pass.
+  __device__ __forceinline__ void eval(R epsp, R depsp, R T, R dt, R &yield, R &hard, bool wantHard) const
+  {
+    R pn = Num<R>::pow_(epsp, n); // epsp^n
+    R hard0 = A + B * pn;
+    bool rate = depsp > depsp0;
+    R visc0 = rate ? R(1) + C * Num<R>::log_(depsp / depsp0) : R(1);
+    R temp0 = R(1), temp1 = R(0);
+    bool hot = T > Tref, melt = !(T < Tm);
+    if (hot)
+    {
+      if (!melt)
+      {
+        temp1 = Num<R>::pow_((T - Tref) * invTmT, m);
+        temp0 = R(1) - temp1;
+      }
+      else
+        temp0 = R(0);
+    }
+    yield = hard0 * visc0 * temp0;
+    if (wantHard)
+    {
+      R h = n * B * (epsp > R(0) ? pn / epsp : R(0)) * visc0 * temp0; // n B epsp^(n-1) ...
+      if (rate)
+        h += hard0 * C * temp0 / (depsp * dt);
+      if (hot && !melt)
+        h -= m * thermal * hard0 * hard0 * visc0 * visc0 * temp0 * temp1 / (T - Tref);
+      hard = h;
+    }
+  }
+};
+
+// Per-point state handled by the radial return.
+template <typename R> struct ReturnState
+{
+  R s[6];   // stress (in: old, out: new, before the final rotation)
+  R ep[6];  // plastic strain tensor
+  R epsp, depsp, gamma, gcum, yield, T, pressure, eint, einel;
+};
+
+// Element::computeStress (Element.C:407-622) for one integration point.  The
+// Newton-bisection iteration on gamma is the reference's; tolNR = 1e-8 and
+// itMax = 250 for FP64.  For FP32 the step tolerance is widened to a few ulp
+// of gamma and `ok` is cleared when the iteration fails to converge in 60
+// steps or the final residual test |f| <= 1e-5 Strial + 2 f' tol fails; the
+// caller then re-solves the point in FP64.
+template <typename R>
+__device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac, R inv_rho0, const R dE[6], R dt,
+                                             ReturnState<R> &st, bool &ok)
+{
+  const R SQ32 = R(1.2247448713915890491), SQ23 = R(0.81649658092772603273);
+  const R gammaInitial = R(1e-8);
+  const bool fp64 = sizeof(R) == 8;
+  const int itMax = fp64 ? 250 : 60;
+  R twoG32 = SQ32 * twoG;
+  R sOld[6], dev[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    sOld[c] = st.s[c];
+  R p0 = (sOld[0] + sOld[3] + sOld[5]) / R(3);
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    dev[c] = sOld[c];
+  dev[0] -= p0;
+  dev[3] -= p0;
+  dev[5] -= p0;
+  R Snorm0 = sym_norm(dev);
+  R pe = (dE[0] + dE[3] + dE[5]) / R(3);
+  dev[0] += twoG * (dE[0] - pe);
+  dev[1] += twoG * dE[1];
+  dev[2] += twoG * dE[2];
+  dev[3] += twoG * (dE[3] - pe);
+  dev[4] += twoG * dE[4];
+  dev[5] += twoG * (dE[5] - pe);
+  R Snorm = sym_norm(dev);
+  R Strial = SQ32 * Snorm;
+  R T0 = st.T, T = T0;
+  R epsp0 = st.epsp;
+  R gamma = R(0);
+  R yield = st.yield;
+  R dummy;
+  int iterate = 0;
+  ok = true;
+  if (yield == R(0))
+  {
+    jc.eval(gammaInitial, gammaInitial / dt, T, dt, yield, dummy, false);
+    st.yield = yield;
+  }
+  if (Strial > yield)
+  {
+    R gammaMin = R(0);
+    R gammaMax = (Strial - yield) / twoG32;
+    gamma = st.gamma;
+    if (epsp0 == R(0))
+      gamma = SQ32 * gammaInitial;
+    R depsp = SQ23 * gamma / dt;
+    R epsp = epsp0 + SQ23 * gamma;
+    T = T0 + R(0.5) * gamma * heatFrac * (SQ23 * yield + Snorm0);
+    R fun = R(0), dfun = twoG32, tol = R(1e-8);
+    for (;;)
+    {
+      R hard;
+      jc.eval(epsp, depsp, T, dt, yield, hard, true);
+      fun = Strial - gamma * twoG32 - yield;
+      if (fun < R(0))
+        gammaMax = gamma;
+      else
+        gammaMin = gamma;
+      dfun = twoG32 + SQ23 * hard;
+      R dgamma = fun / dfun;
+      gamma += dgamma;
+      if ((gammaMax - gamma) * (gamma - gammaMin) < R(0))
+      {
+        dgamma = R(0.5) * (gammaMax - gammaMin);
+        gamma = gammaMin + dgamma;
+      }
+      R tolRel = R(4) * Num<R>::eps * Num<R>::abs_(gamma);
+      tol = (fp64 || tolRel < R(1e-8)) ? R(1e-8) : tolRel;
+      if (Num<R>::abs_(dgamma) < tol)
+        break;
+      depsp = SQ23 * gamma / dt;
+      epsp = epsp0 + SQ23 * gamma;
+      T = T0 + R(0.5) * gamma * heatFrac * (SQ23 * yield + Snorm0);
+      iterate += 1;
+      if (iterate > itMax || !(gamma == gamma))
+      {
+        ok = false;
+        return iterate;
+      }
+    }
+    // FP32 acceptance: the last residual is the one before the final Newton
+    // step, so it is bounded by dfun times the step tolerance
+    if (!fp64 && !(Num<R>::abs_(fun) <= R(1e-5) * Strial + R(2) * dfun * tol))
+    {
+      ok = false;
+      return iterate;
+    }
+    R invS = R(1) / Snorm;
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      st.ep[c] += gamma * dev[c] * invS;
+    R scale = R(1) - twoG * gamma * invS;
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      dev[c] *= scale;
+    st.epsp = epsp0 + SQ23 * gamma;
+    st.depsp = SQ23 * gamma / dt;
+    st.gamma = gamma;
+    st.gcum += gamma;
+    st.yield = yield;
+  }
+  R p = st.pressure;
+  st.s[0] = dev[0] + p;
+  st.s[1] = dev[1];
+  st.s[2] = dev[2];
+  st.s[3] = dev[3] + p;
+  st.s[4] = dev[4];
+  st.s[5] = dev[5] + p;
+  R sum[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    sum[c] = sOld[c] + st.s[c];
+  st.eint += R(0.5) * sym_ddot(dE, sum) * inv_rho0;
+  if (gamma != R(0))
+  {
+    R plWorkInc = R(0.5) * gamma * (sym_norm(dev) + Snorm0);
+    st.einel += plWorkInc * inv_rho0;
+    st.T += heatFrac * plWorkInc;
+  }
+  return iterate;
+}
+
+} // namespace dnl

@@ -1,0 +1,987 @@
+// engine.cu - host side of the B200 explicit-dynamics engine: model upload,
+// node->slot CSR lists, the increment captured as a CUDA graph, the device-
+// resident run loop, state access and the C ABI declared in include/dnlgpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dnl_kernels.cuh"
+#include "dnlgpu.h"
+
+using namespace dnl;
+
+namespace
+{
+char g_create_err[512] = "";
+
+template <typename T> struct DBuf
+{
+  T *p = nullptr;
+  size_t n = 0;
+};
+} // namespace
+
+struct dnl_engine
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int type = 0, npe = 0, dim = 0, precision = 0;
+  int nInst = 0, nN = 0, nE = 0, nIP = 0, nIPpad = 0, nSpeed = 0, nFunc = 0;
+  bool hasSpeed = false;
+  DevModel M{};
+  std::vector<void *> allocs;
+  std::vector<int> elemBegin, nodeBegin;
+  std::vector<Ctl> ctlInit;
+  Ctl *hctl = nullptr; // pinned mirror of the control blocks
+  double *denergy = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  bool timing = false;
+  double times[4] = {0, 0, 0, 0};
+  long long launches = 0;
+  int launchesPerStep = 0;
+  bool initialized = false;
+  std::string err;
+};
+
+namespace
+{
+int fail(dnl_engine *h, int code, const char *fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h)
+    h->err = buf;
+  else
+    snprintf(g_create_err, sizeof(g_create_err), "%s", buf);
+  return code;
+}
+
+#define CK(call)                                                                                                  \
+  do                                                                                                              \
+  {                                                                                                               \
+    cudaError_t e_ = (call);                                                                                      \
+    if (e_ != cudaSuccess)                                                                                        \
+      return fail(h, DNL_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);  \
+  } while (0)
+
+template <typename T> int dalloc(dnl_engine *h, T **p, size_t n)
+{
+  *p = nullptr;
+  if (n == 0)
+    n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(h, DNL_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+  h->allocs.push_back(*p);
+  return DNL_OK;
+}
+
+template <typename T> int upload(dnl_engine *h, T **p, const std::vector<T> &v)
+{
+  int rc = dalloc(h, p, v.size());
+  if (rc)
+    return rc;
+  if (!v.empty())
+    CK(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+  return DNL_OK;
+}
+
+int copy(dnl_engine *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind)
+{
+  CK(cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DNL_OK;
+}
+
+int npe_of(int type) { return type == DNL_ELQUA4NAX ? 4 : (type == DNL_ELHEX8N3D ? 8 : 0); }
+
+int check_desc(const dnl_model_desc *d, int idx)
+{
+  if (!d)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: NULL description", idx);
+  if (npe_of(d->elem_type) == 0)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: unknown element type %d", idx, d->elem_type);
+  if (d->n_nodes <= 0 || d->n_elems <= 0 || !d->coords || !d->conn)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: empty mesh", idx);
+  if (d->n_materials <= 0 || !d->materials)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: no material", idx);
+  if (d->ts_method != DNL_TS_COURANT)
+    return fail(nullptr, DNL_ERR_UNSUPPORTED, "model %d: only the Courant time step is available on the GPU path",
+                idx);
+  if (d->precision != DNL_PREC_FP64 && d->precision != DNL_PREC_MIXED)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: unknown precision %d", idx, d->precision);
+  const int npe = npe_of(d->elem_type);
+  for (long k = 0; k < (long)d->n_elems * npe; k++)
+    if (d->conn[k] < 0 || d->conn[k] >= d->n_nodes)
+      return fail(nullptr, DNL_ERR_ARG, "model %d: connectivity entry %ld = %d out of range", idx, k, d->conn[k]);
+  if (d->elem_mat)
+    for (int e = 0; e < d->n_elems; e++)
+      if (d->elem_mat[e] < 0 || d->elem_mat[e] >= d->n_materials)
+        return fail(nullptr, DNL_ERR_ARG, "model %d: material index of element %d out of range", idx, e);
+  for (int f = 0; f < d->n_functions; f++)
+    if (d->functions[f].n_points < 1 || !d->functions[f].x || !d->functions[f].y)
+      return fail(nullptr, DNL_ERR_ARG, "model %d: empty function %d", idx, f);
+  if (d->bc_code && d->bc_func)
+    for (long k = 0; k < 3L * d->n_nodes; k++)
+      if (d->bc_func[k] >= d->n_functions)
+        return fail(nullptr, DNL_ERR_ARG, "model %d: function index out of range", idx);
+  if (!(d->t_end > d->t_start))
+    return fail(nullptr, DNL_ERR_ARG, "model %d: t_end must exceed t_start", idx);
+  return DNL_OK;
+}
+
+MatDev make_mat(const dnl_material &m)
+{
+  MatDev d;
+  d.young = m.young;
+  d.poisson = m.poisson;
+  d.rho0 = m.density;
+  d.cp = m.heat_capacity;
+  d.tq = m.taylor_quinney;
+  d.T0 = m.T0;
+  d.A = m.A;
+  d.B = m.B;
+  d.C = m.C;
+  d.n = m.n;
+  d.m = m.m;
+  d.depsp0 = m.depsp0;
+  d.Tm = m.Tm;
+  d.Tref = m.Tref;
+  d.twoG = m.young / (1.0 + m.poisson);                 // Material.h:110-114
+  d.K = m.young / (3.0 * (1.0 - 2.0 * m.poisson));      // Material.h:152-156
+  d.heatFrac = m.taylor_quinney / (m.density * m.heat_capacity); // Material.h:165-169
+  d.wave2 = m.young * (1.0 - m.poisson) / ((1.0 + m.poisson) * (1.0 - 2.0 * m.poisson)); // Element.C:358
+  return d;
+}
+
+// ----------------------------------------------------------------- launches
+
+template <typename R> int launch_element(dnl_engine *h, int mode)
+{
+  const int threads = 128;
+  const int blocks = (int)(((long)h->nE * h->npe + threads - 1) / threads);
+  if (h->npe == 8)
+  {
+    if (mode == 0)
+      k_element<R, 8, 0><<<blocks, threads, 0, h->stream>>>(h->M);
+    else
+      k_element<R, 8, 1><<<blocks, threads, 0, h->stream>>>(h->M);
+  }
+  else
+  {
+    if (mode == 0)
+      k_element<R, 4, 0><<<blocks, threads, 0, h->stream>>>(h->M);
+    else
+      k_element<R, 4, 1><<<blocks, threads, 0, h->stream>>>(h->M);
+  }
+  h->launches++;
+  return DNL_OK;
+}
+
+int launch_element_any(dnl_engine *h, int mode)
+{
+  return h->precision == DNL_PREC_MIXED ? launch_element<float>(h, mode) : launch_element<double>(h, mode);
+}
+
+int launch_nodal(dnl_engine *h)
+{
+  const int threads = 256, blocks = (h->nN + threads - 1) / threads;
+  if (h->precision == DNL_PREC_MIXED)
+  {
+    if (h->dim == 3)
+      k_nodal<float, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+    else
+      k_nodal<float, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+  }
+  else
+  {
+    if (h->dim == 3)
+      k_nodal<double, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+    else
+      k_nodal<double, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+  }
+  h->launches++;
+  return DNL_OK;
+}
+
+int launch_courant(dnl_engine *h, int force)
+{
+  const int threads = 256, blocks = (h->nE + threads - 1) / threads;
+  if (h->precision == DNL_PREC_MIXED)
+  {
+    if (h->npe == 8)
+      k_courant<float, 8><<<blocks, threads, 0, h->stream>>>(h->M, force);
+    else
+      k_courant<float, 4><<<blocks, threads, 0, h->stream>>>(h->M, force);
+  }
+  else
+  {
+    if (h->npe == 8)
+      k_courant<double, 8><<<blocks, threads, 0, h->stream>>>(h->M, force);
+    else
+      k_courant<double, 4><<<blocks, threads, 0, h->stream>>>(h->M, force);
+  }
+  h->launches++;
+  return DNL_OK;
+}
+
+int launch_gather(dnl_engine *h, int what)
+{
+  const int threads = 256, blocks = (h->nN + threads - 1) / threads;
+  if (h->precision == DNL_PREC_MIXED)
+    k_gather<float><<<blocks, threads, 0, h->stream>>>(h->M, what);
+  else
+    k_gather<double><<<blocks, threads, 0, h->stream>>>(h->M, what);
+  h->launches++;
+  return DNL_OK;
+}
+
+int launch_control(dnl_engine *h, int phase, double t_stop = 0.0, long long max_incs = 0)
+{
+  const int threads = 128, blocks = (h->nInst + threads - 1) / threads;
+  k_control<<<blocks, threads, 0, h->stream>>>(h->M, phase, t_stop, max_incs);
+  h->launches++;
+  return DNL_OK;
+}
+
+int launch_bc_prep(dnl_engine *h)
+{
+  if (!h->hasSpeed)
+    return DNL_OK;
+  const int threads = 128, blocks = (h->nSpeed + threads - 1) / threads;
+  k_bc_prep<<<blocks, threads, 0, h->stream>>>(h->M);
+  h->launches++;
+  return DNL_OK;
+}
+
+// One increment: the kernels of the graph.
+int enqueue_step(dnl_engine *h)
+{
+  launch_bc_prep(h);
+  launch_element_any(h, 0);
+  launch_nodal(h);
+  launch_courant(h, 0);
+  launch_control(h, CTL_FINISH);
+  return DNL_OK;
+}
+
+int build_graph(dnl_engine *h)
+{
+  if (h->graphExec)
+    return DNL_OK;
+  long long before = h->launches;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(h);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+  if (e != cudaSuccess)
+    return fail(h, DNL_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  CK(cudaGraphInstantiate(&h->graphExec, h->graph, 0));
+  h->launchesPerStep = (int)(h->launches - before);
+  h->launches = before;
+  return DNL_OK;
+}
+
+int sync_ctl(dnl_engine *h)
+{
+  CK(cudaMemcpyAsync(h->hctl, h->M.ctl, sizeof(Ctl) * h->nInst, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DNL_OK;
+}
+
+int check_status(dnl_engine *h)
+{
+  for (int i = 0; i < h->nInst; i++)
+    if (h->hctl[i].status != 0)
+    {
+      const char *what = h->hctl[i].status == DNL_ERR_NEG_JACOBIAN ? "negative Jacobian in element"
+                                                                   : "radial return did not converge at point";
+      return fail(h, h->hctl[i].status, "instance %d: %s %d (time %.6e)", i, what, h->hctl[i].bad, h->hctl[i].t);
+    }
+  return DNL_OK;
+}
+
+} // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+int dnl_device_count(void)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+const char *dnl_engine_last_error(const dnl_engine *h) { return h ? h->err.c_str() : g_create_err; }
+
+int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_engine **out)
+{
+  if (!out || !descs || n <= 0)
+    return fail(nullptr, DNL_ERR_ARG, "invalid arguments");
+  *out = nullptr;
+  for (int i = 0; i < n; i++)
+  {
+    int rc = check_desc(descs[i], i);
+    if (rc)
+      return rc;
+    if (descs[i]->elem_type != descs[0]->elem_type || descs[i]->precision != descs[0]->precision)
+      return fail(nullptr, DNL_ERR_ARG, "all models of a batch share the element type and precision");
+  }
+  if (dnl_device_count() == 0)
+    return fail(nullptr, DNL_ERR_NO_DEVICE, "no CUDA device visible");
+
+  dnl_engine *h = new dnl_engine;
+  cudaGetDevice(&h->device);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  {
+    delete h;
+    return fail(nullptr, DNL_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  h->type = descs[0]->elem_type;
+  h->npe = npe_of(h->type);
+  h->dim = h->npe == 8 ? 3 : 2;
+  h->precision = descs[0]->precision;
+  h->nInst = n;
+
+  // ---- concatenate the instances
+  std::vector<double4> x, v;
+  std::vector<int> conn, emat;
+  std::vector<MatDev> mats;
+  std::vector<uint8_t> bc;
+  std::vector<double4> bcval;
+  std::vector<int4> bcfun;
+  std::vector<int> speedNodes;
+  std::vector<double> fx, fy;
+  std::vector<int> foff(1, 0);
+  h->elemBegin.assign(1, 0);
+  h->nodeBegin.assign(1, 0);
+  for (int i = 0; i < n; i++)
+  {
+    const dnl_model_desc *d = descs[i];
+    const int nb = (int)x.size(), eb = (int)(conn.size() / h->npe), mb = (int)mats.size(), fb = (int)foff.size() - 1;
+    for (int k = 0; k < d->n_nodes; k++)
+    {
+      x.push_back(make_double4(d->coords[3 * k], d->coords[3 * k + 1], d->coords[3 * k + 2], 0.0));
+      if (d->v_init)
+        v.push_back(make_double4(d->v_init[3 * k], d->v_init[3 * k + 1], d->v_init[3 * k + 2], 0.0));
+      else
+        v.push_back(make_double4(0, 0, 0, 0));
+      uint8_t code = 0;
+      double4 sv = make_double4(0, 0, 0, 0);
+      int4 sf = make_int4(-1, -1, -1, -1);
+      bool speed = false;
+      if (d->bc_code)
+        for (int c = 0; c < 3; c++)
+        {
+          int cc = d->bc_code[3 * k + c];
+          double val = d->bc_value ? d->bc_value[3 * k + c] : 0.0;
+          int fn = d->bc_func ? d->bc_func[3 * k + c] : -1;
+          if (cc == DNL_BC_SPEED && val == 0.0)
+            cc = DNL_BC_RESTRAIN; // an imposed zero speed restrains the component
+          if (cc == DNL_BC_SPEED)
+          {
+            speed = true;
+            comp(sv, c) = val;
+            (c == 0 ? sf.x : (c == 1 ? sf.y : sf.z)) = fn >= 0 ? fn + fb : -1;
+          }
+          if (cc == DNL_BC_RESTRAIN || cc == DNL_BC_SPEED)
+            code |= (uint8_t)(cc << (2 * c));
+        }
+      bc.push_back(code);
+      bcval.push_back(sv);
+      bcfun.push_back(sf);
+      if (speed)
+        speedNodes.push_back(nb + k);
+    }
+    for (long k = 0; k < (long)d->n_elems * h->npe; k++)
+      conn.push_back(d->conn[k] + nb);
+    for (int e = 0; e < d->n_elems; e++)
+      emat.push_back(mb + (d->elem_mat ? d->elem_mat[e] : 0));
+    for (int m = 0; m < d->n_materials; m++)
+      mats.push_back(make_mat(d->materials[m]));
+    for (int f = 0; f < d->n_functions; f++)
+    {
+      for (int p = 0; p < d->functions[f].n_points; p++)
+      {
+        fx.push_back(d->functions[f].x[p]);
+        fy.push_back(d->functions[f].y[p]);
+      }
+      foff.push_back((int)fx.size());
+    }
+    h->elemBegin.push_back(eb + d->n_elems);
+    h->nodeBegin.push_back(nb + d->n_nodes);
+
+    Ctl c;
+    memset(&c, 0, sizeof(c));
+    double rb = (d->rho_b >= 0.0 && d->rho_b <= 1.0) ? d->rho_b : 0.8182;
+    // Chung-Hulbert parameters (Explicit.C:86-104)
+    c.alphaM = (2.0 * rb - 1.0) / (1.0 + rb);
+    c.beta = (5.0 - 3.0 * rb) / ((1.0 + rb) * (1.0 + rb) * (2.0 - rb));
+    c.gammaN = 1.5 - c.alphaM;
+    c.omegaS = sqrt((12.0 * pow(1.0 + rb, 3) * (2.0 - rb)) / (10.0 + 15.0 * rb - rb * rb + pow(rb, 3) - pow(rb, 4)));
+    c.safety = d->ts_safety > 0 ? d->ts_safety : 0.9;
+    c.ts_freq = d->ts_freq > 0 ? d->ts_freq : 10;
+    c.ts_method = d->ts_method;
+    c.t = d->t_start;
+    c.t_end = d->t_end;
+    c.t_stop = d->t_end;
+    c.min_bits = INF_BITS;
+    c.inc_stop = 0x7fffffffffffffffll;
+    c.elem_begin = eb;
+    c.elem_end = eb + d->n_elems;
+    c.node_begin = nb;
+    c.node_end = nb + d->n_nodes;
+    h->ctlInit.push_back(c);
+  }
+  h->nN = (int)x.size();
+  h->nE = (int)(conn.size() / h->npe);
+  h->nIP = h->nE * h->npe;
+  h->nIPpad = (h->nIP + 31) / 32 * 32;
+  h->nSpeed = (int)speedNodes.size();
+  h->hasSpeed = h->nSpeed > 0;
+  h->nFunc = (int)foff.size() - 1;
+  if (fx.empty())
+  {
+    fx.push_back(0.0);
+    fy.push_back(0.0);
+  }
+
+  // ---- node -> (element, local node) slots, in element order
+  std::vector<int> off(h->nN + 1, 0), idx((size_t)h->nIP);
+  for (size_t k = 0; k < conn.size(); k++)
+    off[conn[k] + 1]++;
+  for (int i = 0; i < h->nN; i++)
+    off[i + 1] += off[i];
+  {
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (size_t k = 0; k < conn.size(); k++)
+      idx[fill[conn[k]]++] = (int)k;
+  }
+
+  int rc = DNL_OK;
+  DevModel &M = h->M;
+  M.nInst = h->nInst;
+  M.nN = h->nN;
+  M.nE = h->nE;
+  M.nIP = h->nIP;
+  M.nIPpad = h->nIPpad;
+  M.nSpeed = h->nSpeed;
+  M.nFunc = h->nFunc;
+  const size_t rsz = h->precision == DNL_PREC_MIXED ? 4 : 8;
+  int *d_eb = nullptr, *d_nb = nullptr, *d_conn = nullptr, *d_emat = nullptr, *d_off = nullptr, *d_idx = nullptr;
+  int *d_speed = nullptr, *d_foff = nullptr;
+  MatDev *d_mat = nullptr;
+  uint8_t *d_bc = nullptr;
+  double4 *d_bcval = nullptr;
+  int4 *d_bcfun = nullptr;
+  double *d_fx = nullptr, *d_fy = nullptr;
+  std::vector<double4> zeros4(h->nN, make_double4(0, 0, 0, 0));
+  if ((rc = upload(h, &d_eb, h->elemBegin)) || (rc = upload(h, &d_nb, h->nodeBegin)) ||
+      (rc = upload(h, &d_conn, conn)) || (rc = upload(h, &d_emat, emat)) || (rc = upload(h, &d_mat, mats)) ||
+      (rc = upload(h, &d_off, off)) || (rc = upload(h, &d_idx, idx)) || (rc = upload(h, &d_bc, bc)) ||
+      (rc = upload(h, &d_bcval, bcval)) || (rc = upload(h, &d_bcfun, bcfun)) ||
+      (rc = upload(h, &d_speed, speedNodes)) || (rc = upload(h, &d_fx, fx)) || (rc = upload(h, &d_fy, fy)) ||
+      (rc = upload(h, &d_foff, foff)) || (rc = upload(h, &M.x, x)) || (rc = upload(h, &M.disp, zeros4)) ||
+      (rc = upload(h, &M.u[0], zeros4)) || (rc = upload(h, &M.u[1], zeros4)) || (rc = upload(h, &M.v[0], v)) ||
+      (rc = upload(h, &M.v[1], v)) || (rc = upload(h, &M.a[0], zeros4)) || (rc = upload(h, &M.a[1], zeros4)) ||
+      (rc = dalloc(h, &M.mass, h->nN)) || (rc = dalloc(h, &M.fout, h->nN)) ||
+      (rc = upload(h, &M.ctl, h->ctlInit)) || (rc = dalloc(h, &h->denergy, 3 * h->nInst)))
+  {
+    std::string e = h->err;
+    dnl_engine_destroy(h);
+    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+    return rc;
+  }
+  void *ip = nullptr, *slot = nullptr;
+  if ((rc = dalloc(h, (char **)&ip, (size_t)DNL_IP_NCOMP * h->nIPpad * rsz)) ||
+      (rc = dalloc(h, (char **)&slot, (size_t)h->nIP * 4 * rsz)))
+  {
+    std::string e = h->err;
+    dnl_engine_destroy(h);
+    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+    return rc;
+  }
+  M.inst_elem_begin = d_eb;
+  M.inst_node_begin = d_nb;
+  M.conn = d_conn;
+  M.emat = d_emat;
+  M.mat = d_mat;
+  M.csr_off = d_off;
+  M.csr_idx = d_idx;
+  M.bc = d_bc;
+  M.bcval = d_bcval;
+  M.bcfun = d_bcfun;
+  M.speed_nodes = d_speed;
+  M.fx = d_fx;
+  M.fy = d_fy;
+  M.foff = d_foff;
+  M.ip = ip;
+  M.slot = slot;
+  if (cudaMallocHost((void **)&h->hctl, sizeof(Ctl) * h->nInst) != cudaSuccess)
+  {
+    dnl_engine_destroy(h);
+    return fail(nullptr, DNL_ERR_CUDA, "cudaMallocHost failed");
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+  {
+    dnl_engine_destroy(h);
+    return fail(nullptr, DNL_ERR_CUDA, "upload failed");
+  }
+  *out = h;
+  return DNL_OK;
+}
+
+int dnl_engine_create(const dnl_model_desc *desc, dnl_engine **out)
+{
+  const dnl_model_desc *d[1] = {desc};
+  return dnl_engine_batch_create(d, 1, out);
+}
+
+int dnl_engine_destroy(dnl_engine *h)
+{
+  if (!h)
+    return DNL_OK;
+  if (h->stream)
+    cudaStreamSynchronize(h->stream);
+  if (h->graphExec)
+    cudaGraphExecDestroy(h->graphExec);
+  if (h->graph)
+    cudaGraphDestroy(h->graph);
+  for (void *p : h->allocs)
+    cudaFree(p);
+  if (h->hctl)
+    cudaFreeHost(h->hctl);
+  if (h->stream)
+    cudaStreamDestroy(h->stream);
+  delete h;
+  return DNL_OK;
+}
+
+int dnl_engine_init(dnl_engine *h)
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  // reference Jacobian, initial point state, element masses -> nodal lumped mass
+  launch_element_any(h, 1);
+  launch_gather(h, 0);
+  // Solver::computeTimeStep(true) (Explicit.C:156-158)
+  launch_courant(h, 1);
+  launch_control(h, CTL_INIT_DT);
+  // first element pass at t_start (Explicit.C:161-181)
+  launch_element_any(h, 0);
+  launch_control(h, CTL_POST_INIT);
+  CK(cudaGetLastError());
+  int rc = sync_ctl(h);
+  if (rc)
+    return rc;
+  rc = check_status(h);
+  if (rc)
+    return rc;
+  h->initialized = true;
+  return DNL_OK;
+}
+
+int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *incs_done)
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  if (!h->initialized)
+    return fail(h, DNL_ERR_ARG, "dnl_engine_init must be called first");
+  int rc = build_graph(h);
+  if (rc)
+    return rc;
+  std::vector<long long> inc0(h->nInst);
+  if ((rc = sync_ctl(h)))
+    return rc;
+  for (int i = 0; i < h->nInst; i++)
+    inc0[i] = h->hctl[i].inc - ((h->hctl[i].prepared && h->hctl[i].active) ? 1 : 0);
+  h->launches = 0;
+  cudaEvent_t ev0, ev1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  // reset the FP32 re-solve counters
+  for (int i = 0; i < h->nInst; i++)
+    CK(cudaMemsetAsync(&h->M.ctl[i].resolves, 0, sizeof(int), h->stream));
+  CK(cudaEventRecord(ev0, h->stream));
+  launch_control(h, CTL_LIMITS, t_pause, max_incs);
+  if (h->timing)
+  {
+    // kernel-by-kernel with events: per-phase device time
+    cudaEvent_t e[4];
+    for (int k = 0; k < 4; k++)
+      CK(cudaEventCreate(&e[k]));
+    float acc[3] = {0, 0, 0};
+    long long steps = 0;
+    for (;;)
+    {
+      const int chunk = 16;
+      for (int s = 0; s < chunk; s++)
+      {
+        launch_bc_prep(h);
+        CK(cudaEventRecord(e[0], h->stream));
+        launch_element_any(h, 0);
+        CK(cudaEventRecord(e[1], h->stream));
+        launch_nodal(h);
+        CK(cudaEventRecord(e[2], h->stream));
+        launch_courant(h, 0);
+        launch_control(h, CTL_FINISH);
+        CK(cudaEventRecord(e[3], h->stream));
+        CK(cudaEventSynchronize(e[3]));
+        float t01, t12, t23;
+        cudaEventElapsedTime(&t01, e[0], e[1]);
+        cudaEventElapsedTime(&t12, e[1], e[2]);
+        cudaEventElapsedTime(&t23, e[2], e[3]);
+        acc[0] += t01;
+        acc[1] += t12;
+        acc[2] += t23;
+        steps++;
+        if (max_incs > 0 && steps >= max_incs)
+          break;
+      }
+      if ((rc = sync_ctl(h)))
+        return rc;
+      bool any = false;
+      for (int i = 0; i < h->nInst; i++)
+        any = any || h->hctl[i].active;
+      if (!any || (max_incs > 0 && steps >= max_incs))
+        break;
+    }
+    for (int k = 0; k < 4; k++)
+      cudaEventDestroy(e[k]);
+    h->times[0] = acc[0];
+    h->times[1] = acc[1];
+    h->times[2] = acc[2];
+  }
+  else if (max_incs > 0)
+  {
+    // known number of increments: replay the graph without polling
+    for (int64_t s = 0; s < max_incs; s++)
+    {
+      CK(cudaGraphLaunch(h->graphExec, h->stream));
+      h->launches += h->launchesPerStep;
+    }
+  }
+  else
+  {
+    const int chunk = 64;
+    for (;;)
+    {
+      for (int s = 0; s < chunk; s++)
+      {
+        CK(cudaGraphLaunch(h->graphExec, h->stream));
+        h->launches += h->launchesPerStep;
+      }
+      if ((rc = sync_ctl(h)))
+        return rc;
+      bool any = false, bad = false;
+      for (int i = 0; i < h->nInst; i++)
+      {
+        any = any || h->hctl[i].active;
+        bad = bad || h->hctl[i].status;
+      }
+      if (!any || bad)
+        break;
+    }
+  }
+  CK(cudaEventRecord(ev1, h->stream));
+  CK(cudaEventSynchronize(ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  h->times[3] = ms;
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  CK(cudaGetLastError());
+  if ((rc = sync_ctl(h)))
+    return rc;
+  if (incs_done)
+  {
+    long long mx = 0;
+    for (int i = 0; i < h->nInst; i++)
+    {
+      long long now = h->hctl[i].inc - ((h->hctl[i].prepared && h->hctl[i].active) ? 1 : 0);
+      mx = std::max(mx, now - inc0[i]);
+    }
+    *incs_done = mx;
+  }
+  return check_status(h);
+}
+
+int dnl_engine_element_pass(dnl_engine *h, double time_step)
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  if (!h->initialized)
+    return fail(h, DNL_ERR_ARG, "dnl_engine_init must be called first");
+  if (!(time_step > 0))
+    return fail(h, DNL_ERR_ARG, "time step must be positive");
+  // arm instance 0 with the given time step, run the element pass and assemble
+  int rc = sync_ctl(h);
+  if (rc)
+    return rc;
+  Ctl c = h->hctl[0];
+  c.active = 1;
+  c.prepared = 0;
+  c.due = 0;
+  c.dt_eff = time_step;
+  c.t_new = c.t + time_step;
+  for (int i = 1; i < h->nInst; i++)
+  {
+    Ctl ci = h->hctl[i];
+    ci.active = 0;
+    ci.prepared = 0;
+    CK(cudaMemcpyAsync(&h->M.ctl[i], &ci, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(cudaMemcpyAsync(&h->M.ctl[0], &c, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+  launch_element_any(h, 0);
+  launch_gather(h, 1);
+  launch_control(h, CTL_POST_INIT);
+  CK(cudaGetLastError());
+  if ((rc = sync_ctl(h)))
+    return rc;
+  return check_status(h);
+}
+
+int dnl_engine_sizes(const dnl_engine *h, int32_t *ni, int32_t *nn, int32_t *ne, int32_t *nip)
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  if (ni) *ni = h->nInst;
+  if (nn) *nn = h->nN;
+  if (ne) *ne = h->nE;
+  if (nip) *nip = h->nIP;
+  return DNL_OK;
+}
+
+int dnl_engine_instance_offsets(const dnl_engine *h, int32_t i, int32_t *node0, int32_t *elem0, int32_t *ip0)
+{
+  if (!h || i < 0 || i > h->nInst)
+    return DNL_ERR_ARG;
+  if (node0) *node0 = h->nodeBegin[i];
+  if (elem0) *elem0 = h->elemBegin[i];
+  if (ip0) *ip0 = h->elemBegin[i] * h->npe;
+  return DNL_OK;
+}
+
+int dnl_engine_control(const dnl_engine *h, int32_t i, dnl_control *out)
+{
+  if (!h || !out || i < 0 || i >= h->nInst)
+    return DNL_ERR_ARG;
+  dnl_engine *hh = const_cast<dnl_engine *>(h);
+  int rc = sync_ctl(hh);
+  if (rc)
+    return rc;
+  const Ctl &c = h->hctl[i];
+  out->time = c.t;
+  out->time_step = (c.prepared && c.active) ? c.dt_eff : c.dt;
+  out->t_end = c.t_end;
+  out->increment = c.inc - ((c.prepared && c.active) ? 1 : 0);
+  out->status = c.status;
+  out->bad_index = c.bad;
+  out->done = c.t >= c.t_end;
+  out->fp64_resolves = c.resolves;
+  return DNL_OK;
+}
+
+int dnl_engine_get_nodes(dnl_engine *h, int32_t field, double *out)
+{
+  if (!h || !out)
+    return DNL_ERR_ARG;
+  int rc = sync_ctl(h);
+  if (rc)
+    return rc;
+  const int f0 = h->hctl[0].f0; // node fields of all instances share the parity only for one instance
+  std::vector<double4> tmp(h->nN);
+  std::vector<double> m;
+  auto fetch = [&](const double4 *src) -> int {
+    CK(cudaMemcpyAsync(tmp.data(), src, sizeof(double4) * h->nN, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DNL_OK;
+  };
+  if (field == DNL_NODE_MASS)
+  {
+    m.resize(h->nN);
+    CK(cudaMemcpyAsync(m.data(), h->M.mass, sizeof(double) * h->nN, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < h->nN; i++)
+      out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = m[i];
+    return DNL_OK;
+  }
+  // per-instance parity of the ping-pong nodal buffers
+  std::vector<double4> alt;
+  const double4 *src = nullptr, *srcAlt = nullptr;
+  switch (field)
+  {
+  case DNL_NODE_COORDS: src = h->M.x; break;
+  case DNL_NODE_DISP: src = h->M.disp; break;
+  case DNL_NODE_U: src = h->M.u[f0]; srcAlt = h->M.u[1 - f0]; break;
+  case DNL_NODE_SPEED: src = h->M.v[f0]; srcAlt = h->M.v[1 - f0]; break;
+  case DNL_NODE_ACCEL: src = h->M.a[f0]; srcAlt = h->M.a[1 - f0]; break;
+  case DNL_NODE_SPEED_PREV: src = h->M.v[1 - f0]; srcAlt = h->M.v[f0]; break;
+  case DNL_NODE_FORCE: src = h->M.fout; break;
+  default: return fail(h, DNL_ERR_ARG, "unknown nodal field %d", field);
+  }
+  if ((rc = fetch(src)))
+    return rc;
+  if (srcAlt && h->nInst > 1)
+  {
+    alt.resize(h->nN);
+    CK(cudaMemcpyAsync(alt.data(), srcAlt, sizeof(double4) * h->nN, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int i = 1; i < h->nInst; i++)
+      if (h->hctl[i].f0 != f0)
+        for (int k = h->nodeBegin[i]; k < h->nodeBegin[i + 1]; k++)
+          tmp[k] = alt[k];
+  }
+  for (int i = 0; i < h->nN; i++)
+  {
+    out[3 * i] = tmp[i].x;
+    out[3 * i + 1] = tmp[i].y;
+    out[3 * i + 2] = tmp[i].z;
+  }
+  return DNL_OK;
+}
+
+int dnl_engine_set_nodes(dnl_engine *h, int32_t field, const double *in)
+{
+  if (!h || !in)
+    return DNL_ERR_ARG;
+  int rc = sync_ctl(h);
+  if (rc)
+    return rc;
+  std::vector<double4> tmp(h->nN);
+  for (int i = 0; i < h->nN; i++)
+    tmp[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0);
+  if (field == DNL_NODE_U || field == DNL_NODE_SPEED || field == DNL_NODE_ACCEL)
+  {
+    double4 **arr = field == DNL_NODE_U ? h->M.u : (field == DNL_NODE_SPEED ? h->M.v : h->M.a);
+    // write into each instance's field0 buffer
+    std::vector<double4> cur[2];
+    for (int b = 0; b < 2; b++)
+    {
+      cur[b].resize(h->nN);
+      { int rc_ = copy(h, cur[b].data(), arr[b], sizeof(double4) * h->nN, cudaMemcpyDeviceToHost); if (rc_) return rc_; }
+    }
+    for (int i = 0; i < h->nInst; i++)
+      for (int k = h->nodeBegin[i]; k < h->nodeBegin[i + 1]; k++)
+        cur[h->hctl[i].f0][k] = tmp[k];
+    for (int b = 0; b < 2; b++)
+      { int rc_ = copy(h, arr[b], cur[b].data(), sizeof(double4) * h->nN, cudaMemcpyHostToDevice); if (rc_) return rc_; }
+    return DNL_OK;
+  }
+  double4 *dst = nullptr;
+  switch (field)
+  {
+  case DNL_NODE_COORDS: dst = h->M.x; break;
+  case DNL_NODE_DISP: dst = h->M.disp; break;
+  default: return fail(h, DNL_ERR_ARG, "nodal field %d cannot be written", field);
+  }
+  { int rc_ = copy(h, dst, tmp.data(), sizeof(double4) * h->nN, cudaMemcpyHostToDevice); if (rc_) return rc_; }
+  return DNL_OK;
+}
+
+int dnl_engine_get_ips(dnl_engine *h, double *out)
+{
+  if (!h || !out)
+    return DNL_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t n = (size_t)h->nIP;
+  if (h->precision == DNL_PREC_MIXED)
+  {
+    std::vector<float> tmp((size_t)DNL_IP_NCOMP * h->nIPpad);
+    { int rc_ = copy(h, tmp.data(), h->M.ip, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost); if (rc_) return rc_; }
+    for (int c = 0; c < DNL_IP_NCOMP; c++)
+      for (size_t q = 0; q < n; q++)
+        out[c * n + q] = tmp[(size_t)c * h->nIPpad + q];
+  }
+  else
+  {
+    for (int c = 0; c < DNL_IP_NCOMP; c++)
+      { int rc_ = copy(h, out + c * n, (double *)h->M.ip + (size_t)c * h->nIPpad, n * sizeof(double),
+                    cudaMemcpyDeviceToHost); if (rc_) return rc_; }
+  }
+  return DNL_OK;
+}
+
+int dnl_engine_set_ips(dnl_engine *h, const double *in)
+{
+  if (!h || !in)
+    return DNL_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t n = (size_t)h->nIP;
+  if (h->precision == DNL_PREC_MIXED)
+  {
+    std::vector<float> tmp((size_t)DNL_IP_NCOMP * h->nIPpad, 0.0f);
+    for (int c = 0; c < DNL_IP_NCOMP; c++)
+      for (size_t q = 0; q < n; q++)
+        tmp[(size_t)c * h->nIPpad + q] = (float)in[c * n + q];
+    { int rc_ = copy(h, h->M.ip, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice); if (rc_) return rc_; }
+  }
+  else
+  {
+    for (int c = 0; c < DNL_IP_NCOMP; c++)
+      { int rc_ = copy(h, (double *)h->M.ip + (size_t)c * h->nIPpad, in + c * n, n * sizeof(double),
+                    cudaMemcpyHostToDevice); if (rc_) return rc_; }
+  }
+  return DNL_OK;
+}
+
+int dnl_engine_energies(dnl_engine *h, int32_t i, double out[3])
+{
+  if (!h || !out || i < 0 || i >= h->nInst)
+    return DNL_ERR_ARG;
+  if (h->precision == DNL_PREC_MIXED)
+  {
+    if (h->npe == 8)
+      k_energies<float, 8><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+    else
+      k_energies<float, 4><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+  }
+  else
+  {
+    if (h->npe == 8)
+      k_energies<double, 8><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+    else
+      k_energies<double, 4><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, h->denergy + 3 * i, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DNL_OK;
+}
+
+int dnl_engine_set_timing(dnl_engine *h, int32_t on)
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  h->timing = on != 0;
+  return DNL_OK;
+}
+
+int dnl_engine_timings(const dnl_engine *h, double out[4])
+{
+  if (!h || !out)
+    return DNL_ERR_ARG;
+  for (int k = 0; k < 4; k++)
+    out[k] = h->times[k];
+  return DNL_OK;
+}
+
+int64_t dnl_engine_launch_count(const dnl_engine *h) { return h ? h->launches : 0; }
+
+} // extern "C"

@@ -1,0 +1,116 @@
+"""Python handle over the C ABI of ``libdnlgpu.so`` (include/dnlgpu.h).
+
+`Engine` owns one engine handle: one model, or a batch of independent models
+advanced together.  There is no CPU path: construction raises
+:class:`~dnlPython._abi.EngineUnavailable` when the library or a CUDA device is
+missing.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+
+def _pd(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Engine:
+    def __init__(self, descs):
+        lib = _abi.load_library()
+        if lib.dnl_device_count() <= 0:
+            raise _abi.EngineUnavailable("no CUDA device is visible to the engine")
+        if isinstance(descs, _abi.ModelDesc):
+            descs = [descs]
+        self.descs = list(descs)
+        self._cs = [d.cstruct() for d in self.descs]
+        arr = (ctypes.POINTER(_abi.ModelDescC) * len(self._cs))(*[ctypes.pointer(c) for c in self._cs])
+        h = ctypes.c_void_p()
+        rc = lib.dnl_engine_batch_create(arr, len(self._cs), ctypes.byref(h))
+        if rc != 0:
+            raise _abi.EngineError(rc, lib.dnl_engine_last_error(None).decode())
+        self._lib = lib
+        self.h = h
+        ni, nn, ne, nip = (ctypes.c_int32() for _ in range(4))
+        lib.dnl_engine_sizes(h, ctypes.byref(ni), ctypes.byref(nn), ctypes.byref(ne), ctypes.byref(nip))
+        self.n_instances, self.n_nodes, self.n_elems, self.n_ips = ni.value, nn.value, ne.value, nip.value
+
+    def _check(self, rc):
+        if rc != 0:
+            raise _abi.EngineError(rc, self._lib.dnl_engine_last_error(self.h).decode())
+
+    def init(self):
+        self._check(self._lib.dnl_engine_init(self.h))
+        return self
+
+    def run(self, t_pause=np.inf, max_incs=0):
+        done = ctypes.c_int64()
+        self._check(self._lib.dnl_engine_run(self.h, float(t_pause), int(max_incs), ctypes.byref(done)))
+        return done.value
+
+    def element_pass(self, dt):
+        self._check(self._lib.dnl_engine_element_pass(self.h, float(dt)))
+
+    def control(self, instance=0):
+        c = _abi.Control()
+        self._check(self._lib.dnl_engine_control(self.h, int(instance), ctypes.byref(c)))
+        return dict(time=c.time, time_step=c.time_step, t_end=c.t_end, increment=c.increment,
+                    status=c.status, bad_index=c.bad_index, done=bool(c.done), fp64_resolves=c.fp64_resolves)
+
+    def offsets(self, instance):
+        n0, e0, q0 = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._lib.dnl_engine_instance_offsets(self.h, int(instance), ctypes.byref(n0),
+                                                          ctypes.byref(e0), ctypes.byref(q0)))
+        return n0.value, e0.value, q0.value
+
+    def nodes(self, field):
+        out = np.zeros((self.n_nodes, 3))
+        self._check(self._lib.dnl_engine_get_nodes(self.h, int(field), _pd(out)))
+        return out
+
+    def set_nodes(self, field, values):
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(self.n_nodes, 3)
+        self._check(self._lib.dnl_engine_set_nodes(self.h, int(field), _pd(a)))
+
+    def ips(self):
+        out = np.zeros((_abi.IP_NCOMP, self.n_ips))
+        self._check(self._lib.dnl_engine_get_ips(self.h, _pd(out)))
+        return out
+
+    def set_ips(self, values):
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(_abi.IP_NCOMP, self.n_ips)
+        self._check(self._lib.dnl_engine_set_ips(self.h, _pd(a)))
+
+    def energies(self, instance=0):
+        out = np.zeros(3)
+        self._check(self._lib.dnl_engine_energies(self.h, int(instance), _pd(out)))
+        return out
+
+    def set_timing(self, on=True):
+        self._check(self._lib.dnl_engine_set_timing(self.h, int(bool(on))))
+
+    def timings(self):
+        out = np.zeros(4)
+        self._check(self._lib.dnl_engine_timings(self.h, _pd(out)))
+        return dict(element_ms=out[0], nodal_ms=out[1], timestep_ms=out[2], run_ms=out[3])
+
+    def launch_count(self):
+        return int(self._lib.dnl_engine_launch_count(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.dnl_engine_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

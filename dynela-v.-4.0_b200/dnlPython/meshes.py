@@ -1,0 +1,182 @@
+"""Mesh and model generators for the workloads the engine is measured on.
+
+Units follow the DynELA samples: mm, s, tonne, MPa (Samples/Taylor/Taylor-Axi/Taylor.py:22-34).
+Every generator returns a :class:`~dnlPython._abi.ModelDesc`; node and element
+numbers are 0-based and ordered so that consecutive elements share nodes
+(layer by layer along the bar axis), which keeps the nodal gathers local.
+"""
+import numpy as np
+
+from . import _abi
+
+# Copper (Taylor impact of the measured workloads): rho 8930 kg/m3, E 124 GPa,
+# nu 0.34, Johnson-Cook A 90 MPa, B 292 MPa, n 0.31, C 0.025, eps0_dot 1/s,
+# m 1.09, T0 298 K, Tm 1356 K, Cp 383 J/kgK, Taylor-Quinney 0.9.
+COPPER = _abi.material(young=124000.0, poisson=0.34, density=8.93e-9, heat_capacity=3.83e8,
+                       taylor_quinney=0.9, T0=298.0, A=90.0, B=292.0, C=0.025, n=0.31, m=1.09,
+                       depsp0=1.0, Tm=1356.0, Tref=298.0)
+
+# 42CrMo4 steel of the DynELA Taylor and necking samples (Taylor-Axi/Taylor.py:22-34).
+STEEL_42CRMO4 = _abi.material(young=206000.0, poisson=0.3, density=7.83e-9, heat_capacity=4.6e8,
+                              taylor_quinney=0.9, T0=20.0, A=806.0, B=614.0, C=0.0089, n=0.168, m=1.1,
+                              depsp0=1.0, Tm=1540.0, Tref=20.0)
+
+# Steel of the bar/plate necking workloads: rho 7800 kg/m3, E 206.9 GPa, nu 0.29,
+# Johnson-Cook A 806, B 614, n 0.168, C 0.0089, m 1.1, Tm 1540 K, Cp 477 J/kgK.
+STEEL_NECKING = _abi.material(young=206900.0, poisson=0.29, density=7.8e-9, heat_capacity=4.77e8,
+                              taylor_quinney=0.9, T0=20.0, A=806.0, B=614.0, C=0.0089, n=0.168, m=1.1,
+                              depsp0=1.0, Tm=1540.0, Tref=20.0)
+
+
+def taylor_axi(nr=10, nz=80, radius=3.2, length=32.4, speed=227000.0, mat=COPPER, t_end=80e-6,
+               ts_method=_abi.TS_COURANT, ts_freq=10, precision=_abi.PREC_FP64):
+    """Axisymmetric Taylor bar of nr x nz ElQua4NAx elements, numbered as in
+    Samples/Taylor/Taylor-Axi/Taylor.py:43-66 (rows of nr+1 nodes from the impact
+    face up).  Impact face restrained axially, axis restrained radially,
+    initial speed -speed along y."""
+    dx, dy = radius / nr, length / nz
+    j, i = np.meshgrid(np.arange(nz + 1), np.arange(nr + 1), indexing="ij")
+    coords = np.zeros(((nr + 1) * (nz + 1), 3))
+    coords[:, 0] = (i * dx).ravel()
+    coords[:, 1] = (j * dy).ravel()
+    jj, ii = np.meshgrid(np.arange(nz), np.arange(nr), indexing="ij")
+    n1 = (ii + jj * (nr + 1)).ravel()
+    conn = np.stack([n1, n1 + 1, n1 + nr + 2, n1 + nr + 1], axis=1)
+    nN = coords.shape[0]
+    bc = np.zeros((nN, 3), np.int8)
+    bottom = coords[:, 1] == 0.0
+    axis = coords[:, 0] == 0.0
+    bc[bottom, 1] = _abi.BC_RESTRAIN
+    bc[axis, 0] = _abi.BC_RESTRAIN
+    v = np.zeros((nN, 3))
+    v[:, 1] = -speed
+    return _abi.ModelDesc(_abi.ELQUA4NAX, coords, conn, [mat], v_init=v, bc_code=bc, t_end=t_end,
+                          ts_method=ts_method, ts_freq=ts_freq, precision=precision)
+
+
+def _fix_hex_orientation(coords, conn):
+    """Reverse the top/bottom faces of elements whose reference Jacobian is negative."""
+    x = coords[conn]  # (nE, 8, 3)
+    d1 = (x[:, 1] + x[:, 2] + x[:, 6] + x[:, 5]) - (x[:, 0] + x[:, 3] + x[:, 7] + x[:, 4])
+    d2 = (x[:, 3] + x[:, 2] + x[:, 6] + x[:, 7]) - (x[:, 0] + x[:, 1] + x[:, 5] + x[:, 4])
+    d3 = (x[:, 4] + x[:, 5] + x[:, 6] + x[:, 7]) - (x[:, 0] + x[:, 1] + x[:, 2] + x[:, 3])
+    det = np.einsum("ij,ij->i", d1, np.cross(d2, d3))
+    bad = det < 0
+    conn = conn.copy()
+    conn[bad] = conn[bad][:, [4, 5, 6, 7, 0, 1, 2, 3]]
+    return conn
+
+
+def _extrude(points2d, quads, nlayers, length, axis_offsets=None):
+    """Extrude a cross-section in the (x, z) plane along y into hex8 elements."""
+    nq = points2d.shape[0]
+    ys = np.linspace(0.0, length, nlayers + 1) if axis_offsets is None else axis_offsets
+    coords = np.zeros(((nlayers + 1) * nq, 3))
+    for k, y in enumerate(ys):
+        coords[k * nq:(k + 1) * nq, 0] = points2d[:, 0]
+        coords[k * nq:(k + 1) * nq, 1] = y
+        coords[k * nq:(k + 1) * nq, 2] = points2d[:, 1]
+    conn = []
+    for k in range(nlayers):
+        b = quads + k * nq
+        t = quads + (k + 1) * nq
+        conn.append(np.concatenate([b, t], axis=1))
+    conn = np.concatenate(conn, axis=0)
+    return coords, _fix_hex_orientation(coords, conn)
+
+
+def ogrid_section(radius, n_core, n_ring, core_frac=0.45):
+    """O-grid disc: an n_core x n_core square core of half-width core_frac*radius
+    and a ring of 4*n_core x n_ring quads blending the square's perimeter into
+    the circle."""
+    c = core_frac * radius  # half-width of the square core
+    s = np.linspace(-c, c, n_core + 1)
+    gx, gz = np.meshgrid(s, s, indexing="ij")
+    core = np.stack([gx.ravel(), gz.ravel()], axis=1)
+    idx = np.arange((n_core + 1) ** 2).reshape(n_core + 1, n_core + 1)
+    quads = []
+    for a in range(n_core):
+        for b in range(n_core):
+            quads.append([idx[a, b], idx[a + 1, b], idx[a + 1, b + 1], idx[a, b + 1]])
+    # perimeter of the core, counter-clockwise, starting at corner (-c, -c)
+    per = []
+    n = n_core
+    per += [idx[a, 0] for a in range(0, n)]          # bottom edge, x increasing
+    per += [idx[n, b] for b in range(0, n)]          # right edge, z increasing
+    per += [idx[a, n] for a in range(n, 0, -1)]      # top edge, x decreasing
+    per += [idx[0, b] for b in range(n, 0, -1)]      # left edge, z decreasing
+    per = np.array(per)
+    nper = per.shape[0]
+    theta = -0.75 * np.pi + 2.0 * np.pi * np.arange(nper) / nper
+    circle = radius * np.stack([np.cos(theta), np.sin(theta)], axis=1)
+    pts = [core]
+    layer_ids = [per]
+    nxt = core.shape[0]
+    for l in range(1, n_ring + 1):
+        t = l / n_ring
+        p = (1.0 - t) * core[per] + t * circle
+        pts.append(p)
+        layer_ids.append(np.arange(nxt, nxt + nper))
+        nxt += nper
+    for l in range(n_ring):
+        a, b = layer_ids[l], layer_ids[l + 1]
+        for k in range(nper):
+            k1 = (k + 1) % nper
+            quads.append([a[k], a[k1], b[k1], b[k]])
+    return np.concatenate(pts, axis=0), np.array(quads, dtype=np.int64)
+
+
+def taylor_3d(n_core=12, n_ring=17, n_axial=160, radius=3.2, length=32.4, speed=227000.0, mat=COPPER,
+              t_end=80e-6, ts_method=_abi.TS_COURANT, ts_freq=10, precision=_abi.PREC_MIXED):
+    """Full 3-D Taylor bar on ElHex8N3D: an O-grid cross-section of
+    n_core^2 + 4*n_core*n_ring quads extruded in n_axial layers along y.
+    Defaults give 960 x 160 = 153,600 elements.  Impact face (y = 0) restrained
+    along y, initial speed -speed along y."""
+    pts, quads = ogrid_section(radius, n_core, n_ring)
+    coords, conn = _extrude(pts, quads, n_axial, length)
+    nN = coords.shape[0]
+    bc = np.zeros((nN, 3), np.int8)
+    bc[coords[:, 1] == 0.0, 1] = _abi.BC_RESTRAIN
+    v = np.zeros((nN, 3))
+    v[:, 1] = -speed
+    return _abi.ModelDesc(_abi.ELHEX8N3D, coords, conn, [mat], v_init=v, bc_code=bc, t_end=t_end,
+                          ts_method=ts_method, ts_freq=ts_freq, precision=precision)
+
+
+def hex_block(nx, ny, nz, size=(1.0, 1.0, 1.0), mat=COPPER, t_end=1e-6, speed=0.0, seed=None,
+              distort=0.0, precision=_abi.PREC_FP64, ts_freq=10):
+    """Structured block of nx*ny*nz ElHex8N3D (test fixture).  With a seed, the
+    interior nodes are jittered by `distort` x the cell size and the initial
+    speed field is random with magnitude ~speed."""
+    xs = np.linspace(0, size[0], nx + 1)
+    ys = np.linspace(0, size[1], ny + 1)
+    zs = np.linspace(0, size[2], nz + 1)
+    gx, gy, gz = np.meshgrid(xs, ys, zs, indexing="ij")
+    coords = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+    idx = np.arange(coords.shape[0]).reshape(nx + 1, ny + 1, nz + 1)
+    conn = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                conn.append([idx[i, j, k], idx[i + 1, j, k], idx[i + 1, j + 1, k], idx[i, j + 1, k],
+                             idx[i, j, k + 1], idx[i + 1, j, k + 1], idx[i + 1, j + 1, k + 1], idx[i, j + 1, k + 1]])
+    conn = np.array(conn)
+    rng = np.random.default_rng(seed)
+    if seed is not None and distort > 0:
+        h = min(size[0] / nx, size[1] / ny, size[2] / nz)
+        coords = coords + distort * h * rng.uniform(-1, 1, coords.shape)
+    v = np.zeros_like(coords)
+    if speed:
+        if seed is None:
+            v[:, 1] = -speed
+        else:
+            v = speed * rng.uniform(-1, 1, coords.shape)
+    bc = np.zeros(coords.shape, np.int8)
+    bc[coords[:, 1] <= 1e-12, 1] = _abi.BC_RESTRAIN
+    conn = _fix_hex_orientation(coords, conn)
+    return _abi.ModelDesc(_abi.ELHEX8N3D, coords, conn, [mat], v_init=v, bc_code=bc, t_end=t_end,
+                          precision=precision, ts_freq=ts_freq)
+
+
+def nodes_per_element_ratio(desc):
+    return desc.n_nodes / desc.n_elems

@@ -1,0 +1,216 @@
+/*
+ * dnlgpu.h - C ABI of the B200 explicit-dynamics engine for DynELA models.
+ *
+ * The engine replaces everything below DynELA's `Explicit::solve` for one
+ * increment (Sources/dnlFEM/Explicit.C:126-411) and the one-time set-up done by
+ * `Model::initSolve` + the pre-loop part of `Explicit::solve`
+ * (Sources/dnlFEM/Model.C:360-521, Explicit.C:143-181).  The host side that
+ * mirrors DynELA's Python model API (`dnlPython`) fills a `dnl_model_desc`
+ * from the script's nodes, elements, material, boundary conditions and solver
+ * settings, and drives the engine through the entry points below.
+ *
+ * Conventions
+ *  - plain pointers and sizes only; the caller owns every host array passed in
+ *    and may free it as soon as the call returns;
+ *  - every entry point returns an int status: 0 (DNL_OK) or a negative
+ *    DNL_ERR_* code; the library never calls exit();
+ *  - one host thread per handle, one CUDA stream per handle (created by the
+ *    engine on the device that is current when dnl_engine_create is called).
+ */
+#ifndef DNLGPU_H
+#define DNLGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Element families on the path (Sources/dnlElements/Element.h type enum). */
+enum {
+  DNL_ELQUA4NAX = 1, /* 4-node axisymmetric quad, 4 Gauss points (ElQua4NAx.C:21-240) */
+  DNL_ELHEX8N3D = 2  /* 8-node hexahedron, 8 Gauss points (ElHex8N3D.C:25-535) */
+};
+
+/* Critical time step method (Solver.h Courant / PowerIteration). */
+enum { DNL_TS_COURANT = 0, DNL_TS_POWER_ITERATION = 1 };
+
+/* Arithmetic of the element pass: FP64 everywhere, or FP32 element math and
+ * per-point state with FP64 coordinates, displacements, time and energy sums. */
+enum { DNL_PREC_FP64 = 0, DNL_PREC_MIXED = 1 };
+
+/* Constant boundary condition on one node component (BoundaryRestrain.C:98-128,
+ * BoundarySpeed.C:139-206); the last condition attached to a component wins. */
+enum { DNL_BC_FREE = 0, DNL_BC_RESTRAIN = 1, DNL_BC_SPEED = 2 };
+
+/* Status codes. */
+enum {
+  DNL_OK = 0,
+  DNL_ERR_ARG = -1,            /* invalid argument or size */
+  DNL_ERR_CUDA = -2,           /* a CUDA call failed (see dnl_engine_last_error) */
+  DNL_ERR_NEG_JACOBIAN = -3,   /* detJ < 0 (ElementPlane.C:75-79, Element3D.C:88-92) */
+  DNL_ERR_NEWTON = -4,         /* radial return did not converge (Element.C:560-582) */
+  DNL_ERR_POWER_ITERATION = -5,/* power iteration did not converge (Model.C:1002-1005) */
+  DNL_ERR_UNSUPPORTED = -6,    /* option not available on this path */
+  DNL_ERR_NO_DEVICE = -7       /* no CUDA device / library built without one */
+};
+
+/* Per integration point state, component-major: comp*n_ips + ip.
+ * Symmetric tensors are stored xx, xy, xz, yy, yz, zz (SymTensor2 _data). */
+enum {
+  DNL_IP_STRESS = 0,          /* 6 */
+  DNL_IP_STRAIN = 6,          /* 6 */
+  DNL_IP_PLASTIC_STRAIN = 12, /* 6 */
+  DNL_IP_EPSP = 18,           /* equivalent plastic strain */
+  DNL_IP_DEPSP = 19,          /* equivalent plastic strain rate */
+  DNL_IP_GAMMA = 20,          /* last plastic multiplier */
+  DNL_IP_GAMMA_CUM = 21,      /* cumulated plastic multiplier */
+  DNL_IP_YIELD = 22,          /* current yield stress */
+  DNL_IP_T = 23,              /* temperature */
+  DNL_IP_PRESSURE = 24,
+  DNL_IP_EINT = 25,           /* specific internal energy */
+  DNL_IP_EINEL = 26,          /* specific inelastic energy */
+  DNL_IP_DENSITY = 27,
+  DNL_IP_DETJ0 = 28,          /* reference detJ (times radius for axisymmetric) */
+  DNL_IP_NCOMP = 29
+};
+
+/* Nodal fields, each [n_nodes*3] doubles (x, y, z per node). */
+enum {
+  DNL_NODE_COORDS = 0,
+  DNL_NODE_DISP = 1,
+  DNL_NODE_U = 2,      /* displacement increment of the last increment (field0->u) */
+  DNL_NODE_SPEED = 3,  /* field0->speed */
+  DNL_NODE_ACCEL = 4,  /* field0->acceleration */
+  DNL_NODE_MASS = 5,   /* lumped mass, repeated on the 3 components */
+  DNL_NODE_FORCE = 6,  /* assembled internal force of the last element pass */
+  DNL_NODE_SPEED_PREV = 7 /* field1->speed: the speed before the last increment */
+};
+
+/* Johnson-Cook elasto-plastic material (Material.h:26-100 + JohnsonCookLaw.C:132-143). */
+typedef struct dnl_material {
+  double young, poisson, density, heat_capacity, taylor_quinney, T0;
+  double A, B, C, n, m, depsp0, Tm, Tref; /* Johnson-Cook A, B, C, n, m, eps0_dot, Tm, T0 */
+} dnl_material;
+
+/* Piecewise-linear time function (DiscreteFunction.C:188-213); x strictly increasing. */
+typedef struct dnl_function {
+  int32_t n_points;
+  const double *x;
+  const double *y;
+} dnl_function;
+
+/* One model (one simulation instance). */
+typedef struct dnl_model_desc {
+  int32_t elem_type;           /* DNL_ELQUA4NAX or DNL_ELHEX8N3D */
+  int32_t n_nodes;
+  int32_t n_elems;
+  const double *coords;        /* [n_nodes*3] */
+  const int32_t *conn;         /* [n_elems*nodes_per_element], 0-based node indices */
+  const int32_t *elem_mat;     /* [n_elems] material index, or NULL (all 0) */
+  int32_t n_materials;
+  const dnl_material *materials;
+  const double *v_init;        /* [n_nodes*3] initial speed (BoundarySpeed::applyInitial), or NULL */
+  const int8_t *bc_code;       /* [n_nodes*3] DNL_BC_*, or NULL (all free) */
+  const double *bc_value;      /* [n_nodes*3] imposed speed for DNL_BC_SPEED, or NULL */
+  const int32_t *bc_func;      /* [n_nodes*3] function index scaling bc_value, -1 none, or NULL */
+  int32_t n_functions;
+  const dnl_function *functions;
+  double t_start, t_end;       /* Solver::setTimes */
+  int32_t ts_method;           /* DNL_TS_* */
+  int32_t ts_freq;             /* Solver::setComputeTimeStepFrequency (default 10) */
+  double ts_safety;            /* Solver::setTimeStepSafetyFactor (default 0.9) */
+  double rho_b;                /* Explicit::setDissipation (default 0.8182) */
+  int32_t precision;           /* DNL_PREC_* */
+  int32_t reserved;
+} dnl_model_desc;
+
+/* Solver state of one instance. */
+typedef struct dnl_control {
+  double time;        /* Model::currentTime */
+  double time_step;   /* Solver::timeStep (after the clip to the end time) */
+  double t_end;
+  int64_t increment;  /* Solver::currentIncrement */
+  int32_t status;     /* DNL_OK or DNL_ERR_* raised on the device */
+  int32_t bad_index;  /* element (negative detJ) or integration point (Newton) that failed */
+  int32_t done;       /* time >= t_end */
+  int32_t fp64_resolves; /* mixed path: points re-solved in FP64 during the last run call */
+} dnl_control;
+
+typedef struct dnl_engine dnl_engine;
+
+/* Returns the number of CUDA devices visible (0 when none), never fails. */
+int dnl_device_count(void);
+
+/* Create an engine for one model.  Uploads the description to the current
+ * device.  Replaces DynELA::initSolve -> Model::initSolve (Model.C:360-521)
+ * data layout set-up. */
+int dnl_engine_create(const dnl_model_desc *desc, dnl_engine **out);
+
+/* Create one engine that advances n independent models together (batched
+ * mode): one element pass, one nodal pass and one time-step pass per step for
+ * all of them, each with its own time, time step and material. */
+int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_engine **out);
+
+int dnl_engine_destroy(dnl_engine *h);
+
+/* Text of the last error raised on this handle (or the last create error when h is NULL). */
+const char *dnl_engine_last_error(const dnl_engine *h);
+
+/* One-time start of the solve: reference Jacobian, lumped mass, first time
+ * step, first element pass (Explicit.C:143-181 + Model::computeMassMatrix,
+ * Model.C:537-592). */
+int dnl_engine_init(dnl_engine *h);
+
+/* Advance every unfinished instance until its time reaches min(t_pause, t_end)
+ * or max_incs increments have been run in this call (max_incs <= 0: no limit).
+ * Replaces the increment loop of Explicit::solve (Explicit.C:184-256).
+ * *incs_done (may be NULL) receives the largest number of increments run by
+ * one instance in this call. */
+int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *incs_done);
+
+/* Kernel-level entry point: one element pass (strains, pressure, radial
+ * return, final rotation, internal forces and their assembly; Explicit.C:204-226)
+ * on the current state with the given time step, without the nodal update.
+ * Instance 0 only. */
+int dnl_engine_element_pass(dnl_engine *h, double time_step);
+
+/* Number of instances, nodes, elements and integration points (all instances). */
+int dnl_engine_sizes(const dnl_engine *h, int32_t *n_instances, int32_t *n_nodes,
+                     int32_t *n_elems, int32_t *n_ips);
+
+/* First node / element / integration point of instance i in the concatenated arrays. */
+int dnl_engine_instance_offsets(const dnl_engine *h, int32_t i, int32_t *node0,
+                                int32_t *elem0, int32_t *ip0);
+
+int dnl_engine_control(const dnl_engine *h, int32_t instance, dnl_control *out);
+
+/* Copy one nodal field (DNL_NODE_*) of all instances to host memory [n_nodes*3]. */
+int dnl_engine_get_nodes(dnl_engine *h, int32_t field, double *out);
+/* Overwrite one nodal field (coords, disp, u, speed, accel) from host memory. */
+int dnl_engine_set_nodes(dnl_engine *h, int32_t field, const double *in);
+
+/* Copy / overwrite the integration-point state, [DNL_IP_NCOMP * n_ips] doubles
+ * component-major (converted from/to FP32 on the mixed path). */
+int dnl_engine_get_ips(dnl_engine *h, double *out);
+int dnl_engine_set_ips(dnl_engine *h, const double *in);
+
+/* Energies of one instance, FP64 sums: [0] kinetic (Model.C:612-626, field0
+ * speeds), [1] internal = sum rho0*detJ0*w*e_int (x 2 pi for axisymmetric),
+ * [2] inelastic (plastic work), same weights. */
+int dnl_engine_energies(dnl_engine *h, int32_t instance, double out[3]);
+
+/* Device-side time of the kernels of the last dnl_engine_run call, in ms:
+ * [0] element pass, [1] nodal pass, [2] time-step pass, [3] whole run. Only
+ * filled when timing was enabled with dnl_engine_set_timing(h, 1). */
+int dnl_engine_set_timing(dnl_engine *h, int32_t on);
+int dnl_engine_timings(const dnl_engine *h, double out[4]);
+
+/* Number of kernel launches issued on the device by the last run call. */
+int64_t dnl_engine_launch_count(const dnl_engine *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DNLGPU_H */

@@ -1,0 +1,148 @@
+"""Shared helpers of the test suite: model descriptions, seeded random states,
+fixture (de)serialisation and comparison utilities."""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "dynela-v.-4.0_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+for p in (PKG, ORACLE):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from dnlPython import _abi, meshes  # noqa: E402
+
+# tolerance stated for the element pass (internal forces and returned stresses)
+# of the FP64 path against the FP64 oracle: 1e-6 relative
+FP64_PASS_RTOL = 1e-6
+# mixed path (FP32 element math and point state) against the FP64 oracle on one pass
+MIXED_PASS_RTOL = 2e-4
+
+
+def desc_to_npz(desc, prefix=""):
+    out = {}
+    out[prefix + "elem_type"] = np.array(desc.elem_type)
+    out[prefix + "coords"] = desc.coords
+    out[prefix + "conn"] = desc.conn
+    keys = [f[0] for f in _abi.Material._fields_]
+    out[prefix + "materials"] = np.array([[m[k] for k in keys] for m in desc.materials])
+    for name in ("elem_mat", "v_init", "bc_code", "bc_value", "bc_func"):
+        a = getattr(desc, name)
+        if a is not None:
+            out[prefix + name] = a
+    if desc.functions:
+        out[prefix + "func_x"] = np.concatenate([f[0] for f in desc.functions])
+        out[prefix + "func_y"] = np.concatenate([f[1] for f in desc.functions])
+        out[prefix + "func_n"] = np.array([len(f[0]) for f in desc.functions])
+    out[prefix + "solver"] = np.array([desc.t_start, desc.t_end, desc.ts_method, desc.ts_freq, desc.ts_safety,
+                                       desc.rho_b, desc.precision])
+    return out
+
+
+def desc_from_npz(z, prefix="", precision=None):
+    keys = [f[0] for f in _abi.Material._fields_]
+    mats = [dict(zip(keys, row)) for row in z[prefix + "materials"]]
+    funcs = []
+    if prefix + "func_n" in z:
+        x, y, off = z[prefix + "func_x"], z[prefix + "func_y"], 0
+        for n in z[prefix + "func_n"]:
+            funcs.append((x[off:off + n], y[off:off + n]))
+            off += n
+    s = z[prefix + "solver"]
+    opt = {k: z[prefix + k] for k in ("elem_mat", "v_init", "bc_code", "bc_value", "bc_func") if prefix + k in z}
+    return _abi.ModelDesc(int(z[prefix + "elem_type"]), z[prefix + "coords"], z[prefix + "conn"], mats,
+                          functions=funcs, t_start=s[0], t_end=s[1], ts_method=int(s[2]), ts_freq=int(s[3]),
+                          ts_safety=s[4], rho_b=s[5],
+                          precision=int(s[6]) if precision is None else precision, **opt)
+
+
+def random_point_state(desc, ips, seed, stress_scale=200.0):
+    """A seeded, physically plausible integration-point state on top of the
+    initial one (keeps detJ0 and density): stresses around the yield stress,
+    a mix of virgin and plastified points."""
+    rng = np.random.default_rng(seed)
+    n = desc.n_ips
+    s = ips.copy()
+    mat = desc.materials[0]
+    s[0:6] = rng.normal(0.0, stress_scale, (6, n))
+    if desc.elem_type == _abi.ELQUA4NAX:
+        s[2] = s[4] = 0.0
+    s[6:12] = rng.normal(0.0, 0.05, (6, n))
+    s[12:18] = rng.normal(0.0, 0.03, (6, n))
+    if desc.elem_type == _abi.ELQUA4NAX:
+        s[8] = s[10] = s[14] = s[16] = 0.0
+    plastic = rng.uniform(size=n) < 0.7
+    epsp = np.where(plastic, rng.uniform(0.0, 0.6, n), 0.0)
+    s[_abi.IP_EPSP] = epsp
+    s[_abi.IP_DEPSP] = np.where(plastic, rng.uniform(0.0, 2e4, n), 0.0)
+    s[_abi.IP_GAMMA] = np.where(plastic, rng.uniform(1e-6, 5e-4, n), 0.0)
+    s[_abi.IP_GAMMA_CUM] = np.where(plastic, epsp * 1.2247, 0.0)
+    s[_abi.IP_YIELD] = np.where(plastic, mat["A"] + mat["B"] * np.power(np.maximum(epsp, 1e-12), mat["n"]), 0.0)
+    s[_abi.IP_T] = mat["T0"] + rng.uniform(0.0, 250.0, n)
+    s[_abi.IP_PRESSURE] = 0.0
+    s[_abi.IP_EINT] = rng.uniform(0.0, 1e5, n)
+    s[_abi.IP_EINEL] = rng.uniform(0.0, 1e5, n)
+    return s
+
+
+def random_increment(desc, seed, strain=2e-3):
+    """Seeded displacement increment (field0->u) giving strain increments ~strain."""
+    rng = np.random.default_rng(seed)
+    x = desc.coords
+    h = (x.max(0) - x.min(0)).max() / max(desc.n_elems ** (1.0 / (2 if desc.elem_type == _abi.ELQUA4NAX else 3)), 1)
+    u = strain * h * rng.normal(size=(desc.n_nodes, 3))
+    u += rng.normal(size=3) * 1e-3  # rigid translation part
+    if desc.elem_type == _abi.ELQUA4NAX:
+        u[:, 2] = 0.0
+    return u
+
+
+def rel_err(a, b, axis=None):
+    """max |a - b| / max |b| (per row when axis=1)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if axis is None:
+        return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max(axis=axis) / np.maximum(np.abs(b).max(axis=axis), 1e-300)
+
+
+def field_errors(ga, gb):
+    """Relative error of each point-state component: tensor components are
+    scaled by the largest component of their tensor (stress, strain, plastic
+    strain), scalars by their own largest value."""
+    ga, gb = np.asarray(ga), np.asarray(gb)
+    err = np.abs(ga - gb).max(axis=1)
+    scale = np.abs(gb).max(axis=1)
+    for b in (0, 6, 12):
+        scale[b:b + 6] = scale[b:b + 6].max()
+    return err / np.maximum(scale, 1e-300)
+
+
+# model cases shared by the golden fixtures and the parity tests
+def case_axi_small(precision=_abi.PREC_FP64):
+    return meshes.taylor_axi(nr=5, nz=20, radius=3.2, length=8.1, speed=227000.0, t_end=4e-6, ts_freq=1,
+                             precision=precision)
+
+
+def case_hex_small(precision=_abi.PREC_FP64):
+    return meshes.hex_block(3, 4, 3, size=(0.9, 1.2, 0.9), speed=60000.0, seed=11, distort=0.12, t_end=5e-6,
+                            precision=precision, ts_freq=3)
+
+
+def case_hex_speed(precision=_abi.PREC_FP64):
+    """Hex block pulled at its top face by an imposed speed ramped by a
+    piecewise-linear function, bottom face restrained (necking-like loading)."""
+    d = meshes.hex_block(3, 5, 3, size=(0.9, 1.5, 0.9), mat=meshes.STEEL_NECKING, t_end=4e-6, precision=precision,
+                         ts_freq=2)
+    top = d.coords[:, 1] >= d.coords[:, 1].max() - 1e-12
+    bc = d.bc_code.copy()
+    val = np.zeros_like(d.coords)
+    fun = -np.ones(d.coords.shape, np.int32)
+    bc[top, 1] = _abi.BC_SPEED
+    val[top, 1] = 5000.0
+    fun[top, 1] = 0
+    ramp = (np.array([0.0, 1e-6, 1.0]), np.array([0.0, 1.0, 1.0]))
+    return d.copy(bc_code=bc, bc_value=val, bc_func=fun, functions=[ramp], v_init=np.zeros_like(d.coords))

@@ -1,0 +1,212 @@
+"""Parity of the CUDA engine (through the C ABI) with the oracle and with the
+reference's golden fixtures.
+
+Tolerances: the FP64 path must agree with the FP64 oracle within 1e-6 relative
+on internal forces and returned stresses of one element pass (we assert much
+tighter bounds where the arithmetic allows); the mixed path (FP32 element math
+and point state, FP64 positions/displacements/time/energy sums) is held to
+MIXED_PASS_RTOL on one pass and to 1e-4 on final bar length / radius and 1e-3
+on the maximum equivalent plastic strain of a whole Taylor run."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import helpers
+from helpers import _abi, meshes
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+RUNS = sorted(glob.glob(os.path.join(helpers.GOLDEN, "*_run.npz")))
+PASSES = sorted(glob.glob(os.path.join(helpers.GOLDEN, "*_pass.npz")))
+
+
+def engine(desc):
+    from dnlPython.engine import Engine
+    return Engine(desc)
+
+
+@pytest.mark.parametrize("path", PASSES, ids=[os.path.basename(p) for p in PASSES])
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_element_pass_matches_reference(path, precision):
+    z = np.load(path)
+    desc = helpers.desc_from_npz(z, precision=precision)
+    with engine(desc) as e:
+        e.init()
+        e.set_ips(z["in_ips"])
+        e.set_nodes(_abi.NODE_U, z["in_u"])
+        e.element_pass(float(z["dt"]))
+        errs = helpers.field_errors(e.ips(), z["out_ips"])
+        ferr = helpers.rel_err(e.nodes(_abi.NODE_FORCE), z["out_force"])
+    if precision == _abi.PREC_FP64:
+        assert errs.max() < 1e-9, errs
+        assert ferr < 1e-9
+        assert max(errs[:6].max(), ferr) < helpers.FP64_PASS_RTOL
+    else:
+        assert errs.max() < helpers.MIXED_PASS_RTOL, errs
+        assert ferr < helpers.MIXED_PASS_RTOL
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+@pytest.mark.parametrize("case", ["hex", "axi"])
+def test_element_pass_random_states_vs_oracle(case, seed):
+    desc = helpers.case_hex_small() if case == "hex" else helpers.case_axi_small()
+    with oracle.OracleModel(desc) as o, engine(desc) as e:
+        o.init()
+        e.init()
+        ips = helpers.random_point_state(desc, o.ips(), seed, stress_scale=150.0 * seed)
+        u = helpers.random_increment(desc, seed + 7, strain=1e-3 * seed)
+        dt = 4e-9 * seed
+        for m in (o, e):
+            m.set_ips(ips)
+            m.set_nodes(_abi.NODE_U, u)
+            m.element_pass(dt)
+        assert helpers.field_errors(e.ips(), o.ips()).max() < 1e-9
+        assert helpers.rel_err(e.nodes(_abi.NODE_FORCE), o.nodes(_abi.NODE_FORCE)) < 1e-9
+
+
+@pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
+def test_fp64_runs_match_reference(path):
+    z = np.load(path)
+    desc = helpers.desc_from_npz(z, precision=_abi.PREC_FP64)
+    with engine(desc) as e:
+        e.init()
+        assert helpers.rel_err(e.nodes(_abi.NODE_MASS), z["init_mass"]) < 1e-13
+        assert abs(e.control()["time_step"] - z["init_control"][1]) < 1e-12 * z["init_control"][1]
+        done = 0
+        for k in z["checkpoints"]:
+            n = e.run(max_incs=int(k) - done)
+            assert n == int(k) - done
+            done = int(k)
+            c = e.control()
+            assert c["increment"] == int(z[f"inc{k}_control"][2])
+            assert abs(c["time"] - z[f"inc{k}_control"][0]) <= 1e-12 * z[f"inc{k}_control"][0]
+            assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), z[f"inc{k}_coords"]) < 1e-12
+            assert helpers.rel_err(e.nodes(_abi.NODE_DISP), z[f"inc{k}_disp"]) < 1e-9
+            assert helpers.rel_err(e.nodes(_abi.NODE_SPEED), z[f"inc{k}_speed"]) < 1e-8
+            errs = helpers.field_errors(e.ips(), z[f"inc{k}_ips"])
+            assert errs.max() < 1e-8, errs
+
+
+@pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
+def test_mixed_runs_track_reference(path):
+    z = np.load(path)
+    desc = helpers.desc_from_npz(z, precision=_abi.PREC_MIXED)
+    k = int(z["checkpoints"][-1])
+    with engine(desc) as e:
+        e.init()
+        e.run(max_incs=k)
+        span = np.ptp(z[f"inc{k}_coords"], axis=0).max()
+        assert np.abs(e.nodes(_abi.NODE_COORDS) - z[f"inc{k}_coords"]).max() < 1e-5 * span
+        errs = helpers.field_errors(e.ips(), z[f"inc{k}_ips"])
+        assert errs[:6].max() < 5e-3, errs
+        assert errs[_abi.IP_EPSP] < 1e-3 and errs[_abi.IP_T] < 1e-4
+
+
+def _taylor_summary(desc, m, nr):
+    c = m.nodes(_abi.NODE_COORDS)
+    ip = m.ips()
+    return dict(radius=c[nr, 0], height=c[desc.n_nodes - 1 - nr, 1], epsp=ip[_abi.IP_EPSP].max(),
+                energies=m.energies())
+
+
+@pytest.fixture(scope="module")
+def config0_oracle():
+    """Copper Taylor impact, 10 x 80 ElQua4NAx, 227 m/s, 80 us (Courant, every 10 increments)."""
+    desc = meshes.taylor_axi(precision=_abi.PREC_FP64)
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        n = o.run()
+        return n, _taylor_summary(desc, o, 10), o.nodes(_abi.NODE_COORDS), o.ips()
+
+
+def test_config0_fp64_whole_run(config0_oracle):
+    n_o, s_o, x_o, ip_o = config0_oracle
+    desc = meshes.taylor_axi(precision=_abi.PREC_FP64)
+    with engine(desc) as e:
+        e.init()
+        n = e.run()
+        s = _taylor_summary(desc, e, 10)
+        assert n == n_o and e.control()["done"]
+        assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), x_o) < 1e-9
+        assert helpers.field_errors(e.ips(), ip_o).max() < 1e-6
+        assert abs(s["height"] - s_o["height"]) < 1e-9 * s_o["height"]
+        assert np.allclose(s["energies"], s_o["energies"], rtol=1e-9)
+
+
+def test_config0_mixed_whole_run(config0_oracle):
+    n_o, s_o, x_o, ip_o = config0_oracle
+    desc = meshes.taylor_axi(precision=_abi.PREC_MIXED)
+    with engine(desc) as e:
+        e.init()
+        e.run()
+        s = _taylor_summary(desc, e, 10)
+        c = e.control()
+    assert c["done"]
+    assert abs(s["height"] - s_o["height"]) < 1e-4 * s_o["height"]
+    assert abs(s["radius"] - s_o["radius"]) < 1e-4 * s_o["radius"]
+    assert abs(s["epsp"] - s_o["epsp"]) < 1e-3 * s_o["epsp"]
+    assert np.allclose(s["energies"], s_o["energies"], rtol=1e-3)
+
+
+def test_batched_instances_match_single_runs():
+    descs = [helpers.case_hex_small(), helpers.case_hex_small().copy(t_end=3e-6),
+             meshes.hex_block(2, 3, 2, speed=90000.0, seed=4, distort=0.05, t_end=6e-6)]
+    descs[1].materials[0]["A"] *= 1.1
+    singles = []
+    for d in descs:
+        with engine(d) as e:
+            e.init()
+            e.run()
+            singles.append((e.nodes(_abi.NODE_COORDS), e.ips(), e.control()))
+    with engine(descs) as b:
+        b.init()
+        b.run()
+        X, IP = b.nodes(_abi.NODE_COORDS), b.ips()
+        for i, (x, ip, c) in enumerate(singles):
+            n0, e0, q0 = b.offsets(i)
+            n1, e1, q1 = b.offsets(i + 1) if i + 1 < len(descs) else (b.n_nodes, b.n_elems, b.n_ips)
+            assert np.array_equal(X[n0:n1], x)
+            assert np.array_equal(IP[:, q0:q1], ip)
+            cb = b.control(i)
+            assert cb["increment"] == c["increment"] and cb["time"] == c["time"]
+
+
+def test_runs_are_deterministic():
+    d = helpers.case_hex_small(_abi.PREC_MIXED)
+    out = []
+    for _ in range(2):
+        with engine(d) as e:
+            e.init()
+            e.run(max_incs=40)
+            out.append((e.nodes(_abi.NODE_COORDS), e.ips()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_pause_and_resume_equal_one_run():
+    d = helpers.case_hex_speed()
+    with engine(d) as a, engine(d) as b:
+        a.init()
+        b.init()
+        a.run(max_incs=50)
+        t_half = b.control()["time"] + 20 * b.control()["time_step"]
+        b.run(t_pause=t_half)
+        b.run(max_incs=50 - b.control()["increment"])
+        assert a.control()["increment"] == b.control()["increment"] == 50
+        assert np.array_equal(a.nodes(_abi.NODE_COORDS), b.nodes(_abi.NODE_COORDS))
+
+
+def test_inverted_element_raises_status():
+    d = helpers.case_hex_small()
+    with engine(d) as e:
+        e.init()
+        x = e.nodes(_abi.NODE_COORDS)
+        k = d.conn[0]
+        x[k[6]] = x[k[0]] - (x[k[6]] - x[k[0]])  # fold element 0 through itself
+        e.set_nodes(_abi.NODE_COORDS, x)
+        with pytest.raises(_abi.EngineError) as ei:
+            e.run(max_incs=3)
+        assert ei.value.code == -3
+        assert e.control()["status"] == -3

@@ -1,0 +1,205 @@
+"""The CPU restatement (oracle/dnl_oracle.c) pinned against the reference:
+golden fixtures made by the reference compiled from its own sources
+(tests/golden/make_golden.py), live comparisons when oracle/_ref is built,
+and unit properties of its building blocks."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import helpers
+from helpers import _abi, meshes
+import oracle
+import ref
+
+RUNS = sorted(glob.glob(os.path.join(helpers.GOLDEN, "*_run.npz")))
+PASSES = sorted(glob.glob(os.path.join(helpers.GOLDEN, "*_pass.npz")))
+
+
+@pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
+def test_oracle_matches_reference_runs(path):
+    z = np.load(path)
+    desc = helpers.desc_from_npz(z)
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        assert helpers.rel_err(o.nodes(_abi.NODE_MASS), z["init_mass"]) < 1e-13
+        assert helpers.field_errors(o.ips(), z["init_ips"]).max() < 1e-12
+        done = 0
+        for k in z["checkpoints"]:
+            o.run(max_incs=int(k) - done)
+            done = int(k)
+            c = o.control()
+            assert c["increment"] == int(z[f"inc{k}_control"][2])
+            assert abs(c["time"] - z[f"inc{k}_control"][0]) <= 1e-12 * z[f"inc{k}_control"][0]
+            assert helpers.rel_err(o.nodes(_abi.NODE_COORDS), z[f"inc{k}_coords"]) < 1e-12
+            assert helpers.rel_err(o.nodes(_abi.NODE_SPEED), z[f"inc{k}_speed"]) < 1e-8
+            errs = helpers.field_errors(o.ips(), z[f"inc{k}_ips"])
+            assert errs.max() < 1e-8, errs
+
+
+@pytest.mark.parametrize("path", PASSES, ids=[os.path.basename(p) for p in PASSES])
+def test_oracle_matches_reference_element_pass(path):
+    z = np.load(path)
+    desc = helpers.desc_from_npz(z)
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        o.set_ips(z["in_ips"])
+        o.set_nodes(_abi.NODE_U, z["in_u"])
+        o.element_pass(float(z["dt"]))
+        errs = helpers.field_errors(o.ips(), z["out_ips"])
+        assert errs.max() < 1e-10, errs
+        assert helpers.rel_err(o.nodes(_abi.NODE_FORCE), z["out_force"]) < 1e-10
+
+
+def test_oracle_reproduces_published_taylor_axi():
+    """Samples/Taylor/Taylor-Axi (Documentation/Samples-Impacts.tex:102-110 publishes
+    L_f 26.52 mm, D_f 11.15 mm, eps_p 1.78): the reference gives 26.5293 / 5.5791 /
+    1.7895 with the power-iteration time step; the oracle restates the Courant
+    runs, which must match the reference to rounding."""
+    rows = np.load(os.path.join(helpers.GOLDEN, "taylor_axi_sample.npz"))["rows"]
+    pub = rows[rows[:, 0] == _abi.TS_POWER_ITERATION][0]
+    assert abs(pub[4] - 26.52) < 0.01 and abs(2 * pub[3] - 11.15) < 0.02 and abs(pub[5] - 1.78) < 0.01
+    for row in rows[rows[:, 0] == _abi.TS_COURANT]:
+        d = meshes.taylor_axi(nr=5, nz=50, radius=3.2, length=32.4, speed=287000.0, mat=meshes.STEEL_42CRMO4,
+                              t_end=80e-6, ts_method=_abi.TS_COURANT, ts_freq=int(row[1]))
+        with oracle.OracleModel(d) as o:
+            o.init()
+            n = o.run()
+            c = o.nodes(_abi.NODE_COORDS)
+            ip = o.ips()
+        assert n == int(row[2])
+        assert abs(c[5, 0] - row[3]) < 1e-9 and abs(c[d.n_nodes - 6, 1] - row[4]) < 1e-9
+        assert abs(ip[_abi.IP_EPSP].reshape(-1, 4).mean(1).max() - row[5]) < 1e-9
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_oracle_vs_live_reference_random_pass():
+    for seed, desc in ((21, helpers.case_hex_small()), (22, helpers.case_axi_small())):
+        with ref.RefModel(desc) as r:
+            r.init()
+            ips = helpers.random_point_state(desc, r.ips(), seed, stress_scale=400.0)
+            u = helpers.random_increment(desc, seed + 100, strain=5e-3)
+            r.set_ips(ips)
+            r.set_nodes(_abi.NODE_U, u)
+            r.element_pass(7e-9)
+            ref_ips, ref_f = r.ips(), r.nodes(_abi.NODE_FORCE)
+        with oracle.OracleModel(desc) as o:
+            o.init()
+            o.set_ips(ips)
+            o.set_nodes(_abi.NODE_U, u)
+            o.element_pass(7e-9)
+            assert helpers.field_errors(o.ips(), ref_ips).max() < 1e-9
+            assert helpers.rel_err(o.nodes(_abi.NODE_FORCE), ref_f) < 1e-9
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_oracle_courant_lengths_match_reference():
+    desc = meshes.taylor_3d(n_core=4, n_ring=3, n_axial=6, precision=_abi.PREC_FP64)
+    with ref.RefModel(desc) as r:
+        r.init()
+        lr, wr = r.element_lengths()
+        cr = r.courant()
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        lo, wo = o.element_lengths()
+        assert helpers.rel_err(lo, lr) < 1e-12 and helpers.rel_err(wo, wr) < 1e-14
+        assert abs(o.courant() - cr) < 1e-12 * cr
+
+
+def test_polar_decomposition_properties():
+    rng = np.random.default_rng(3)
+    for k in range(200):
+        F = np.eye(3) + (0.3 if k % 2 else 1e-4) * rng.normal(size=(3, 3))
+        if np.linalg.det(F) <= 0:
+            continue
+        lnU, R = oracle.polar_lnU(F)
+        S = np.array([[lnU[0], lnU[1], lnU[2]], [lnU[1], lnU[3], lnU[4]], [lnU[2], lnU[4], lnU[5]]])
+        w, V = np.linalg.eigh(S)
+        U = V @ np.diag(np.exp(w)) @ V.T
+        assert np.abs(R @ R.T - np.eye(3)).max() < 1e-12
+        assert np.abs(R @ U - F).max() < 1e-12
+        wc, Vc = np.linalg.eigh(F.T @ F)
+        ref_ln = Vc @ np.diag(0.5 * np.log(wc)) @ Vc.T
+        assert np.abs(S - ref_ln).max() < 1e-12
+
+
+def test_eigen_repeated_eigenvalues():
+    lam, vec = oracle.sym_eigen3(np.array([2.0, 0.0, 0.0, 2.0, 0.0, 2.0]))
+    assert np.allclose(lam, 2.0) and np.allclose(vec, np.eye(3))
+    a = np.array([1.0, 1e-9, 0.0, 1.0, 0.0, 3.0])
+    lam, vec = oracle.sym_eigen3(a)
+    A = np.array([[a[0], a[1], a[2]], [a[1], a[3], a[4]], [a[2], a[4], a[5]]])
+    assert np.abs(A @ vec - vec @ np.diag(lam)).max() < 1e-14
+
+
+def test_johnson_cook_law():
+    mat = meshes.COPPER
+    for epsp, depsp, T in ((0.1, 0.5, 298.0), (0.3, 1e4, 500.0), (1e-8, 10.0, 1500.0), (2.0, 3e5, 900.0)):
+        hard = mat["A"] + mat["B"] * epsp ** mat["n"]
+        visc = 1 + mat["C"] * np.log(depsp / mat["depsp0"]) if depsp > mat["depsp0"] else 1.0
+        temp = 1.0
+        if T > mat["Tref"]:
+            temp = 1 - ((T - mat["Tref"]) / (mat["Tm"] - mat["Tref"])) ** mat["m"] if T < mat["Tm"] else 0.0
+        assert abs(oracle.jc_yield(mat, epsp, depsp, T) - hard * visc * temp) < 1e-12 * max(hard, 1)
+        # total derivative (JohnsonCookLaw.C:298-339) against central differences
+        dt = 1e-8
+        y0 = oracle.jc_yield(mat, epsp, depsp, T)
+
+        def cd(f, x, h):
+            return (f(x + h) - f(x - h)) / (2 * h)
+
+        fd_e = cd(lambda e: oracle.jc_yield(mat, e, depsp, T), epsp, 1e-4 * epsp)
+        fd_d = cd(lambda r: oracle.jc_yield(mat, epsp, r, T), depsp, 1e-4 * depsp) / dt \
+            if depsp > mat["depsp0"] * 1.01 else 0.0
+        ana = oracle.jc_hardening(mat, epsp, depsp, T, dt)
+        heat = mat["taylor_quinney"] / (mat["density"] * mat["heat_capacity"])
+        fd_t = 0.0
+        if mat["Tref"] < T < mat["Tm"]:
+            fd_t = cd(lambda t: oracle.jc_yield(mat, epsp, depsp, t), T, 1e-3) * heat * y0
+        assert abs(ana - (fd_e + fd_d + fd_t)) < 1e-4 * max(abs(ana), 1.0)
+
+
+def test_radial_return_consistency():
+    """After the return the von Mises stress sits on the yield surface when
+    plastic, and the plastic work heats the point (Element.C:587-620)."""
+    mat = meshes.COPPER
+    rng = np.random.default_rng(9)
+    for k in range(50):
+        dE = rng.normal(0, 2e-3, 6)
+        st = np.zeros(21)
+        st[0:6] = rng.normal(0, 80.0, 6)
+        st[12] = 0.05 * k / 50
+        st[14] = 1e-4
+        st[16] = mat["A"] + mat["B"] * st[12] ** mat["n"] if st[12] > 0 else 0.0
+        st[17] = 298.0
+        st[18] = (st[0] + st[3] + st[5]) / 3
+        it, out = oracle.radial_return(mat, dE, 1e-8, st)
+        assert it >= 0
+        s = out[0:6].copy()
+        p = (s[0] + s[3] + s[5]) / 3
+        s[[0, 3, 5]] -= p
+        vm = np.sqrt(1.5 * (s[0] ** 2 + s[3] ** 2 + s[5] ** 2 + 2 * (s[1] ** 2 + s[2] ** 2 + s[4] ** 2)))
+        if out[14] != st[14] or out[12] > st[12]:
+            assert abs(vm - out[16]) < 1e-6 * out[16]
+            assert out[17] > st[17]
+        else:
+            assert vm <= out[16] * (1 + 1e-12)
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_reference_bulk_model_building_is_equivalent():
+    """The harness's bulk mesh creation (used for large meshes) builds the same
+    reference model as DynELA::createNode / createElement."""
+    desc = helpers.case_hex_small()
+    out = []
+    for bulk in ("1000000", "1"):
+        os.environ["DNL_REF_BULK_MIN_ELEMS"] = bulk
+        try:
+            with ref.RefModel(desc) as r:
+                r.init()
+                r.run(max_incs=20)
+                out.append((r.nodes(_abi.NODE_COORDS), r.ips()))
+        finally:
+            del os.environ["DNL_REF_BULK_MIN_ELEMS"]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
