@@ -155,53 +155,153 @@ __device__ __forceinline__ void raise_status(Ctl *c, int code, int index)
     c->bad = index;
 }
 
-// FP64 re-solve of a point whose FP32 return failed its tests.
-__device__ __noinline__ bool resolve_fp64(const MatDev &mp, const float dE[6], double dt, ReturnState<float> &st,
-                                          const ReturnState<float> &st0)
+// FP64 re-solve of a point whose FP32 return failed its tests.  The point
+// state is re-read from global memory (it is written back only after the
+// return) and the result comes back by value, so the common path keeps its
+// state in registers.
+struct Resolved
 {
+  float s[6], dep[6];
+  float epsp, depsp, gamma, gcum, yield, T, eint, einel;
+  int ok;
+};
+
+__device__ __noinline__ Resolved resolve_fp64(const float *ip, int nIPpad, int q, const MatDev *matp, float e0,
+                                              float e1, float e2, float e3, float e4, float e5, double dt,
+                                              float pressure)
+{
+  const MatDev &mp = *matp;
   JC<double> jc;
   jc.load(mp);
   ReturnState<double> d;
-#pragma unroll
   for (int c = 0; c < 6; c++)
   {
-    d.s[c] = st0.s[c];
-    d.ep[c] = st0.ep[c];
+    d.s[c] = ip[(size_t)(DNL_IP_STRESS + c) * nIPpad + q];
+    d.ep[c] = 0.0;
   }
-  d.epsp = st0.epsp;
-  d.depsp = st0.depsp;
-  d.gamma = st0.gamma;
-  d.gcum = st0.gcum;
-  d.yield = st0.yield;
-  d.T = st0.T;
-  d.pressure = st0.pressure;
-  d.eint = st0.eint;
-  d.einel = st0.einel;
-  double de[6];
-#pragma unroll
-  for (int c = 0; c < 6; c++)
-    de[c] = dE[c];
+  d.epsp = ip[(size_t)DNL_IP_EPSP * nIPpad + q];
+  d.depsp = ip[(size_t)DNL_IP_DEPSP * nIPpad + q];
+  d.gamma = ip[(size_t)DNL_IP_GAMMA * nIPpad + q];
+  d.gcum = ip[(size_t)DNL_IP_GAMMA_CUM * nIPpad + q];
+  d.yield = ip[(size_t)DNL_IP_YIELD * nIPpad + q];
+  d.T = ip[(size_t)DNL_IP_T * nIPpad + q];
+  d.eint = ip[(size_t)DNL_IP_EINT * nIPpad + q];
+  d.einel = ip[(size_t)DNL_IP_EINEL * nIPpad + q];
+  d.pressure = pressure;
+  const double de[6] = {e0, e1, e2, e3, e4, e5};
   bool ok;
   radial_return<double>(jc, mp.twoG, mp.heatFrac, 1.0 / mp.rho0, de, dt, d, ok);
-#pragma unroll
+  Resolved r;
   for (int c = 0; c < 6; c++)
   {
-    st.s[c] = (float)d.s[c];
-    st.ep[c] = (float)d.ep[c];
+    r.s[c] = (float)d.s[c];
+    r.dep[c] = (float)d.ep[c];
   }
-  st.epsp = (float)d.epsp;
-  st.depsp = (float)d.depsp;
-  st.gamma = (float)d.gamma;
-  st.gcum = (float)d.gcum;
-  st.yield = (float)d.yield;
-  st.T = (float)d.T;
-  st.pressure = (float)d.pressure;
-  st.eint = (float)d.eint;
-  st.einel = (float)d.einel;
-  return ok;
+  r.epsp = (float)d.epsp;
+  r.depsp = (float)d.depsp;
+  r.gamma = (float)d.gamma;
+  r.gcum = (float)d.gcum;
+  r.yield = (float)d.yield;
+  r.T = (float)d.T;
+  r.eint = (float)d.eint;
+  r.einel = (float)d.einel;
+  r.ok = ok;
+  return r;
 }
 
+// Derivatives of the shape functions of node N at the Gauss point with local
+// coordinates (xi0, xi1, xi2) (ElHex8N3D.C:561-632, ElQua4NAx.C:269-297).
+template <typename R, int NPE, int N>
+__device__ __forceinline__ void shape(R xi0, R xi1, R xi2, R dN[3], R &Nv)
+{
+  const R s0 = R(node_sign(N, 0)), s1 = R(node_sign(N, 1)), s2 = R(node_sign(N, 2));
+  if constexpr (NPE == 8)
+  {
+    const R f0 = R(1) + s0 * xi0, f1 = R(1) + s1 * xi1, f2 = R(1) + s2 * xi2;
+    dN[0] = s0 * f1 * f2 * R(0.125);
+    dN[1] = s1 * f0 * f2 * R(0.125);
+    dN[2] = s2 * f0 * f1 * R(0.125);
+    Nv = f0 * f1 * f2 * R(0.125);
+  }
+  else
+  {
+    const R f0 = R(1) + s0 * xi0, f1 = R(1) + s1 * xi1;
+    dN[0] = s0 * f1 * R(0.25);
+    dN[1] = s1 * f0 * R(0.25);
+    dN[2] = R(0);
+    Nv = f0 * f1 * R(0.25);
+  }
+}
+
+template <typename R, int NPE, int N> struct GatherJG
+{
+  static __device__ __forceinline__ void run(unsigned amask, int base, R xi0, R xi1, R xi2, R rx, R ry, R rz, R urx,
+                                             R ury, R urz, R (&J)[3][3], R (&G)[3][3], R &Nr, R &Vr)
+  {
+    constexpr int DIM = (NPE == 8) ? 3 : 2;
+    R dN[3], Nv;
+    shape<R, NPE, N>(xi0, xi1, xi2, dN, Nv);
+    const R xn[3] = {__shfl_sync(amask, rx, base + N), __shfl_sync(amask, ry, base + N),
+                     DIM == 3 ? __shfl_sync(amask, rz, base + N) : R(0)};
+    const R un[3] = {__shfl_sync(amask, urx, base + N), __shfl_sync(amask, ury, base + N),
+                     DIM == 3 ? __shfl_sync(amask, urz, base + N) : R(0)};
+#pragma unroll
+    for (int i = 0; i < DIM; i++)
+#pragma unroll
+      for (int j = 0; j < DIM; j++)
+      {
+        J[i][j] += dN[j] * xn[i];
+        G[i][j] += dN[j] * un[i];
+      }
+    if constexpr (NPE == 4)
+    {
+      Nr += Nv * xn[0];
+      Vr += Nv * un[0];
+    }
+    if constexpr (N + 1 < NPE)
+      GatherJG<R, NPE, N + 1>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
+  }
+};
+
+// Per-(lane, node) element forces written to shared memory for the transpose.
+template <typename R, int NPE, int N> struct ForcesToShared
+{
+  static __device__ __forceinline__ void run(R xi0, R xi1, R xi2, const R (&P)[3][3], R hoop, R *row)
+  {
+    constexpr int DIM = (NPE == 8) ? 3 : 2;
+    R dN[3], Nv;
+    shape<R, NPE, N>(xi0, xi1, xi2, dN, Nv);
+#pragma unroll
+    for (int i = 0; i < DIM; i++)
+    {
+      R s = R(0);
+#pragma unroll
+      for (int k = 0; k < DIM; k++)
+        s += dN[k] * P[k][i];
+      if (NPE == 4 && i == 0)
+        s -= Nv * hoop;
+      row[N * DIM + i] = s;
+    }
+    if constexpr (N + 1 < NPE)
+      ForcesToShared<R, NPE, N + 1>::run(xi0, xi1, xi2, P, hoop, row);
+  }
+};
+
+template <typename R, int NPE, int N> struct MassToShared
+{
+  static __device__ __forceinline__ void run(R xi0, R xi1, R xi2, R scale, R *row)
+  {
+    R dN[3], Nv;
+    shape<R, NPE, N>(xi0, xi1, xi2, dN, Nv);
+    row[N] = scale * Nv;
+    if constexpr (N + 1 < NPE)
+      MassToShared<R, NPE, N + 1>::run(xi0, xi1, xi2, scale, row);
+  }
+};
+
 // ---------------------------------------------------------- element pass
+
+constexpr int ELEM_THREADS = 128;
 
 // One thread per integration point; the NPE points of an element are NPE
 // consecutive lanes, and lane g also loads node g of the element.
@@ -211,12 +311,16 @@ __device__ __noinline__ bool resolve_fp64(const MatDev &mp, const float dE[6], d
 // MODE 1: start of the solve: reference Jacobian detJ0, initial point state
 //         (Element::initializeData, Element.C:258-301) and the element lumped
 //         masses (Element::computeMassMatrix, Element.C:304-339) into the slots.
+// The element's nodal forces are summed over its points through shared memory
+// (each lane writes its NPE x DIM contributions, lane g then adds node g's).
 template <typename R, int NPE, int MODE>
-__global__ void __launch_bounds__(128) k_element(DevModel M)
+__global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_element(DevModel M)
 {
   constexpr int DIM = (NPE == 8) ? 3 : 2;
   constexpr bool AXI = (NPE == 4);
+  constexpr int ROW = NPE * DIM + 1; // padded shared-memory row (bank spread)
   using R4 = typename V4<R>::type;
+  __shared__ R sh[ELEM_THREADS * ROW];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int g = lane & (NPE - 1);
@@ -231,7 +335,8 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
   if (!act)
     return;
   const int f0 = C->f0;
-  const MatDev &mp = M.mat[M.emat[e]];
+  const int mi = M.emat[e];
+  const MatDev &mp = M.mat[mi];
 
   // ---- gather the element's nodes (lane g <- node g)
   const int node = M.conn[q];
@@ -245,7 +350,7 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
   const R rx = R(X.x - x0), ry = R(X.y - y0), rz = R(X.z - z0);
   const R urx = R(U.x - ux0), ury = R(U.y - uy0), urz = R(U.z - uz0);
 
-  // ---- Jacobian J = sum x_n dN_n/dxi and G = sum du_n dN_n/dxi at this Gauss point
+  // ---- J = sum x_n dN_n/dxi and G = sum du_n dN_n/dxi at this Gauss point
   const R a = R(0.57735026918962576451); // 1/sqrt(3)
   const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
   R J[3][3], G[3][3];
@@ -255,48 +360,11 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
     for (int j = 0; j < 3; j++)
       J[i][j] = G[i][j] = R(0);
   R Nr = R(0), Vr = R(0);
-  R dN[NPE][DIM], Nv[NPE];
-#pragma unroll
-  for (int n = 0; n < NPE; n++)
-  {
-    const R s0 = R(node_sign(n, 0)), s1 = R(node_sign(n, 1)), s2 = R(node_sign(n, 2));
-    if constexpr (NPE == 8)
-    {
-      const R f0_ = R(1) + s0 * xi0, f1_ = R(1) + s1 * xi1, f2_ = R(1) + s2 * xi2;
-      dN[n][0] = s0 * f1_ * f2_ / R(8);
-      dN[n][1] = s1 * f0_ * f2_ / R(8);
-      dN[n][2] = s2 * f0_ * f1_ / R(8);
-      Nv[n] = f0_ * f1_ * f2_ / R(8);
-    }
-    else
-    {
-      const R f0_ = R(1) + s0 * xi0, f1_ = R(1) + s1 * xi1;
-      dN[n][0] = s0 * f1_ / R(4);
-      dN[n][1] = s1 * f0_ / R(4);
-      Nv[n] = f0_ * f1_ / R(4);
-    }
-    const R xn[3] = {__shfl_sync(amask, rx, base + n), __shfl_sync(amask, ry, base + n),
-                     DIM == 3 ? __shfl_sync(amask, rz, base + n) : R(0)};
-    const R un[3] = {__shfl_sync(amask, urx, base + n), __shfl_sync(amask, ury, base + n),
-                     DIM == 3 ? __shfl_sync(amask, urz, base + n) : R(0)};
-#pragma unroll
-    for (int i = 0; i < DIM; i++)
-#pragma unroll
-      for (int j = 0; j < DIM; j++)
-      {
-        J[i][j] += dN[n][j] * xn[i];
-        G[i][j] += dN[n][j] * un[i];
-      }
-    if (AXI)
-    {
-      Nr += Nv[n] * xn[0];
-      Vr += Nv[n] * un[0];
-    }
-  }
+  GatherJG<R, NPE, 0>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
   // axisymmetric radius r = sum N_n x_n (ElementAxi.C:46-59) and the radial
   // displacement increment sum N_n du_n (ElementAxi.C:88-99), from the offsets
   R radius = R(1);
-  if (AXI)
+  if constexpr (AXI)
   {
     radius = R(x0 + (double)Nr);
     Vr += R(ux0);
@@ -336,10 +404,11 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
   if (detJ < R(0))
     raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
 
-  const R TWO_PI = R(6.28318530717958647692);
   R WxdJ = detJ; // Gauss weight 1
-  if (AXI)
-    WxdJ *= TWO_PI * radius;
+  if constexpr (AXI)
+    WxdJ *= R(6.28318530717958647692) * radius;
+  R *row = sh + threadIdx.x * ROW;
+  R *grp = sh + (threadIdx.x - g) * ROW;
 
   if constexpr (MODE == 1)
   {
@@ -351,13 +420,14 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
       ipw<R>(M, c, q, R(0));
     ipw<R>(M, DNL_IP_T, q, R(mp.T0));
     ipw<R>(M, DNL_IP_DENSITY, q, rho0);
-    R me[NPE];
+    MassToShared<R, NPE, 0>::run(xi0, xi1, xi2, rho0 * WxdJ, row);
+    __syncwarp(amask);
+    R m = R(0);
 #pragma unroll
-    for (int n = 0; n < NPE; n++)
-      me[n] = rho0 * Nv[n] * WxdJ;
-    reduce_scatter<R, NPE, 1>(amask, g, me);
+    for (int l = 0; l < NPE; l++)
+      m += grp[l * ROW + g];
     R4 s;
-    s.x = me[0];
+    s.x = m;
     s.y = s.z = s.w = R(0);
     reinterpret_cast<R4 *>(M.slot)[q] = s;
     return;
@@ -365,35 +435,47 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
 
   const double dt = C->dt_eff;
   // ---- F - I = G J^-1 (+ axisymmetric hoop term), polar decomposition
-  R H[9];
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-    {
-      R s = R(0);
-#pragma unroll
-      for (int k = 0; k < DIM; k++)
-        s += G[i][k] * inv[k][j];
-      H[3 * i + j] = (i < DIM && j < DIM) ? s : R(0);
-    }
-  if (AXI)
-    H[8] = Vr / radius;
   R dE[6], Rot[9];
-  polar_lnU<R>(H, dE, Rot);
+  {
+    R H[9];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+      {
+        R s = R(0);
+#pragma unroll
+        for (int k = 0; k < DIM; k++)
+          s += G[i][k] * inv[k][j];
+        H[3 * i + j] = (i < DIM && j < DIM) ? s : R(0);
+      }
+    if constexpr (AXI)
+      H[8] = Vr / radius;
+    polar_lnU<R>(H, dE, Rot);
+  }
 
   // ---- element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
   const R trSum = group_sum<NPE>(amask, dE[0] + dE[3] + dE[5]);
 
-  // ---- point state
+  // ---- total strain: Strain += dE, then the final rotation (Element.C:1116-1161)
+  {
+    R strain[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      strain[c] = ipv<R>(M, DNL_IP_STRAIN + c, q) + dE[c];
+    rotate_sym<R>(Rot, strain);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      ipw<R>(M, DNL_IP_STRAIN + c, q, strain[c]);
+  }
+
+  // ---- J2 radial return with Johnson-Cook hardening (Element.C:407-622)
   ReturnState<R> st;
-  R strain[6];
 #pragma unroll
   for (int c = 0; c < 6; c++)
   {
     st.s[c] = ipv<R>(M, DNL_IP_STRESS + c, q);
-    strain[c] = ipv<R>(M, DNL_IP_STRAIN + c, q);
-    st.ep[c] = ipv<R>(M, DNL_IP_PLASTIC_STRAIN + c, q);
+    st.ep[c] = R(0); // receives the plastic strain increment
   }
   st.epsp = ipv<R>(M, DNL_IP_EPSP, q);
   st.depsp = ipv<R>(M, DNL_IP_DEPSP, q);
@@ -403,14 +485,10 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
   st.T = ipv<R>(M, DNL_IP_T, q);
   st.eint = ipv<R>(M, DNL_IP_EINT, q);
   st.einel = ipv<R>(M, DNL_IP_EINEL, q);
-  const R detJ0 = ipv<R>(M, DNL_IP_DETJ0, q);
   st.pressure = (st.s[0] + st.s[3] + st.s[5]) / R(3) + R(mp.K) * (trSum / R(NPE));
-
-  // ---- J2 radial return with Johnson-Cook hardening (Element.C:407-622)
   {
     JC<R> jc;
     jc.load(mp);
-    ReturnState<R> st0 = st;
     bool ok;
     radial_return<R>(jc, R(mp.twoG), R(mp.heatFrac), R(1.0 / mp.rho0), dE, R(dt), st, ok);
     if (!ok)
@@ -418,35 +496,48 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
       if constexpr (sizeof(R) == 4)
       {
         atomicAdd(&C->resolves, 1);
-        bool ok64 = resolve_fp64(mp, reinterpret_cast<const float *>(dE), dt,
-                                 reinterpret_cast<ReturnState<float> &>(st),
-                                 reinterpret_cast<const ReturnState<float> &>(st0));
-        if (!ok64)
+        const Resolved r = resolve_fp64(reinterpret_cast<const float *>(M.ip), M.nIPpad, q, M.mat + mi, dE[0],
+                                        dE[1], dE[2], dE[3], dE[4], dE[5], dt, st.pressure);
+        if (!r.ok)
           raise_status(C, DNL_ERR_NEWTON, q);
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+        {
+          st.s[c] = r.s[c];
+          st.ep[c] = r.dep[c];
+        }
+        st.epsp = r.epsp;
+        st.depsp = r.depsp;
+        st.gamma = r.gamma;
+        st.gcum = r.gcum;
+        st.yield = r.yield;
+        st.T = r.T;
+        st.eint = r.eint;
+        st.einel = r.einel;
       }
       else
         raise_status(C, DNL_ERR_NEWTON, q);
     }
   }
 
-  // ---- total strain, final rotation for objectivity (Element.C:1116-1161)
-#pragma unroll
-  for (int c = 0; c < 6; c++)
-    strain[c] += dE[c];
+  // ---- final rotation of the stress and of the plastic strain, state write-back
   rotate_sym<R>(Rot, st.s);
-  rotate_sym<R>(Rot, strain);
-  rotate_sym<R>(Rot, st.ep);
-  R rho = R(mp.rho0) * detJ0 / detJ; // Element::computeDensity (Element.C:1243-1256)
-  if (AXI)
+  {
+    R ep[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      ep[c] = ipv<R>(M, DNL_IP_PLASTIC_STRAIN + c, q) + st.ep[c];
+    rotate_sym<R>(Rot, ep);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      ipw<R>(M, DNL_IP_PLASTIC_STRAIN + c, q, ep[c]);
+  }
+  R rho = R(mp.rho0) * ipv<R>(M, DNL_IP_DETJ0, q) / detJ; // Element::computeDensity (Element.C:1243-1256)
+  if constexpr (AXI)
     rho /= radius;
-
 #pragma unroll
   for (int c = 0; c < 6; c++)
-  {
     ipw<R>(M, DNL_IP_STRESS + c, q, st.s[c]);
-    ipw<R>(M, DNL_IP_STRAIN + c, q, strain[c]);
-    ipw<R>(M, DNL_IP_PLASTIC_STRAIN + c, q, st.ep[c]);
-  }
   ipw<R>(M, DNL_IP_EPSP, q, st.epsp);
   ipw<R>(M, DNL_IP_DEPSP, q, st.depsp);
   ipw<R>(M, DNL_IP_GAMMA, q, st.gamma);
@@ -460,11 +551,11 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
 
   // ---- internal forces f_n = -sum_g dN_n/dx . sigma w detJ (Element.C:362-404):
   // with P = -w detJ J^-1 sigma, f_n,i = sum_k dN_n/dxi_k P_ki
-  R P[DIM][DIM];
+  R P[3][3];
 #pragma unroll
-  for (int k = 0; k < DIM; k++)
+  for (int k = 0; k < 3; k++)
 #pragma unroll
-    for (int i = 0; i < DIM; i++)
+    for (int i = 0; i < 3; i++)
     {
       R s = R(0);
 #pragma unroll
@@ -472,27 +563,19 @@ __global__ void __launch_bounds__(128) k_element(DevModel M)
         s += inv[k][j] * st.s[sym_index(j, i)];
       P[k][i] = -WxdJ * s;
     }
-  R f[NPE * DIM];
   const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
-#pragma unroll
-  for (int n = 0; n < NPE; n++)
-#pragma unroll
-    for (int i = 0; i < DIM; i++)
-    {
-      R s = R(0);
-#pragma unroll
-      for (int k = 0; k < DIM; k++)
-        s += dN[n][k] * P[k][i];
-      if (AXI && i == 0)
-        s -= Nv[n] * hoop;
-      f[n * DIM + i] = s;
-    }
-  reduce_scatter<R, NPE, DIM>(amask, g, f);
+  ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
+  __syncwarp(amask);
   R4 fs;
-  fs.x = f[0];
-  fs.y = f[1];
-  fs.z = (DIM == 3) ? f[DIM - 1] : R(0);
-  fs.w = R(0);
+  fs.x = fs.y = fs.z = fs.w = R(0);
+#pragma unroll
+  for (int l = 0; l < NPE; l++)
+  {
+    fs.x += grp[l * ROW + g * DIM];
+    fs.y += grp[l * ROW + g * DIM + 1];
+    if constexpr (DIM == 3)
+      fs.z += grp[l * ROW + g * DIM + 2];
+  }
   reinterpret_cast<R4 *>(M.slot)[q] = fs;
 }
 
