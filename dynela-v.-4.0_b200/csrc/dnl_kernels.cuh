@@ -11,8 +11,10 @@
 //   nodes        double4 AoS (x, y, z, pad): coords, disp, u[2], v[2], a[2]; double mass
 //   elements     int32 conn[nE*npe]; int32 material
 //   points       Real ip[29][nIPpad] component-major (coalesced per component)
-//   force slots  Real4 slot[nE*npe]: one per (element, local node), written by the
-//                element pass, gathered per node in element order through a CSR list
+//   force slots  Real4 slot[nE*npe]: one per (element, local node), stored in node
+//                order (the slots of a node are contiguous, its elements in
+//                increasing order); the element pass scatters to slot_pos[q], the
+//                nodal pass reads its node's run of slots
 #pragma once
 
 #include "dnl_math.cuh"
@@ -55,7 +57,8 @@ struct DevModel
   const MatDev *mat;
   void *ip;
   void *slot;
-  const int *csr_off, *csr_idx;
+  const int *csr_off;      // [nN+1] first slot of each node
+  const int *slot_pos;     // [nE*npe] slot of (element, local node) in node order
   const uint8_t *bc;       // per node: 2 bits per component (DNL_BC_*)
   const double4 *bcval;    // per node imposed speed (only read where the code is DNL_BC_SPEED)
   const int4 *bcfun;       // per node function index per component (-1 none)
@@ -161,8 +164,8 @@ __device__ __forceinline__ void raise_status(Ctl *c, int code, int index)
 // state in registers.
 struct Resolved
 {
-  float s[6], dep[6];
-  float epsp, depsp, gamma, gcum, yield, T, eint, einel;
+  float s[6];
+  float epsp, depsp, gamma, gcum, yield, T, eint, einel, kplast;
   int ok;
 };
 
@@ -175,10 +178,7 @@ __device__ __noinline__ Resolved resolve_fp64(const float *ip, int nIPpad, int q
   jc.load(mp);
   ReturnState<double> d;
   for (int c = 0; c < 6; c++)
-  {
     d.s[c] = ip[(size_t)(DNL_IP_STRESS + c) * nIPpad + q];
-    d.ep[c] = 0.0;
-  }
   d.epsp = ip[(size_t)DNL_IP_EPSP * nIPpad + q];
   d.depsp = ip[(size_t)DNL_IP_DEPSP * nIPpad + q];
   d.gamma = ip[(size_t)DNL_IP_GAMMA * nIPpad + q];
@@ -193,10 +193,8 @@ __device__ __noinline__ Resolved resolve_fp64(const float *ip, int nIPpad, int q
   radial_return<double>(jc, mp.twoG, mp.heatFrac, 1.0 / mp.rho0, de, dt, d, ok);
   Resolved r;
   for (int c = 0; c < 6; c++)
-  {
     r.s[c] = (float)d.s[c];
-    r.dep[c] = (float)d.ep[c];
-  }
+  r.kplast = (float)d.kplast;
   r.epsp = (float)d.epsp;
   r.depsp = (float)d.depsp;
   r.gamma = (float)d.gamma;
@@ -302,6 +300,12 @@ template <typename R, int NPE, int N> struct MassToShared
 // ---------------------------------------------------------- element pass
 
 constexpr int ELEM_THREADS = 128;
+#ifndef DNL_ELEM_MINB_F32
+#define DNL_ELEM_MINB_F32 6
+#endif
+#ifndef DNL_ELEM_MINB_F64
+#define DNL_ELEM_MINB_F64 4
+#endif
 
 // One thread per integration point; the NPE points of an element are NPE
 // consecutive lanes, and lane g also loads node g of the element.
@@ -314,11 +318,13 @@ constexpr int ELEM_THREADS = 128;
 // The element's nodal forces are summed over its points through shared memory
 // (each lane writes its NPE x DIM contributions, lane g then adds node g's).
 template <typename R, int NPE, int MODE>
-__global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_element(DevModel M)
+__global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_F32 : DNL_ELEM_MINB_F64))
+    k_element(DevModel M)
 {
   constexpr int DIM = (NPE == 8) ? 3 : 2;
   constexpr bool AXI = (NPE == 4);
-  constexpr int ROW = NPE * DIM + 1; // padded shared-memory row (bank spread)
+  // padded shared-memory row (bank spread): forces, or rotation + inverse Jacobian
+  constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
   using R4 = typename V4<R>::type;
   __shared__ R sh[ELEM_THREADS * ROW];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -407,7 +413,6 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
   R WxdJ = detJ; // Gauss weight 1
   if constexpr (AXI)
     WxdJ *= R(6.28318530717958647692) * radius;
-  R *row = sh + threadIdx.x * ROW;
   R *grp = sh + (threadIdx.x - g) * ROW;
 
   if constexpr (MODE == 1)
@@ -420,7 +425,7 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
       ipw<R>(M, c, q, R(0));
     ipw<R>(M, DNL_IP_T, q, R(mp.T0));
     ipw<R>(M, DNL_IP_DENSITY, q, rho0);
-    MassToShared<R, NPE, 0>::run(xi0, xi1, xi2, rho0 * WxdJ, row);
+    MassToShared<R, NPE, 0>::run(xi0, xi1, xi2, rho0 * WxdJ, sh + threadIdx.x * ROW);
     __syncwarp(amask);
     R m = R(0);
 #pragma unroll
@@ -429,7 +434,7 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
     R4 s;
     s.x = m;
     s.y = s.z = s.w = R(0);
-    reinterpret_cast<R4 *>(M.slot)[q] = s;
+    reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = s;
     return;
   }
 
@@ -469,14 +474,21 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
       ipw<R>(M, DNL_IP_STRAIN + c, q, strain[c]);
   }
 
+  // rotation and inverse Jacobian wait in this lane's shared-memory row while
+  // the radial return holds its registers
+  R *row = sh + threadIdx.x * ROW;
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+  {
+    row[k] = Rot[k];
+    row[9 + k] = inv[k / 3][k % 3];
+  }
+
   // ---- J2 radial return with Johnson-Cook hardening (Element.C:407-622)
   ReturnState<R> st;
 #pragma unroll
   for (int c = 0; c < 6; c++)
-  {
     st.s[c] = ipv<R>(M, DNL_IP_STRESS + c, q);
-    st.ep[c] = R(0); // receives the plastic strain increment
-  }
   st.epsp = ipv<R>(M, DNL_IP_EPSP, q);
   st.depsp = ipv<R>(M, DNL_IP_DEPSP, q);
   st.gamma = ipv<R>(M, DNL_IP_GAMMA, q);
@@ -502,10 +514,8 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
           raise_status(C, DNL_ERR_NEWTON, q);
 #pragma unroll
         for (int c = 0; c < 6; c++)
-        {
           st.s[c] = r.s[c];
-          st.ep[c] = r.dep[c];
-        }
+        st.kplast = r.kplast;
         st.epsp = r.epsp;
         st.depsp = r.depsp;
         st.gamma = r.gamma;
@@ -521,17 +531,23 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
   }
 
   // ---- final rotation of the stress and of the plastic strain, state write-back
-  rotate_sym<R>(Rot, st.s);
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+    Rot[k] = row[k];
   {
+    // PlasticStrain += gamma s*/|s*| (Element.C:587), then rotated
     R ep[6];
+    const R pn = (st.s[0] + st.s[3] + st.s[5]) / R(3);
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      ep[c] = ipv<R>(M, DNL_IP_PLASTIC_STRAIN + c, q) + st.ep[c];
+      ep[c] = ipv<R>(M, DNL_IP_PLASTIC_STRAIN + c, q) +
+              st.kplast * (st.s[c] - ((c == 0 || c == 3 || c == 5) ? pn : R(0)));
     rotate_sym<R>(Rot, ep);
 #pragma unroll
     for (int c = 0; c < 6; c++)
       ipw<R>(M, DNL_IP_PLASTIC_STRAIN + c, q, ep[c]);
   }
+  rotate_sym<R>(Rot, st.s);
   R rho = R(mp.rho0) * ipv<R>(M, DNL_IP_DETJ0, q) / detJ; // Element::computeDensity (Element.C:1243-1256)
   if constexpr (AXI)
     rho /= radius;
@@ -560,7 +576,7 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
       R s = R(0);
 #pragma unroll
       for (int j = 0; j < DIM; j++)
-        s += inv[k][j] * st.s[sym_index(j, i)];
+        s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
       P[k][i] = -WxdJ * s;
     }
   const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
@@ -576,7 +592,7 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? 4 : 3)) k_elem
     if constexpr (DIM == 3)
       fs.z += grp[l * ROW + g * DIM + 2];
   }
-  reinterpret_cast<R4 *>(M.slot)[q] = fs;
+  reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = fs;
 }
 
 // ------------------------------------------------------------ nodal update
@@ -603,9 +619,10 @@ __global__ void __launch_bounds__(256) k_nodal(DevModel M)
   double4 f = make_double4(0, 0, 0, 0);
   const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
   const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
+#pragma unroll 4
   for (int k = kb; k < ke; k++)
   {
-    const R4 s = slot[M.csr_idx[k]];
+    const R4 s = slot[k];
     f.x += (double)s.x;
     f.y += (double)s.y;
     f.z += (double)s.z;
@@ -734,7 +751,7 @@ __global__ void k_gather(DevModel M, int what)
   double4 f = make_double4(0, 0, 0, 0);
   for (int k = M.csr_off[i]; k < M.csr_off[i + 1]; k++)
   {
-    const R4 s = slot[M.csr_idx[k]];
+    const R4 s = slot[k];
     f.x += (double)s.x;
     f.y += (double)s.y;
     f.z += (double)s.z;

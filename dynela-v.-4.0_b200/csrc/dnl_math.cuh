@@ -130,7 +130,8 @@ template <typename R> __device__ __forceinline__ void sym_eigen3(const R a6[6], 
       A[i][j] = a6[sym_index(i, j)];
       V[i][j] = (i == j) ? R(1) : R(0);
     }
-  const R tol = Num<R>::eps * R(1e-2);
+  // stop once the off-diagonal part is at the rounding level of the diagonal
+  const R tol = Num<R>::eps;
   for (int sweep = 0; sweep < 12; sweep++)
   {
     R off = Num<R>::abs_(A[0][1]) + Num<R>::abs_(A[0][2]) + Num<R>::abs_(A[1][2]);
@@ -146,19 +147,10 @@ template <typename R> __device__ __forceinline__ void sym_eigen3(const R a6[6], 
   mu[2] = A[2][2];
 }
 
-// Polar decomposition F = R U of F = I + H and the logarithmic strain
-// increment ln U (Tensor2::polarCuppenLnU, Tensor2.C:1237-1457, restated):
-// with A = F^T F - I = H + H^T + H^T H and its eigenpairs (mu_k, n_k),
-// ln U = sum log1p(mu_k)/2 n_k n_k and R = F U^-1, U^-1 = sum (1+mu_k)^-1/2 n_k n_k.
-// Working on F^T F - I keeps the relative precision of the small increments.
-template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R lnU[6], R Rot[9])
+// Spectral functions of the small symmetric A = C - I (C = F^T F) by cyclic
+// Jacobi: lnU = sum log1p(mu_k)/2 n_k n_k, Wm = U^-1 - I = sum ((1+mu_k)^-1/2 - 1) n_k n_k.
+template <typename R> __device__ __noinline__ void spectral_jacobi(const R A[6], R lnU[6], R Wm[6])
 {
-  R A[6];
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = i; j < 3; j++)
-      A[sym_index(i, j)] = H[3 * i + j] + H[3 * j + i] + H[i] * H[j] + H[3 + i] * H[3 + j] + H[6 + i] * H[6 + j];
   R mu[3], V[3][3];
   sym_eigen3<R>(A, mu, V);
   R hl[3], g[3];
@@ -166,9 +158,8 @@ template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R 
   for (int k = 0; k < 3; k++)
   {
     hl[k] = R(0.5) * Num<R>::log1p_(mu[k]);
-    g[k] = Num<R>::rsqrt_(R(1) + mu[k]) - R(1); // (1+mu)^-1/2 - 1
+    g[k] = Num<R>::rsqrt_(R(1) + mu[k]) - R(1);
   }
-  R Wm[6]; // U^-1 - I
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -185,6 +176,83 @@ template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R 
       lnU[sym_index(i, j)] = a;
       Wm[sym_index(i, j)] = b;
     }
+}
+
+// The same two functions as power series, without eigenvectors.  By
+// Cayley-Hamilton every power is A^k = al I + be A + ga A^2 with the scalar
+// recurrence A^(k+1) = (ga I3) I + (al - ga I2) A + (be + ga I1) A^2 (I1, I2,
+// I3 the invariants of A), so both series cost a few scalar operations per
+// term:  log(1+x) = sum (-1)^(k+1) x^k / k,  (1+x)^-1/2 - 1 = sum binom(-1/2, k) x^k.
+// The series stop when |A|_F^k falls below the rounding level; returns false
+// when |A|_F is too large for a short series (the caller then uses Jacobi).
+template <typename R> __device__ __forceinline__ bool spectral_series(const R A[6], R lnU[6], R Wm[6])
+{
+  const bool fp64 = sizeof(R) == 8;
+  const R r = Num<R>::sqrt_(A[0] * A[0] + A[3] * A[3] + A[5] * A[5] + R(2) * (A[1] * A[1] + A[2] * A[2] + A[4] * A[4]));
+  const R rmax = fp64 ? R(0.25) : R(0.35);
+  if (!(r < rmax))
+    return false;
+  const R tol = fp64 ? R(2e-17) : R(3e-8);
+  const R I1 = A[0] + A[3] + A[5];
+  const R I2 = A[0] * A[3] + A[3] * A[5] + A[5] * A[0] - A[1] * A[1] - A[2] * A[2] - A[4] * A[4];
+  const R I3 = A[0] * (A[3] * A[5] - A[4] * A[4]) - A[1] * (A[1] * A[5] - A[4] * A[2]) + A[2] * (A[1] * A[4] - A[3] * A[2]);
+  R al = R(0), be = R(1), ga = R(0);      // A^1
+  R l0 = R(0), l1 = R(0), l2 = R(0);      // log(I + A)
+  R w0 = R(0), w1 = R(0), w2 = R(0);      // (I + A)^-1/2 - I
+  R cl = R(1), cw = R(-0.5), rk = r;
+  for (int k = 1; k < 64; k++)
+  {
+    l0 += cl * al;
+    l1 += cl * be;
+    l2 += cl * ga;
+    w0 += cw * al;
+    w1 += cw * be;
+    w2 += cw * ga;
+    if (rk < tol)
+      break;
+    const R nal = ga * I3, nbe = al - ga * I2, nga = be + ga * I1;
+    al = nal;
+    be = nbe;
+    ga = nga;
+    cl = -cl * R(k) / R(k + 1);
+    cw = -cw * R(2 * k + 1) / R(2 * k + 2);
+    rk *= r;
+  }
+  // A^2
+  R A2[6];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++)
+      A2[sym_index(i, j)] = A[sym_index(i, 0)] * A[sym_index(0, j)] + A[sym_index(i, 1)] * A[sym_index(1, j)] +
+                            A[sym_index(i, 2)] * A[sym_index(2, j)];
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+  {
+    const R d = (c == 0 || c == 3 || c == 5) ? R(1) : R(0);
+    lnU[c] = R(0.5) * (l0 * d + l1 * A[c] + l2 * A2[c]);
+    Wm[c] = w0 * d + w1 * A[c] + w2 * A2[c];
+  }
+  return true;
+}
+
+// Polar decomposition F = R U of F = I + H and the logarithmic strain
+// increment ln U (Tensor2::polarCuppenLnU, Tensor2.C:1237-1457, restated):
+// with A = F^T F - I = H + H^T + H^T H, ln U = log(I + A)/2 and
+// R = F U^-1, U^-1 = (I + A)^-1/2.  Working on A keeps the relative precision
+// of the small increments; the series above is used when |A| is small, the
+// Jacobi eigen-decomposition otherwise.
+template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R lnU[6], R Rot[9])
+{
+  R A[6];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++)
+      A[sym_index(i, j)] = H[3 * i + j] + H[3 * j + i] + H[i] * H[j] + H[3 + i] * H[3 + j] + H[6 + i] * H[6 + j];
+  R Wm[6]; // U^-1 - I
+  if (!spectral_series<R>(A, lnU, Wm))
+    spectral_jacobi<R>(A, lnU, Wm);
   // R = (I + H)(I + Wm) = I + H + Wm + H Wm
 #pragma unroll
   for (int i = 0; i < 3; i++)
@@ -248,12 +316,14 @@ template <typename R> struct JC
   }
 };
 
-// Per-point state handled by the radial return.
+// Per-point state handled by the radial return.  The plastic strain tensor is
+// not carried: its increment is kplast times the deviator of the returned
+// stress (gamma s*/|s*| = gamma/(|s*| - 2G gamma) s_new, Element.C:587-590).
 template <typename R> struct ReturnState
 {
-  R s[6];   // stress (in: old, out: new, before the final rotation)
-  R ep[6];  // plastic strain tensor
+  R s[6]; // stress (in: old, out: new, before the final rotation)
   R epsp, depsp, gamma, gcum, yield, T, pressure, eint, einel;
+  R kplast; // out: plastic strain increment / deviator of the new stress (0 if elastic)
 };
 
 // Element::computeStress (Element.C:407-622) for one integration point.  The
@@ -271,14 +341,13 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
   const bool fp64 = sizeof(R) == 8;
   const int itMax = fp64 ? 250 : 60;
   R twoG32 = SQ32 * twoG;
-  R sOld[6], dev[6];
+  R dev[6];
+  // dE : sigma_old, the first half of the stress power (Element.C:608)
+  const R dEsOld = sym_ddot(dE, st.s);
+  R p0 = (st.s[0] + st.s[3] + st.s[5]) / R(3);
 #pragma unroll
   for (int c = 0; c < 6; c++)
-    sOld[c] = st.s[c];
-  R p0 = (sOld[0] + sOld[3] + sOld[5]) / R(3);
-#pragma unroll
-  for (int c = 0; c < 6; c++)
-    dev[c] = sOld[c];
+    dev[c] = st.s[c];
   dev[0] -= p0;
   dev[3] -= p0;
   dev[5] -= p0;
@@ -299,6 +368,7 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
   R dummy;
   int iterate = 0;
   ok = true;
+  st.kplast = R(0);
   if (yield == R(0))
   {
     jc.eval(gammaInitial, gammaInitial / dt, T, dt, yield, dummy, false);
@@ -353,11 +423,10 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
       ok = false;
       return iterate;
     }
-    R invS = R(1) / Snorm;
-#pragma unroll
-    for (int c = 0; c < 6; c++)
-      st.ep[c] += gamma * dev[c] * invS;
-    R scale = R(1) - twoG * gamma * invS;
+    const R invS = R(1) / Snorm;
+    const R scale = R(1) - twoG * gamma * invS;
+    // plastic strain increment gamma dev*/Snorm = kplast * (scale dev*)
+    st.kplast = gamma * invS / scale;
 #pragma unroll
     for (int c = 0; c < 6; c++)
       dev[c] *= scale;
@@ -374,11 +443,7 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
   st.s[3] = dev[3] + p;
   st.s[4] = dev[4];
   st.s[5] = dev[5] + p;
-  R sum[6];
-#pragma unroll
-  for (int c = 0; c < 6; c++)
-    sum[c] = sOld[c] + st.s[c];
-  st.eint += R(0.5) * sym_ddot(dE, sum) * inv_rho0;
+  st.eint += R(0.5) * (dEsOld + sym_ddot(dE, st.s)) * inv_rho0;
   if (gamma != R(0))
   {
     R plWorkInc = R(0.5) * gamma * (sym_norm(dev) + Snorm0);

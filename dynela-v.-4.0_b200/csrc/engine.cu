@@ -463,7 +463,9 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   }
 
   // ---- node -> (element, local node) slots, in element order
-  std::vector<int> off(h->nN + 1, 0), idx((size_t)h->nIP);
+  // slot of incidence k = e*npe + n in node order; within a node, elements in
+  // increasing order (the order of the reference's scatter-add, Model.C:881-898)
+  std::vector<int> off(h->nN + 1, 0), pos((size_t)h->nIP);
   for (size_t k = 0; k < conn.size(); k++)
     off[conn[k] + 1]++;
   for (int i = 0; i < h->nN; i++)
@@ -471,7 +473,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   {
     std::vector<int> fill(off.begin(), off.end() - 1);
     for (size_t k = 0; k < conn.size(); k++)
-      idx[fill[conn[k]]++] = (int)k;
+      pos[k] = fill[conn[k]]++;
   }
 
   int rc = DNL_OK;
@@ -484,7 +486,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.nSpeed = h->nSpeed;
   M.nFunc = h->nFunc;
   const size_t rsz = h->precision == DNL_PREC_MIXED ? 4 : 8;
-  int *d_eb = nullptr, *d_nb = nullptr, *d_conn = nullptr, *d_emat = nullptr, *d_off = nullptr, *d_idx = nullptr;
+  int *d_eb = nullptr, *d_nb = nullptr, *d_conn = nullptr, *d_emat = nullptr, *d_off = nullptr, *d_pos = nullptr;
   int *d_speed = nullptr, *d_foff = nullptr;
   MatDev *d_mat = nullptr;
   uint8_t *d_bc = nullptr;
@@ -494,7 +496,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   std::vector<double4> zeros4(h->nN, make_double4(0, 0, 0, 0));
   if ((rc = upload(h, &d_eb, h->elemBegin)) || (rc = upload(h, &d_nb, h->nodeBegin)) ||
       (rc = upload(h, &d_conn, conn)) || (rc = upload(h, &d_emat, emat)) || (rc = upload(h, &d_mat, mats)) ||
-      (rc = upload(h, &d_off, off)) || (rc = upload(h, &d_idx, idx)) || (rc = upload(h, &d_bc, bc)) ||
+      (rc = upload(h, &d_off, off)) || (rc = upload(h, &d_pos, pos)) || (rc = upload(h, &d_bc, bc)) ||
       (rc = upload(h, &d_bcval, bcval)) || (rc = upload(h, &d_bcfun, bcfun)) ||
       (rc = upload(h, &d_speed, speedNodes)) || (rc = upload(h, &d_fx, fx)) || (rc = upload(h, &d_fy, fy)) ||
       (rc = upload(h, &d_foff, foff)) || (rc = upload(h, &M.x, x)) || (rc = upload(h, &M.disp, zeros4)) ||
@@ -523,7 +525,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.emat = d_emat;
   M.mat = d_mat;
   M.csr_off = d_off;
-  M.csr_idx = d_idx;
+  M.slot_pos = d_pos;
   M.bc = d_bc;
   M.bcval = d_bcval;
   M.bcfun = d_bcfun;
