@@ -237,6 +237,7 @@ def run_engine_arm(args, rank, world, dist):
     desc = workload(args.precision)
     word = 4 if args.precision == "mixed" else 8
     eng = Engine(desc).init()
+    variant, variant_ms = eng.autotune(steps=6)  # leaves the state unchanged
     if args.warmup:
         eng.run(max_incs=args.warmup)
 
@@ -279,6 +280,7 @@ def run_engine_arm(args, rank, world, dist):
     if args.precision == "mixed" and not args.no_fp64:
         d64 = workload("fp64")
         e64 = Engine(d64).init()
+        e64.autotune(steps=6)
         if args.warmup:
             e64.run(max_incs=args.warmup)
         k64 = min(args.steps, 500)
@@ -294,6 +296,7 @@ def run_engine_arm(args, rank, world, dist):
         t0 = time.perf_counter()
         e = Engine(desc)
         e.init()
+        e.set_variant(variant)
         e.run(max_incs=args.steps)
         coords = e.nodes(_abi.NODE_COORDS)
         ips = e.ips()
@@ -321,6 +324,7 @@ def run_engine_arm(args, rank, world, dist):
         "step_roofline": step_roofline,
         "gpu_launches": launches,
         "fp64_resolves": ctl["fp64_resolves"],
+        "element_variant": {"chosen": int(variant), "autotune_ms": [round(float(x), 5) for x in variant_ms]},
     }
     if fp64:
         out["fp64_path"] = fp64

@@ -143,13 +143,22 @@ __host__ __device__ constexpr int node_sign(int n, int k)
   return k == 0 ? ((n & 3) == 1 || (n & 3) == 2 ? 1 : -1) : (k == 1 ? ((n & 3) >= 2 ? 1 : -1) : (n >= 4 ? 1 : -1));
 }
 
+// Point state in tiles of TILE consecutive integration points: within a tile,
+// component-major (one TILE-long run per component), so that a tile is one
+// contiguous block for a bulk copy and every component access is coalesced.
+constexpr int TILE = 128;
+__host__ __device__ __forceinline__ size_t ip_index(int c, int q)
+{
+  return (size_t)(q / TILE) * (DNL_IP_NCOMP * TILE) + (size_t)c * TILE + (q % TILE);
+}
+
 template <typename R> __device__ __forceinline__ R ipv(const DevModel &M, int c, int q)
 {
-  return reinterpret_cast<const R *>(M.ip)[(size_t)c * M.nIPpad + q];
+  return reinterpret_cast<const R *>(M.ip)[ip_index(c, q)];
 }
 template <typename R> __device__ __forceinline__ void ipw(const DevModel &M, int c, int q, R v)
 {
-  reinterpret_cast<R *>(M.ip)[(size_t)c * M.nIPpad + q] = v;
+  reinterpret_cast<R *>(M.ip)[ip_index(c, q)] = v;
 }
 
 __device__ __forceinline__ void raise_status(Ctl *c, int code, int index)
@@ -169,24 +178,23 @@ struct Resolved
   int ok;
 };
 
-__device__ __noinline__ Resolved resolve_fp64(const float *ip, int nIPpad, int q, const MatDev *matp, float e0,
-                                              float e1, float e2, float e3, float e4, float e5, double dt,
-                                              float pressure)
+__device__ __noinline__ Resolved resolve_fp64(const float *ip, int q, const MatDev *matp, float e0, float e1,
+                                              float e2, float e3, float e4, float e5, double dt, float pressure)
 {
   const MatDev &mp = *matp;
   JC<double> jc;
   jc.load(mp);
   ReturnState<double> d;
   for (int c = 0; c < 6; c++)
-    d.s[c] = ip[(size_t)(DNL_IP_STRESS + c) * nIPpad + q];
-  d.epsp = ip[(size_t)DNL_IP_EPSP * nIPpad + q];
-  d.depsp = ip[(size_t)DNL_IP_DEPSP * nIPpad + q];
-  d.gamma = ip[(size_t)DNL_IP_GAMMA * nIPpad + q];
-  d.gcum = ip[(size_t)DNL_IP_GAMMA_CUM * nIPpad + q];
-  d.yield = ip[(size_t)DNL_IP_YIELD * nIPpad + q];
-  d.T = ip[(size_t)DNL_IP_T * nIPpad + q];
-  d.eint = ip[(size_t)DNL_IP_EINT * nIPpad + q];
-  d.einel = ip[(size_t)DNL_IP_EINEL * nIPpad + q];
+    d.s[c] = ip[ip_index(DNL_IP_STRESS + c, q)];
+  d.epsp = ip[ip_index(DNL_IP_EPSP, q)];
+  d.depsp = ip[ip_index(DNL_IP_DEPSP, q)];
+  d.gamma = ip[ip_index(DNL_IP_GAMMA, q)];
+  d.gcum = ip[ip_index(DNL_IP_GAMMA_CUM, q)];
+  d.yield = ip[ip_index(DNL_IP_YIELD, q)];
+  d.T = ip[ip_index(DNL_IP_T, q)];
+  d.eint = ip[ip_index(DNL_IP_EINT, q)];
+  d.einel = ip[ip_index(DNL_IP_EINEL, q)];
   d.pressure = pressure;
   const double de[6] = {e0, e1, e2, e3, e4, e5};
   bool ok;
@@ -299,7 +307,6 @@ template <typename R, int NPE, int N> struct MassToShared
 
 // ---------------------------------------------------------- element pass
 
-constexpr int ELEM_THREADS = 128;
 #ifndef DNL_ELEM_MINB_F32
 #define DNL_ELEM_MINB_F32 6
 #endif
@@ -307,47 +314,40 @@ constexpr int ELEM_THREADS = 128;
 #define DNL_ELEM_MINB_F64 4
 #endif
 
-// One thread per integration point; the NPE points of an element are NPE
-// consecutive lanes, and lane g also loads node g of the element.
-// MODE 0: one increment's element work (Explicit.C:204-226 + computeDensity,
-//         Element.C:1103-1256, with the Jacobian of ElementPlane.C:46-102 /
-//         Element3D.C:64-115 computed from the current coordinates).
-// MODE 1: start of the solve: reference Jacobian detJ0, initial point state
-//         (Element::initializeData, Element.C:258-301) and the element lumped
-//         masses (Element::computeMassMatrix, Element.C:304-339) into the slots.
-// The element's nodal forces are summed over its points through shared memory
-// (each lane writes its NPE x DIM contributions, lane g then adds node g's).
-template <typename R, int NPE, int MODE>
-__global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_F32 : DNL_ELEM_MINB_F64))
-    k_element(DevModel M)
+template <int NPE> struct ElemShape
 {
-  constexpr int DIM = (NPE == 8) ? 3 : 2;
-  constexpr bool AXI = (NPE == 4);
-  // padded shared-memory row (bank spread): forces, or rotation + inverse Jacobian
-  constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
-  using R4 = typename V4<R>::type;
-  __shared__ R sh[ELEM_THREADS * ROW];
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const int g = lane & (NPE - 1);
-  const int base = lane & ~(NPE - 1);
-  const int e = q / NPE;
-  const bool valid = e < M.nE;
-  const int ec = valid ? e : M.nE - 1;
-  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
-  Ctl *C = M.ctl + inst;
-  const bool act = valid && (MODE == 1 || C->active);
-  const unsigned amask = __ballot_sync(0xffffffffu, act);
-  if (!act)
-    return;
-  const int f0 = C->f0;
-  const int mi = M.emat[e];
-  const MatDev &mp = M.mat[mi];
+  static constexpr int DIM = (NPE == 8) ? 3 : 2;
+  static constexpr bool AXI = (NPE == 4);
+  // shared-memory row per point (padded for bank spread): the element forces
+  // of the transpose, or the rotation and inverse Jacobian parked across the return
+  static constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
+};
 
-  // ---- gather the element's nodes (lane g <- node g)
-  const int node = M.conn[q];
-  const double4 X = M.x[node];
-  const double4 U = M.u[f0][node];
+// Where the element update reads the old point state from: global memory, or
+// the tile staged in shared memory by the bulk copies.
+template <typename R> struct GlobalState
+{
+  const DevModel &M;
+  int q;
+  __device__ __forceinline__ R operator()(int c) const { return ipv<R>(M, c, q); }
+};
+template <typename R> struct SharedTile
+{
+  const R *buf;
+  int t;
+  __device__ __forceinline__ R operator()(int c) const { return buf[c * TILE + t]; }
+};
+
+// Jacobian J = sum x_n dN_n/dxi and G = sum du_n dN_n/dxi at this lane's Gauss
+// point from the element's nodes (lane g holds node g), then detJ, J^-1 and the
+// displacement gradient H = F - I = G J^-1 (+ the axisymmetric hoop term
+// F33 - 1 = sum N_n du_r,n / r, ElementAxi.C:78-100).
+template <typename R, int NPE>
+__device__ __forceinline__ void kinematics(unsigned amask, int g, int base, const double4 &X, const double4 &U, R &detJ,
+                                           R (&inv)[3][3], R &radius, R (&H)[9])
+{
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  constexpr bool AXI = ElemShape<NPE>::AXI;
   const double x0 = __shfl_sync(amask, X.x, base), y0 = __shfl_sync(amask, X.y, base),
                z0 = __shfl_sync(amask, X.z, base);
   const double ux0 = __shfl_sync(amask, U.x, base), uy0 = __shfl_sync(amask, U.y, base),
@@ -355,8 +355,6 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
   // element-local offsets keep the FP32 path free of large-coordinate cancellation
   const R rx = R(X.x - x0), ry = R(X.y - y0), rz = R(X.z - z0);
   const R urx = R(U.x - ux0), ury = R(U.y - uy0), urz = R(U.z - uz0);
-
-  // ---- J = sum x_n dN_n/dxi and G = sum du_n dN_n/dxi at this Gauss point
   const R a = R(0.57735026918962576451); // 1/sqrt(3)
   const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
   R J[3][3], G[3][3];
@@ -367,15 +365,13 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
       J[i][j] = G[i][j] = R(0);
   R Nr = R(0), Vr = R(0);
   GatherJG<R, NPE, 0>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
-  // axisymmetric radius r = sum N_n x_n (ElementAxi.C:46-59) and the radial
-  // displacement increment sum N_n du_n (ElementAxi.C:88-99), from the offsets
-  R radius = R(1);
+  radius = R(1);
   if constexpr (AXI)
   {
+    // r = sum N_n x_n (ElementAxi.C:46-59) and sum N_n du_n, from the offsets
     radius = R(x0 + (double)Nr);
     Vr += R(ux0);
   }
-  R detJ, inv[3][3];
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -407,76 +403,71 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
     inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
     inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
   }
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+    {
+      R s = R(0);
+#pragma unroll
+      for (int k = 0; k < DIM; k++)
+        s += G[i][k] * inv[k][j];
+      H[3 * i + j] = (i < DIM && j < DIM) ? s : R(0);
+    }
+  if constexpr (AXI)
+    H[8] = Vr / radius;
+}
+
+// One increment's work at one Gauss point (Explicit.C:204-226 + the density of
+// Explicit::computeDensity; Element.C:1103-1256 with the Jacobian of
+// ElementPlane.C:46-102 / Element3D.C:64-115 on the current coordinates):
+// strain increment and rotation by polar decomposition, element-mean pressure,
+// radial return, final rotation, density, and the element's nodal forces,
+// summed over its points through shared memory and stored in node order.
+// `row` is this lane's shared-memory row, `grp` the row of the element's first lane.
+template <typename R, int NPE, class Src>
+__device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q, int e, int g, int base,
+                                               unsigned amask, int node, const Src &old, R *row, R *grp)
+{
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  constexpr bool AXI = ElemShape<NPE>::AXI;
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  using R4 = typename V4<R>::type;
+  const int f0 = C->f0;
+  const double dt = C->dt_eff;
+  const int mi = M.emat[e];
+  const MatDev &mp = M.mat[mi];
+  const double4 X = M.x[node];
+  const double4 U = M.u[f0][node];
+
+  R detJ, inv[3][3], radius, dE[6], Rot[9];
+  {
+    R H[9];
+    kinematics<R, NPE>(amask, g, base, X, U, detJ, inv, radius, H);
+    polar_lnU<R>(H, dE, Rot);
+  }
   if (detJ < R(0))
     raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
-
   R WxdJ = detJ; // Gauss weight 1
   if constexpr (AXI)
     WxdJ *= R(6.28318530717958647692) * radius;
-  R *grp = sh + (threadIdx.x - g) * ROW;
 
-  if constexpr (MODE == 1)
-  {
-    // reference Jacobian (ElementPlane.C:96-100), initial state, element masses
-    const R rho0 = R(mp.rho0);
-    ipw<R>(M, DNL_IP_DETJ0, q, AXI ? detJ * radius : detJ);
-#pragma unroll
-    for (int c = 0; c < DNL_IP_DETJ0; c++)
-      ipw<R>(M, c, q, R(0));
-    ipw<R>(M, DNL_IP_T, q, R(mp.T0));
-    ipw<R>(M, DNL_IP_DENSITY, q, rho0);
-    MassToShared<R, NPE, 0>::run(xi0, xi1, xi2, rho0 * WxdJ, sh + threadIdx.x * ROW);
-    __syncwarp(amask);
-    R m = R(0);
-#pragma unroll
-    for (int l = 0; l < NPE; l++)
-      m += grp[l * ROW + g];
-    R4 s;
-    s.x = m;
-    s.y = s.z = s.w = R(0);
-    reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = s;
-    return;
-  }
-
-  const double dt = C->dt_eff;
-  // ---- F - I = G J^-1 (+ axisymmetric hoop term), polar decomposition
-  R dE[6], Rot[9];
-  {
-    R H[9];
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-      for (int j = 0; j < 3; j++)
-      {
-        R s = R(0);
-#pragma unroll
-        for (int k = 0; k < DIM; k++)
-          s += G[i][k] * inv[k][j];
-        H[3 * i + j] = (i < DIM && j < DIM) ? s : R(0);
-      }
-    if constexpr (AXI)
-      H[8] = Vr / radius;
-    polar_lnU<R>(H, dE, Rot);
-  }
-
-  // ---- element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
+  // element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
   const R trSum = group_sum<NPE>(amask, dE[0] + dE[3] + dE[5]);
 
-  // ---- total strain: Strain += dE, then the final rotation (Element.C:1116-1161)
+  // total strain: Strain += dE, then the final rotation (Element.C:1116-1161)
   {
     R strain[6];
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      strain[c] = ipv<R>(M, DNL_IP_STRAIN + c, q) + dE[c];
+      strain[c] = old(DNL_IP_STRAIN + c) + dE[c];
     rotate_sym<R>(Rot, strain);
 #pragma unroll
     for (int c = 0; c < 6; c++)
       ipw<R>(M, DNL_IP_STRAIN + c, q, strain[c]);
   }
 
-  // rotation and inverse Jacobian wait in this lane's shared-memory row while
-  // the radial return holds its registers
-  R *row = sh + threadIdx.x * ROW;
+  // the rotation and J^-1 wait in shared memory while the return holds its registers
 #pragma unroll
   for (int k = 0; k < 9; k++)
   {
@@ -484,19 +475,19 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
     row[9 + k] = inv[k / 3][k % 3];
   }
 
-  // ---- J2 radial return with Johnson-Cook hardening (Element.C:407-622)
+  // J2 radial return with Johnson-Cook hardening (Element.C:407-622)
   ReturnState<R> st;
 #pragma unroll
   for (int c = 0; c < 6; c++)
-    st.s[c] = ipv<R>(M, DNL_IP_STRESS + c, q);
-  st.epsp = ipv<R>(M, DNL_IP_EPSP, q);
-  st.depsp = ipv<R>(M, DNL_IP_DEPSP, q);
-  st.gamma = ipv<R>(M, DNL_IP_GAMMA, q);
-  st.gcum = ipv<R>(M, DNL_IP_GAMMA_CUM, q);
-  st.yield = ipv<R>(M, DNL_IP_YIELD, q);
-  st.T = ipv<R>(M, DNL_IP_T, q);
-  st.eint = ipv<R>(M, DNL_IP_EINT, q);
-  st.einel = ipv<R>(M, DNL_IP_EINEL, q);
+    st.s[c] = old(DNL_IP_STRESS + c);
+  st.epsp = old(DNL_IP_EPSP);
+  st.depsp = old(DNL_IP_DEPSP);
+  st.gamma = old(DNL_IP_GAMMA);
+  st.gcum = old(DNL_IP_GAMMA_CUM);
+  st.yield = old(DNL_IP_YIELD);
+  st.T = old(DNL_IP_T);
+  st.eint = old(DNL_IP_EINT);
+  st.einel = old(DNL_IP_EINEL);
   st.pressure = (st.s[0] + st.s[3] + st.s[5]) / R(3) + R(mp.K) * (trSum / R(NPE));
   {
     JC<R> jc;
@@ -508,8 +499,8 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
       if constexpr (sizeof(R) == 4)
       {
         atomicAdd(&C->resolves, 1);
-        const Resolved r = resolve_fp64(reinterpret_cast<const float *>(M.ip), M.nIPpad, q, M.mat + mi, dE[0],
-                                        dE[1], dE[2], dE[3], dE[4], dE[5], dt, st.pressure);
+        const Resolved r = resolve_fp64(reinterpret_cast<const float *>(M.ip), q, M.mat + mi, dE[0], dE[1], dE[2],
+                                        dE[3], dE[4], dE[5], dt, st.pressure);
         if (!r.ok)
           raise_status(C, DNL_ERR_NEWTON, q);
 #pragma unroll
@@ -530,25 +521,24 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
     }
   }
 
-  // ---- final rotation of the stress and of the plastic strain, state write-back
+  // final rotation of the plastic strain (PlasticStrain += gamma s*/|s*|,
+  // Element.C:587) and of the stress, state write-back
 #pragma unroll
   for (int k = 0; k < 9; k++)
     Rot[k] = row[k];
   {
-    // PlasticStrain += gamma s*/|s*| (Element.C:587), then rotated
     R ep[6];
     const R pn = (st.s[0] + st.s[3] + st.s[5]) / R(3);
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      ep[c] = ipv<R>(M, DNL_IP_PLASTIC_STRAIN + c, q) +
-              st.kplast * (st.s[c] - ((c == 0 || c == 3 || c == 5) ? pn : R(0)));
+      ep[c] = old(DNL_IP_PLASTIC_STRAIN + c) + st.kplast * (st.s[c] - ((c == 0 || c == 3 || c == 5) ? pn : R(0)));
     rotate_sym<R>(Rot, ep);
 #pragma unroll
     for (int c = 0; c < 6; c++)
       ipw<R>(M, DNL_IP_PLASTIC_STRAIN + c, q, ep[c]);
   }
   rotate_sym<R>(Rot, st.s);
-  R rho = R(mp.rho0) * ipv<R>(M, DNL_IP_DETJ0, q) / detJ; // Element::computeDensity (Element.C:1243-1256)
+  R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
   if constexpr (AXI)
     rho /= radius;
 #pragma unroll
@@ -565,7 +555,7 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
   ipw<R>(M, DNL_IP_EINEL, q, st.einel);
   ipw<R>(M, DNL_IP_DENSITY, q, rho);
 
-  // ---- internal forces f_n = -sum_g dN_n/dx . sigma w detJ (Element.C:362-404):
+  // internal forces f_n = -sum_g dN_n/dx . sigma w detJ (Element.C:362-404):
   // with P = -w detJ J^-1 sigma, f_n,i = sum_k dN_n/dxi_k P_ki
   R P[3][3];
 #pragma unroll
@@ -579,6 +569,8 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
         s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
       P[k][i] = -WxdJ * s;
     }
+  const R a = R(0.57735026918962576451);
+  const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
   const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
   ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
   __syncwarp(amask);
@@ -593,6 +585,190 @@ __global__ void __launch_bounds__(ELEM_THREADS, (sizeof(R) == 4 ? DNL_ELEM_MINB_
       fs.z += grp[l * ROW + g * DIM + 2];
   }
   reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = fs;
+}
+
+// Start of the solve: reference Jacobian detJ0 (ElementPlane.C:96-100,
+// Element3D.C:111-112), initial point state (Element::initializeData,
+// Element.C:258-301) and the element lumped masses (Element::computeMassMatrix,
+// Element.C:304-339) into the slots.  One thread per Gauss point.
+template <typename R, int NPE>
+__global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
+{
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr bool AXI = ElemShape<NPE>::AXI;
+  using R4 = typename V4<R>::type;
+  __shared__ R sh[TILE * ROW];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int g = lane & (NPE - 1);
+  const int base = lane & ~(NPE - 1);
+  const int e = q / NPE;
+  const bool act = e < M.nE;
+  const unsigned amask = __ballot_sync(0xffffffffu, act);
+  if (!act)
+    return;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, e) : 0;
+  const MatDev &mp = M.mat[M.emat[e]];
+  const int node = M.conn[q];
+  R detJ, inv[3][3], radius, H[9];
+  kinematics<R, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H);
+  if (detJ < R(0))
+    raise_status(M.ctl + inst, DNL_ERR_NEG_JACOBIAN, e);
+  R WxdJ = detJ;
+  if constexpr (AXI)
+    WxdJ *= R(6.28318530717958647692) * radius;
+  const R rho0 = R(mp.rho0);
+#pragma unroll
+  for (int c = 0; c < DNL_IP_DETJ0; c++)
+    ipw<R>(M, c, q, R(0));
+  ipw<R>(M, DNL_IP_DETJ0, q, AXI ? detJ * radius : detJ);
+  ipw<R>(M, DNL_IP_T, q, R(mp.T0));
+  ipw<R>(M, DNL_IP_DENSITY, q, rho0);
+  const R a = R(0.57735026918962576451);
+  R *row = sh + threadIdx.x * ROW, *grp = sh + (threadIdx.x - g) * ROW;
+  MassToShared<R, NPE, 0>::run(R(node_sign(g, 0)) * a, R(node_sign(g, 1)) * a, R(node_sign(g, 2)) * a,
+                               rho0 * WxdJ, row);
+  __syncwarp(amask);
+  R m = R(0);
+#pragma unroll
+  for (int l = 0; l < NPE; l++)
+    m += grp[l * ROW + g];
+  R4 s;
+  s.x = m;
+  s.y = s.z = s.w = R(0);
+  reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = s;
+}
+
+// Element pass, one thread per Gauss point, state read straight from global memory.
+template <typename R, int NPE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M)
+{
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  __shared__ R sh[TILE * ROW];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int g = lane & (NPE - 1);
+  const int base = lane & ~(NPE - 1);
+  const int e = q / NPE;
+  const bool valid = e < M.nE;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
+  Ctl *C = M.ctl + inst;
+  const bool act = valid && C->active;
+  const unsigned amask = __ballot_sync(0xffffffffu, act);
+  if (!act)
+    return;
+  GlobalState<R> old{M, q};
+  element_update<R, NPE>(M, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
+                         sh + (threadIdx.x - g) * ROW);
+}
+
+// ----------------------------------------------- bulk-copy (TMA) primitives
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// global -> shared bulk copy completing on an mbarrier (no multicast)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase `parity` of a bulk-copy barrier; false when it
+// did not complete within the limit (the caller flags an error and stops).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+  for (int i = 0; i < (1 << 24); i++)
+    if (mbar_try_wait(bar, parity))
+      return true;
+  return false;
+}
+
+// Element pass as a persistent kernel over tiles of TILE Gauss points: while a
+// block computes one tile, the bulk-copy engine brings the next tile's point
+// state (one contiguous block in the tile-major layout) and connectivity into
+// the other shared-memory buffer.  Results go straight to global memory.
+template <typename R, int NPE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTiles, int *err)
+{
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
+  constexpr uint32_t CONN_BYTES = TILE * sizeof(int);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R *state[2] = {reinterpret_cast<R *>(smem_raw), reinterpret_cast<R *>(smem_raw + STATE_BYTES)};
+  int *conn[2] = {reinterpret_cast<int *>(smem_raw + 2 * STATE_BYTES),
+                  reinterpret_cast<int *>(smem_raw + 2 * STATE_BYTES + CONN_BYTES)};
+  R *rows = reinterpret_cast<R *>(smem_raw + 2 * STATE_BYTES + 2 * CONN_BYTES);
+  __shared__ __align__(8) uint64_t bar[2];
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  const int g = lane & (NPE - 1);
+  const int base = lane & ~(NPE - 1);
+  if (t == 0)
+  {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int tile, int b) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[b], STATE_BYTES + CONN_BYTES);
+    bulk_g2s(state[b], reinterpret_cast<const R *>(M.ip) + (size_t)tile * DNL_IP_NCOMP * TILE, STATE_BYTES, &bar[b]);
+    bulk_g2s(conn[b], M.conn + (size_t)tile * TILE, CONN_BYTES, &bar[b]);
+  };
+  int tile = blockIdx.x;
+  if (t == 0 && tile < nTiles)
+    issue(tile, 0);
+  uint32_t phase[2] = {0, 0};
+  for (int b = 0; tile < nTiles; tile += gridDim.x, b ^= 1)
+  {
+    const int next = tile + gridDim.x;
+    if (t == 0 && next < nTiles)
+      issue(next, b ^ 1);
+    if (!mbar_wait(&bar[b], phase[b]))
+    {
+      atomicExch(err, 1);
+      mbar_wait(&bar[b], phase[b]);
+      return;
+    }
+    phase[b] ^= 1;
+    const int q = tile * TILE + t;
+    const int e = q / NPE;
+    const bool valid = e < M.nE;
+    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
+    Ctl *C = M.ctl + inst;
+    const bool act = valid && C->active;
+    const unsigned amask = __ballot_sync(0xffffffffu, act);
+    if (act)
+    {
+      SharedTile<R> old{state[b], t};
+      element_update<R, NPE>(M, C, q, e, g, base, amask, conn[b][t], old, rows + t * ROW, rows + (t - g) * ROW);
+    }
+    __syncthreads(); // the buffer is refilled two tiles later
+  }
 }
 
 // ------------------------------------------------------------ nodal update

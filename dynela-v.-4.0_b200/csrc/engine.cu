@@ -48,6 +48,12 @@ struct dnl_engine
   long long launches = 0;
   int launchesPerStep = 0;
   bool initialized = false;
+  int nTiles = 0;
+  int variant = 0;          // element-pass kernel variant (see kVariants)
+  bool tuned = false;
+  double variantMs[8] = {0};
+  int *derr = nullptr;      // bulk-copy wait failure flag
+  int numSMs = 0;
   std::string err;
 };
 
@@ -167,31 +173,104 @@ MatDev make_mat(const dnl_material &m)
 
 // ----------------------------------------------------------------- launches
 
-template <typename R> int launch_element(dnl_engine *h, int mode)
+// Element-pass variants the autotuner chooses from: plain (state loaded from
+// global memory) or persistent with bulk-copy staging of each tile, each with
+// its register budget (blocks of TILE threads per SM asked of the compiler).
+struct Variant
 {
-  const int threads = 128;
-  const int blocks = (int)(((long)h->nE * h->npe + threads - 1) / threads);
-  if (h->npe == 8)
-  {
-    if (mode == 0)
-      k_element<R, 8, 0><<<blocks, threads, 0, h->stream>>>(h->M);
-    else
-      k_element<R, 8, 1><<<blocks, threads, 0, h->stream>>>(h->M);
-  }
-  else
-  {
-    if (mode == 0)
-      k_element<R, 4, 0><<<blocks, threads, 0, h->stream>>>(h->M);
-    else
-      k_element<R, 4, 1><<<blocks, threads, 0, h->stream>>>(h->M);
-  }
-  h->launches++;
+  const char *name;
+  int tma;
+  int minb;
+};
+const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4}, {"tma/5", 1, 5}};
+const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2}, {"tma/3", 1, 3}};
+constexpr int kNumVariants = 4;
+
+const Variant &variant_of(const dnl_engine *h, int v)
+{
+  return h->precision == DNL_PREC_MIXED ? kVariantsF32[v] : kVariantsF64[v];
+}
+
+template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
+{
+  const int blocks = (int)(((long)h->nE * NPE + TILE - 1) / TILE);
+  k_element<R, NPE, MINB><<<blocks, TILE, 0, h->stream>>>(h->M);
   return DNL_OK;
+}
+
+template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
+{
+  const size_t smem = 2 * (DNL_IP_NCOMP * TILE * sizeof(R) + TILE * sizeof(int)) + TILE * ElemShape<NPE>::ROW * sizeof(R);
+  static int perSM = -1; // per instantiation
+  if (perSM < 0)
+  {
+    CK(cudaFuncSetAttribute(k_element_tma<R, NPE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_tma<R, NPE, MINB>, TILE, smem));
+    if (perSM < 1)
+      perSM = 1;
+  }
+  const int grid = std::min(h->nTiles, perSM * h->numSMs);
+  k_element_tma<R, NPE, MINB><<<grid, TILE, smem, h->stream>>>(h->M, h->nTiles, h->derr);
+  return DNL_OK;
+}
+
+template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
+{
+  const Variant &vv = variant_of(h, v);
+  if (sizeof(R) == 4)
+  {
+    switch (v)
+    {
+    case 0: return launch_plain<R, NPE, 6>(h);
+    case 1: return launch_plain<R, NPE, 8>(h);
+    case 2: return launch_tma<R, NPE, 4>(h);
+    default: return launch_tma<R, NPE, 5>(h);
+    }
+  }
+  (void)vv;
+  switch (v)
+  {
+  case 0: return launch_plain<R, NPE, 4>(h);
+  case 1: return launch_plain<R, NPE, 3>(h);
+  case 2: return launch_tma<R, NPE, 2>(h);
+  default: return launch_tma<R, NPE, 3>(h);
+  }
 }
 
 int launch_element_any(dnl_engine *h, int mode)
 {
-  return h->precision == DNL_PREC_MIXED ? launch_element<float>(h, mode) : launch_element<double>(h, mode);
+  const int blocks = (int)(((long)h->nE * h->npe + TILE - 1) / TILE);
+  int rc = DNL_OK;
+  if (mode == 1)
+  {
+    if (h->precision == DNL_PREC_MIXED)
+    {
+      if (h->npe == 8)
+        k_element_start<float, 8><<<blocks, TILE, 0, h->stream>>>(h->M);
+      else
+        k_element_start<float, 4><<<blocks, TILE, 0, h->stream>>>(h->M);
+    }
+    else
+    {
+      if (h->npe == 8)
+        k_element_start<double, 8><<<blocks, TILE, 0, h->stream>>>(h->M);
+      else
+        k_element_start<double, 4><<<blocks, TILE, 0, h->stream>>>(h->M);
+    }
+  }
+  else if (h->npe == 4)
+  {
+    // the axisymmetric models are small: one plain variant
+    if (h->precision == DNL_PREC_MIXED)
+      rc = launch_plain<float, 4, 6>(h);
+    else
+      rc = launch_plain<double, 4, 4>(h);
+  }
+  else
+    rc = h->precision == DNL_PREC_MIXED ? launch_variant<float, 8>(h, h->variant)
+                                        : launch_variant<double, 8>(h, h->variant);
+  h->launches++;
+  return rc;
 }
 
 int launch_nodal(dnl_engine *h)
@@ -301,6 +380,10 @@ int sync_ctl(dnl_engine *h)
 
 int check_status(dnl_engine *h)
 {
+  int e = 0;
+  if (cudaMemcpyAsync(&e, h->derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream) == cudaSuccess &&
+      cudaStreamSynchronize(h->stream) == cudaSuccess && e != 0)
+    return fail(h, DNL_ERR_CUDA, "a bulk copy of the element pass did not complete in time");
   for (int i = 0; i < h->nInst; i++)
     if (h->hctl[i].status != 0)
     {
@@ -452,7 +535,9 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   h->nN = (int)x.size();
   h->nE = (int)(conn.size() / h->npe);
   h->nIP = h->nE * h->npe;
-  h->nIPpad = (h->nIP + 31) / 32 * 32;
+  h->nTiles = (h->nIP + TILE - 1) / TILE;
+  h->nIPpad = h->nTiles * TILE;
+  conn.resize((size_t)h->nIPpad, 0); // whole tiles for the bulk copies (padding lanes are inactive)
   h->nSpeed = (int)speedNodes.size();
   h->hasSpeed = h->nSpeed > 0;
   h->nFunc = (int)foff.size() - 1;
@@ -466,13 +551,13 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   // slot of incidence k = e*npe + n in node order; within a node, elements in
   // increasing order (the order of the reference's scatter-add, Model.C:881-898)
   std::vector<int> off(h->nN + 1, 0), pos((size_t)h->nIP);
-  for (size_t k = 0; k < conn.size(); k++)
+  for (size_t k = 0; k < (size_t)h->nIP; k++)
     off[conn[k] + 1]++;
   for (int i = 0; i < h->nN; i++)
     off[i + 1] += off[i];
   {
     std::vector<int> fill(off.begin(), off.end() - 1);
-    for (size_t k = 0; k < conn.size(); k++)
+    for (size_t k = 0; k < (size_t)h->nIP; k++)
       pos[k] = fill[conn[k]]++;
   }
 
@@ -503,7 +588,8 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
       (rc = upload(h, &M.u[0], zeros4)) || (rc = upload(h, &M.u[1], zeros4)) || (rc = upload(h, &M.v[0], v)) ||
       (rc = upload(h, &M.v[1], v)) || (rc = upload(h, &M.a[0], zeros4)) || (rc = upload(h, &M.a[1], zeros4)) ||
       (rc = dalloc(h, &M.mass, h->nN)) || (rc = dalloc(h, &M.fout, h->nN)) ||
-      (rc = upload(h, &M.ctl, h->ctlInit)) || (rc = dalloc(h, &h->denergy, 3 * h->nInst)))
+      (rc = upload(h, &M.ctl, h->ctlInit)) || (rc = dalloc(h, &h->denergy, 3 * h->nInst)) ||
+      (rc = dalloc(h, &h->derr, 1)))
   {
     std::string e = h->err;
     dnl_engine_destroy(h);
@@ -535,6 +621,9 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.foff = d_foff;
   M.ip = ip;
   M.slot = slot;
+  cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
+  cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream);
+  h->variant = 0;
   if (cudaMallocHost((void **)&h->hctl, sizeof(Ctl) * h->nInst) != cudaSuccess)
   {
     dnl_engine_destroy(h);
@@ -901,21 +990,25 @@ int dnl_engine_get_ips(dnl_engine *h, double *out)
 {
   if (!h || !out)
     return DNL_ERR_ARG;
-  CK(cudaStreamSynchronize(h->stream));
-  const size_t n = (size_t)h->nIP;
+  const size_t n = (size_t)h->nIP, total = (size_t)DNL_IP_NCOMP * h->nIPpad;
+  int rc;
   if (h->precision == DNL_PREC_MIXED)
   {
-    std::vector<float> tmp((size_t)DNL_IP_NCOMP * h->nIPpad);
-    { int rc_ = copy(h, tmp.data(), h->M.ip, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost); if (rc_) return rc_; }
+    std::vector<float> tmp(total);
+    if ((rc = copy(h, tmp.data(), h->M.ip, total * sizeof(float), cudaMemcpyDeviceToHost)))
+      return rc;
     for (int c = 0; c < DNL_IP_NCOMP; c++)
       for (size_t q = 0; q < n; q++)
-        out[c * n + q] = tmp[(size_t)c * h->nIPpad + q];
+        out[c * n + q] = tmp[ip_index(c, (int)q)];
   }
   else
   {
+    std::vector<double> tmp(total);
+    if ((rc = copy(h, tmp.data(), h->M.ip, total * sizeof(double), cudaMemcpyDeviceToHost)))
+      return rc;
     for (int c = 0; c < DNL_IP_NCOMP; c++)
-      { int rc_ = copy(h, out + c * n, (double *)h->M.ip + (size_t)c * h->nIPpad, n * sizeof(double),
-                    cudaMemcpyDeviceToHost); if (rc_) return rc_; }
+      for (size_t q = 0; q < n; q++)
+        out[c * n + q] = tmp[ip_index(c, (int)q)];
   }
   return DNL_OK;
 }
@@ -924,23 +1017,20 @@ int dnl_engine_set_ips(dnl_engine *h, const double *in)
 {
   if (!h || !in)
     return DNL_ERR_ARG;
-  CK(cudaStreamSynchronize(h->stream));
-  const size_t n = (size_t)h->nIP;
+  const size_t n = (size_t)h->nIP, total = (size_t)DNL_IP_NCOMP * h->nIPpad;
   if (h->precision == DNL_PREC_MIXED)
   {
-    std::vector<float> tmp((size_t)DNL_IP_NCOMP * h->nIPpad, 0.0f);
+    std::vector<float> tmp(total, 0.0f);
     for (int c = 0; c < DNL_IP_NCOMP; c++)
       for (size_t q = 0; q < n; q++)
-        tmp[(size_t)c * h->nIPpad + q] = (float)in[c * n + q];
-    { int rc_ = copy(h, h->M.ip, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice); if (rc_) return rc_; }
+        tmp[ip_index(c, (int)q)] = (float)in[c * n + q];
+    return copy(h, h->M.ip, tmp.data(), total * sizeof(float), cudaMemcpyHostToDevice);
   }
-  else
-  {
-    for (int c = 0; c < DNL_IP_NCOMP; c++)
-      { int rc_ = copy(h, (double *)h->M.ip + (size_t)c * h->nIPpad, in + c * n, n * sizeof(double),
-                    cudaMemcpyHostToDevice); if (rc_) return rc_; }
-  }
-  return DNL_OK;
+  std::vector<double> tmp(total, 0.0);
+  for (int c = 0; c < DNL_IP_NCOMP; c++)
+    for (size_t q = 0; q < n; q++)
+      tmp[ip_index(c, (int)q)] = in[c * n + q];
+  return copy(h, h->M.ip, tmp.data(), total * sizeof(double), cudaMemcpyHostToDevice);
 }
 
 int dnl_engine_energies(dnl_engine *h, int32_t i, double out[3])
@@ -964,6 +1054,124 @@ int dnl_engine_energies(dnl_engine *h, int32_t i, double out[3])
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, h->denergy + 3 * i, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return DNL_OK;
+}
+
+// Element-pass autotuner: time every kernel variant over `steps` increments
+// started from the same saved state, keep the fastest, and restore the state,
+// so the simulation is left exactly where it was.
+int dnl_engine_autotune(dnl_engine *h, int32_t steps)
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  if (!h->initialized)
+    return fail(h, DNL_ERR_ARG, "dnl_engine_init must be called first");
+  if (h->npe != 8 || steps <= 0)
+    return DNL_OK;
+  const size_t rsz = h->precision == DNL_PREC_MIXED ? 4 : 8;
+  const size_t ipBytes = (size_t)DNL_IP_NCOMP * h->nIPpad * rsz, nb = sizeof(double4) * h->nN;
+  struct Saved
+  {
+    void *dst;
+    const void *src;
+    size_t bytes;
+  };
+  std::vector<Saved> parts = {{nullptr, h->M.ip, ipBytes},      {nullptr, h->M.x, nb},      {nullptr, h->M.disp, nb},
+                              {nullptr, h->M.u[0], nb},        {nullptr, h->M.u[1], nb},   {nullptr, h->M.v[0], nb},
+                              {nullptr, h->M.v[1], nb},        {nullptr, h->M.a[0], nb},   {nullptr, h->M.a[1], nb},
+                              {nullptr, h->M.ctl, sizeof(Ctl) * h->nInst}};
+  size_t total = 0;
+  for (auto &p : parts)
+    total += (p.bytes + 255) / 256 * 256;
+  char *save = nullptr;
+  if (cudaMalloc((void **)&save, total) != cudaSuccess)
+    return fail(h, DNL_ERR_CUDA, "autotune: no room for the state snapshot (%zu bytes)", total);
+  size_t off = 0;
+  for (auto &p : parts)
+  {
+    p.dst = save + off;
+    off += (p.bytes + 255) / 256 * 256;
+    CK(cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int best = 0;
+  double bestMs = 1e30;
+  for (int v = 0; v < kNumVariants; v++)
+  {
+    for (auto &p : parts)
+      CK(cudaMemcpyAsync(const_cast<void *>(p.src), p.dst, p.bytes, cudaMemcpyDeviceToDevice, h->stream));
+    h->variant = v;
+    launch_control(h, CTL_LIMITS, 1e300, steps);
+    double ms = 0.0;
+    for (int k = 0; k < steps; k++)
+    {
+      launch_bc_prep(h);
+      CK(cudaEventRecord(e0, h->stream));
+      launch_element_any(h, 0);
+      CK(cudaEventRecord(e1, h->stream));
+      launch_nodal(h);
+      launch_courant(h, 0);
+      launch_control(h, CTL_FINISH);
+      CK(cudaEventSynchronize(e1));
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (k > 0 || steps == 1)
+        ms += t;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    ms /= (steps > 1 ? steps - 1 : 1);
+    h->variantMs[v] = ms;
+    if (ms < bestMs)
+    {
+      bestMs = ms;
+      best = v;
+    }
+  }
+  for (auto &p : parts)
+    CK(cudaMemcpyAsync(const_cast<void *>(p.src), p.dst, p.bytes, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  cudaFree(save);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->variant = best;
+  h->tuned = true;
+  if (h->graphExec)
+  {
+    cudaGraphExecDestroy(h->graphExec);
+    cudaGraphDestroy(h->graph);
+    h->graphExec = nullptr;
+    h->graph = nullptr;
+  }
+  return check_status(h);
+}
+
+int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[4])
+{
+  if (!h)
+    return DNL_ERR_ARG;
+  if (variant)
+    *variant = h->variant;
+  if (ms)
+    for (int v = 0; v < kNumVariants; v++)
+      ms[v] = h->variantMs[v];
+  return DNL_OK;
+}
+
+int dnl_engine_set_variant(dnl_engine *h, int32_t variant)
+{
+  if (!h || variant < 0 || variant >= kNumVariants)
+    return DNL_ERR_ARG;
+  h->variant = variant;
+  if (h->graphExec)
+  {
+    cudaGraphExecDestroy(h->graphExec);
+    cudaGraphDestroy(h->graph);
+    h->graphExec = nullptr;
+    h->graph = nullptr;
+  }
   return DNL_OK;
 }
 

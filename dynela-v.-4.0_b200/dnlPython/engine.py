@@ -95,6 +95,20 @@ class Engine:
         self._check(self._lib.dnl_engine_timings(self.h, _pd(out)))
         return dict(element_ms=out[0], nodal_ms=out[1], timestep_ms=out[2], run_ms=out[3])
 
+    def autotune(self, steps=8):
+        """Pick the fastest element-pass variant; the simulation state is unchanged."""
+        self._check(self._lib.dnl_engine_autotune(self.h, int(steps)))
+        return self.variant()
+
+    def variant(self):
+        v = ctypes.c_int32()
+        ms = np.zeros(4)
+        self._check(self._lib.dnl_engine_variant(self.h, ctypes.byref(v), _pd(ms)))
+        return v.value, ms
+
+    def set_variant(self, v):
+        self._check(self._lib.dnl_engine_set_variant(self.h, int(v)))
+
     def launch_count(self):
         return int(self._lib.dnl_engine_launch_count(self.h))
 

@@ -209,6 +209,17 @@ int dnl_engine_timings(const dnl_engine *h, double out[4]);
 /* Number of kernel launches issued on the device by the last run call. */
 int64_t dnl_engine_launch_count(const dnl_engine *h);
 
+/* Element-pass autotuner (hex8 models): times each kernel variant (register
+ * budget, plain or bulk-copy-staged persistent tiles) over `steps` increments
+ * run from a saved copy of the state, keeps the fastest for the following runs
+ * and restores the state.  No counterpart in the reference (its element loop
+ * has one implementation). */
+int dnl_engine_autotune(dnl_engine *h, int32_t steps);
+/* Variant in use and the element-pass time (ms) the autotuner measured for each. */
+int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[4]);
+/* Force an element-pass variant (0..3). */
+int dnl_engine_set_variant(dnl_engine *h, int32_t variant);
+
 #ifdef __cplusplus
 }
 #endif

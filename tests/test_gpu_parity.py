@@ -210,3 +210,33 @@ def test_inverted_element_raises_status():
             e.run(max_incs=3)
         assert ei.value.code == -3
         assert e.control()["status"] == -3
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_element_variants_agree_and_autotune_keeps_state(precision):
+    """Every element-pass variant the autotuner may pick (register budgets,
+    plain or bulk-copy-staged tiles) computes the same increments (to the
+    rounding of the compiler's fused multiply-add choices), and autotuning
+    leaves the simulation state untouched."""
+    d = meshes.taylor_3d(n_core=4, n_ring=3, n_axial=40, precision=precision)
+    results = []
+    for v in range(4):
+        with engine(d) as e:
+            e.init()
+            e.set_variant(v)
+            e.run(max_incs=25)
+            results.append((e.nodes(_abi.NODE_COORDS), e.ips()))
+    xtol, iptol = (1e-12, 1e-8) if precision == _abi.PREC_FP64 else (1e-7, 1e-3)
+    for x, ip in results[1:]:
+        ex, eip = helpers.rel_err(x, results[0][0]), helpers.field_errors(ip, results[0][1]).max()
+        assert ex < xtol and eip < iptol, (ex, eip)
+    with engine(d) as e:
+        e.init()
+        e.run(max_incs=5)
+        before = (e.nodes(_abi.NODE_COORDS), e.ips(), e.control())
+        v, ms = e.autotune(steps=3)
+        assert 0 <= v < 4 and (ms > 0).all()
+        assert np.array_equal(e.nodes(_abi.NODE_COORDS), before[0]) and np.array_equal(e.ips(), before[1])
+        assert e.control()["increment"] == before[2]["increment"]
+        e.run(max_incs=20)
+        assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), results[0][0]) < xtol
