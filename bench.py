@@ -149,6 +149,23 @@ class ClockSampler:
 
 # -------------------------------------------------------------- CPU baseline
 
+class quiet_stdout:
+    """Send the C-level stdout to /dev/null (the reference prints progress
+    lines; the bench prints exactly one JSON line)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.null)
+        os.close(self.saved)
+
+
 def reference_rate(desc, steps, warmup, threads):
     """The DynELA reference (oracle/_ref) on the host cores: elem-steps/s of
     `steps` increments after `warmup` ones, from its own solver-loop clock.
@@ -157,16 +174,17 @@ def reference_rate(desc, steps, warmup, threads):
     import ref
     if not ref.available():
         return None
-    r = ref.RefModel(desc.copy(precision=0), threads=threads)
-    try:
-        r.init()
-        if warmup:
-            r.run(max_incs=warmup)
-        s0 = r.solver_seconds()
-        n = r.run(max_incs=steps)
-        sec = r.solver_seconds() - s0
-    finally:
-        r.close()
+    with quiet_stdout():
+        r = ref.RefModel(desc.copy(precision=0), threads=threads)
+        try:
+            r.init()
+            if warmup:
+                r.run(max_incs=warmup)
+            s0 = r.solver_seconds()
+            n = r.run(max_incs=steps)
+            sec = r.solver_seconds() - s0
+        finally:
+            r.close()
     return desc.n_elems * n / sec, "reference", threads, \
         f"{n} increments of the full {desc.n_elems}-element mesh from t=0 after {warmup} warm-up increments, " \
         f"FP64, OpenMP {threads} threads (model build and start of the solve excluded)"

@@ -22,6 +22,10 @@
 
 namespace dnl
 {
+// internal linkage: every translation unit that includes this header gets its
+// own copy of the kernels and helpers
+namespace
+{
 
 // Per-instance solver state, resident on the device.
 struct __align__(128) Ctl
@@ -323,6 +327,22 @@ template <int NPE> struct ElemShape
   static constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
 };
 
+// How the element update reaches nodes, materials and its outputs in the
+// engine's own arrays (tile-major point state, node-ordered force slots).
+template <typename R> struct EngineIo
+{
+  using R4 = typename V4<R>::type;
+  const DevModel &M;
+  int q, f0;
+  __device__ __forceinline__ double4 x(int n) const { return M.x[n]; }
+  __device__ __forceinline__ double4 u(int n) const { return M.u[f0][n]; }
+  __device__ __forceinline__ const MatDev &mat(int e) const { return M.mat[M.emat[e]]; }
+  __device__ __forceinline__ const MatDev *matp(int e) const { return M.mat + M.emat[e]; }
+  __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
+  __device__ __forceinline__ void slot(const R4 &v) const { reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = v; }
+  __device__ __forceinline__ const float *ip32() const { return reinterpret_cast<const float *>(M.ip); }
+};
+
 // Where the element update reads the old point state from: global memory, or
 // the tile staged in shared memory by the bulk copies.
 template <typename R> struct GlobalState
@@ -425,20 +445,18 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
 // radial return, final rotation, density, and the element's nodal forces,
 // summed over its points through shared memory and stored in node order.
 // `row` is this lane's shared-memory row, `grp` the row of the element's first lane.
-template <typename R, int NPE, class Src>
-__device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q, int e, int g, int base,
-                                               unsigned amask, int node, const Src &old, R *row, R *grp)
+template <typename R, int NPE, class Src, class Io>
+__device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int e, int g, int base, unsigned amask,
+                                               int node, const Src &old, R *row, R *grp)
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
   constexpr bool AXI = ElemShape<NPE>::AXI;
   constexpr int ROW = ElemShape<NPE>::ROW;
   using R4 = typename V4<R>::type;
-  const int f0 = C->f0;
   const double dt = C->dt_eff;
-  const int mi = M.emat[e];
-  const MatDev &mp = M.mat[mi];
-  const double4 X = M.x[node];
-  const double4 U = M.u[f0][node];
+  const MatDev &mp = io.mat(e);
+  const double4 X = io.x(node);
+  const double4 U = io.u(node);
 
   R detJ, inv[3][3], radius, dE[6], Rot[9];
   {
@@ -464,7 +482,7 @@ __device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q,
     rotate_sym<R>(Rot, strain);
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      ipw<R>(M, DNL_IP_STRAIN + c, q, strain[c]);
+      io.put(DNL_IP_STRAIN + c, strain[c]);
   }
 
   // the rotation and J^-1 wait in shared memory while the return holds its registers
@@ -499,8 +517,8 @@ __device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q,
       if constexpr (sizeof(R) == 4)
       {
         atomicAdd(&C->resolves, 1);
-        const Resolved r = resolve_fp64(reinterpret_cast<const float *>(M.ip), q, M.mat + mi, dE[0], dE[1], dE[2],
-                                        dE[3], dE[4], dE[5], dt, st.pressure);
+        const Resolved r = resolve_fp64(io.ip32(), q, io.matp(e), dE[0], dE[1], dE[2], dE[3], dE[4], dE[5], dt,
+                                        st.pressure);
         if (!r.ok)
           raise_status(C, DNL_ERR_NEWTON, q);
 #pragma unroll
@@ -535,7 +553,7 @@ __device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q,
     rotate_sym<R>(Rot, ep);
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      ipw<R>(M, DNL_IP_PLASTIC_STRAIN + c, q, ep[c]);
+      io.put(DNL_IP_PLASTIC_STRAIN + c, ep[c]);
   }
   rotate_sym<R>(Rot, st.s);
   R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
@@ -543,17 +561,17 @@ __device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q,
     rho /= radius;
 #pragma unroll
   for (int c = 0; c < 6; c++)
-    ipw<R>(M, DNL_IP_STRESS + c, q, st.s[c]);
-  ipw<R>(M, DNL_IP_EPSP, q, st.epsp);
-  ipw<R>(M, DNL_IP_DEPSP, q, st.depsp);
-  ipw<R>(M, DNL_IP_GAMMA, q, st.gamma);
-  ipw<R>(M, DNL_IP_GAMMA_CUM, q, st.gcum);
-  ipw<R>(M, DNL_IP_YIELD, q, st.yield);
-  ipw<R>(M, DNL_IP_T, q, st.T);
-  ipw<R>(M, DNL_IP_PRESSURE, q, st.pressure);
-  ipw<R>(M, DNL_IP_EINT, q, st.eint);
-  ipw<R>(M, DNL_IP_EINEL, q, st.einel);
-  ipw<R>(M, DNL_IP_DENSITY, q, rho);
+    io.put(DNL_IP_STRESS + c, st.s[c]);
+  io.put(DNL_IP_EPSP, st.epsp);
+  io.put(DNL_IP_DEPSP, st.depsp);
+  io.put(DNL_IP_GAMMA, st.gamma);
+  io.put(DNL_IP_GAMMA_CUM, st.gcum);
+  io.put(DNL_IP_YIELD, st.yield);
+  io.put(DNL_IP_T, st.T);
+  io.put(DNL_IP_PRESSURE, st.pressure);
+  io.put(DNL_IP_EINT, st.eint);
+  io.put(DNL_IP_EINEL, st.einel);
+  io.put(DNL_IP_DENSITY, rho);
 
   // internal forces f_n = -sum_g dN_n/dx . sigma w detJ (Element.C:362-404):
   // with P = -w detJ J^-1 sigma, f_n,i = sum_k dN_n/dxi_k P_ki
@@ -584,7 +602,7 @@ __device__ __forceinline__ void element_update(const DevModel &M, Ctl *C, int q,
     if constexpr (DIM == 3)
       fs.z += grp[l * ROW + g * DIM + 2];
   }
-  reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = fs;
+  io.slot(fs);
 }
 
 // Start of the solve: reference Jacobian detJ0 (ElementPlane.C:96-100,
@@ -658,7 +676,8 @@ __global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M)
   if (!act)
     return;
   GlobalState<R> old{M, q};
-  element_update<R, NPE>(M, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
+  EngineIo<R> io{M, q, C->f0};
+  element_update<R, NPE>(io, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
                          sh + (threadIdx.x - g) * ROW);
 }
 
@@ -765,7 +784,8 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
     if (act)
     {
       SharedTile<R> old{state[b], t};
-      element_update<R, NPE>(M, C, q, e, g, base, amask, conn[b][t], old, rows + t * ROW, rows + (t - g) * ROW);
+      EngineIo<R> io{M, q, C->f0};
+      element_update<R, NPE>(io, C, q, e, g, base, amask, conn[b][t], old, rows + t * ROW, rows + (t - g) * ROW);
     }
     __syncthreads(); // the buffer is refilled two tiles later
   }
@@ -1159,4 +1179,5 @@ __global__ void k_energies(DevModel M, double *out /* [nInst*3] */, int speed_fi
       out[3 * inst + k] = sh[k][0];
 }
 
+} // namespace
 } // namespace dnl

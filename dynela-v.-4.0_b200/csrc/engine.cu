@@ -57,6 +57,9 @@ struct dnl_engine
   std::string err;
 };
 
+// error text of the entry points that have no handle (static_pass.cu)
+void dnl_internal_set_error(const char *msg) { snprintf(g_create_err, sizeof(g_create_err), "%s", msg); }
+
 namespace
 {
 int fail(dnl_engine *h, int code, const char *fmt, ...)
