@@ -220,6 +220,31 @@ int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[4]);
 /* Force an element-pass variant (0..3). */
 int dnl_engine_set_variant(dnl_engine *h, int32_t variant);
 
+/* Element pass that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc (a host application
+ * whose own memory manager owns the GPU, or code between stream captures where
+ * an allocation would synchronize the device): every input and output is a
+ * caller-owned device array, and the scratch (per element-node force slots,
+ * node -> slot lists, a control block) is a static device array of about
+ * 5.3 MB that every GPU loading the library keeps until the process exits.
+ * One call = strains, pressure, radial return, final rotation, density and the
+ * nodal internal forces (the same element pass as dnl_engine_element_pass) in
+ * FP64 for a model of at most DNL_STATIC_MAX_ELEMS elements and
+ * DNL_STATIC_MAX_NODES nodes; larger sizes return DNL_ERR_ARG.
+ *   d_coords, d_du [n_nodes*3]: current coordinates and displacement increment
+ *   d_conn [n_elems*nodes_per_element]: 0-based connectivity
+ *   d_ips [DNL_IP_NCOMP*n_ips] FP64 component-major point state, updated in place
+ *   d_force [n_nodes*3]: assembled internal forces (output)
+ *   stream: a cudaStream_t (NULL: the default stream); the call waits for it at the end.
+ * The first call on a device looks up the scratch address: make it before any
+ * stream capture.  All calls share the scratch, so calls that overlap on the
+ * GPU (other streams, other threads) race: serialise them. */
+#define DNL_STATIC_MAX_ELEMS 16384
+#define DNL_STATIC_MAX_NODES 65536
+int dnl_element_pass_static(int32_t elem_type, int32_t n_nodes, int32_t n_elems, const double *d_coords,
+                            const double *d_du, const int32_t *d_conn, const dnl_material *material,
+                            double time_step, double *d_ips, double *d_force, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
