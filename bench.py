@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="element-pass variant (0-3); default: chosen by the autotuner")
     p.add_argument("--axial", type=int, default=160,
                    help="axial element layers (160 = the measured workload; fewer for profiling captures)")
     return p.parse_args()
@@ -255,7 +257,11 @@ def run_engine_arm(args, rank, world, dist):
     desc = workload(args.precision)
     word = 4 if args.precision == "mixed" else 8
     eng = Engine(desc).init()
-    variant, variant_ms = eng.autotune(steps=6)  # leaves the state unchanged
+    if args.variant >= 0:
+        eng.set_variant(args.variant)
+        variant, variant_ms = eng.variant()
+    else:
+        variant, variant_ms = eng.autotune(steps=6)  # leaves the state unchanged
     if args.warmup:
         eng.run(max_incs=args.warmup)
 
