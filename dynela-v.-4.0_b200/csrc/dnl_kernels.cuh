@@ -17,6 +17,8 @@
 //                nodal pass reads its node's run of slots
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "dnl_math.cuh"
 #include "dnlgpu.h"
 
@@ -38,7 +40,8 @@ struct __align__(128) Ctl
   int status, bad, resolves, ts_freq;
   double safety, omegaS, alphaM, beta, gammaN;
   int elem_begin, elem_end, node_begin, node_end;
-  int ts_method, fun_time_base, pad0, pad1;
+  int ts_method, pi_iters, pad0, pad1;
+  double pi_fmax, pi_omega; // power iteration: Model::_powerIterationFreqMax, last omega_max
 };
 
 static constexpr unsigned long long INF_BITS = 0x7ff0000000000000ull;
@@ -70,6 +73,10 @@ struct DevModel
   const double *fx, *fy;   // packed function points
   const int *foff;         // [nFunc+1]
   double4 *fout;           // assembled forces (kernel-level entry point)
+  // power-iteration time step (single-model engines)
+  double *pv, *pv2;        // [nN*3] iteration vectors (dof = 3 node + component)
+  double4 *pislot;         // [nE*npe] element K v contributions, node order
+  double *blockmax;        // [gridDim] per-block max |v|
 };
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
@@ -1056,6 +1063,222 @@ __global__ void __launch_bounds__(256) k_courant(DevModel M, int force)
     atomicMin(&C->min_bits, (unsigned long long)__double_as_longlong(ratio));
 }
 
+// ------------------------------------------------- power-iteration time step
+
+// K_e v_e of one element at this lane's Gauss point, added over the element's
+// points through shared memory (ElementPlane.C:182-292, Element3D.C:303-399,
+// applied without forming K_e): eps = B v (Voigt, engineering shear), sig = C eps
+// with the Hooke matrices of Material.C:98-152 (shear modulus term E/(1+nu)),
+// y_n = B_n^T sig w detJ (x 2 pi r, + the hoop row for axisymmetric elements).
+template <int NPE>
+__device__ __forceinline__ void element_Kv(const DevModel &M, int q, int e, int g, int base, unsigned amask,
+                                           const double *v, double scale, double *row, double *grp)
+{
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  constexpr bool AXI = ElemShape<NPE>::AXI;
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  const int node = M.conn[q];
+  const MatDev &mp = M.mat[M.emat[e]];
+  double detJ, inv[3][3], radius, H[9];
+  kinematics<double, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H);
+  double WxdJ = detJ;
+  if constexpr (AXI)
+    WxdJ *= 6.28318530717958647692 * radius;
+  const double vx = v[3 * node] * scale, vy = v[3 * node + 1] * scale, vz = DIM == 3 ? v[3 * node + 2] * scale : 0.0;
+  const double a = 0.57735026918962576451;
+  const double xi0 = node_sign(g, 0) * a, xi1 = node_sign(g, 1) * a, xi2 = node_sign(g, 2) * a;
+  // strains of B v
+  double eps[6] = {0, 0, 0, 0, 0, 0};
+  double dNx[NPE][3], Nv[NPE];
+#pragma unroll
+  for (int n = 0; n < NPE; n++)
+  {
+    double dxi[3], Nn;
+    switch (n)
+    {
+#define DNL_SHAPE_CASE(K)                                                                                          \
+  case K:                                                                                                          \
+    shape<double, NPE, (K < NPE ? K : 0)>(xi0, xi1, xi2, dxi, Nn);                                                  \
+    break;
+      DNL_SHAPE_CASE(0) DNL_SHAPE_CASE(1) DNL_SHAPE_CASE(2) DNL_SHAPE_CASE(3) DNL_SHAPE_CASE(4) DNL_SHAPE_CASE(5)
+      DNL_SHAPE_CASE(6) DNL_SHAPE_CASE(7)
+#undef DNL_SHAPE_CASE
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+    {
+      double s_ = 0.0;
+#pragma unroll
+      for (int j = 0; j < DIM; j++)
+        s_ += dxi[j] * inv[j][k];
+      dNx[n][k] = (k < DIM) ? s_ : 0.0;
+    }
+    Nv[n] = Nn;
+    const double ux = __shfl_sync(amask, vx, base + n), uy = __shfl_sync(amask, vy, base + n),
+                 uz = DIM == 3 ? __shfl_sync(amask, vz, base + n) : 0.0;
+    if constexpr (DIM == 3)
+    {
+      eps[0] += dNx[n][0] * ux;
+      eps[1] += dNx[n][1] * uy;
+      eps[2] += dNx[n][2] * uz;
+      eps[3] += dNx[n][1] * ux + dNx[n][0] * uy;
+      eps[4] += dNx[n][2] * uy + dNx[n][1] * uz;
+      eps[5] += dNx[n][2] * ux + dNx[n][0] * uz;
+    }
+    else
+    {
+      eps[0] += dNx[n][0] * ux;
+      eps[1] += dNx[n][1] * uy;
+      eps[2] += dNx[n][1] * ux + dNx[n][0] * uy;
+      eps[3] += Nn / radius * ux;
+    }
+  }
+  const double E = mp.young, nu = mp.poisson, f = E / ((1 + nu) * (1 - 2 * nu));
+  const double cd = (1 - nu) * f, co = nu * f, cs = (1 - 2 * nu) * f;
+  double sig[6];
+  if constexpr (DIM == 3)
+  {
+    sig[0] = cd * eps[0] + co * (eps[1] + eps[2]);
+    sig[1] = cd * eps[1] + co * (eps[0] + eps[2]);
+    sig[2] = cd * eps[2] + co * (eps[0] + eps[1]);
+    sig[3] = cs * eps[3];
+    sig[4] = cs * eps[4];
+    sig[5] = cs * eps[5];
+  }
+  else
+  {
+    sig[0] = cd * eps[0] + co * (eps[1] + eps[3]);
+    sig[1] = cd * eps[1] + co * (eps[0] + eps[3]);
+    sig[2] = cs * eps[2];
+    sig[3] = cd * eps[3] + co * (eps[0] + eps[1]);
+  }
+#pragma unroll
+  for (int n = 0; n < NPE; n++)
+  {
+    if constexpr (DIM == 3)
+    {
+      row[n * 3] = (dNx[n][0] * sig[0] + dNx[n][1] * sig[3] + dNx[n][2] * sig[5]) * WxdJ;
+      row[n * 3 + 1] = (dNx[n][1] * sig[1] + dNx[n][0] * sig[3] + dNx[n][2] * sig[4]) * WxdJ;
+      row[n * 3 + 2] = (dNx[n][2] * sig[2] + dNx[n][1] * sig[4] + dNx[n][0] * sig[5]) * WxdJ;
+    }
+    else
+    {
+      row[n * 2] = (dNx[n][0] * sig[0] + dNx[n][1] * sig[2] + Nv[n] / radius * sig[3]) * WxdJ;
+      row[n * 2 + 1] = (dNx[n][1] * sig[1] + dNx[n][0] * sig[2]) * WxdJ;
+    }
+  }
+  __syncwarp(amask);
+  double4 y = make_double4(0, 0, 0, 0);
+#pragma unroll
+  for (int l = 0; l < NPE; l++)
+  {
+    y.x += grp[l * ROW + g * DIM];
+    y.y += grp[l * ROW + g * DIM + 1];
+    if constexpr (DIM == 3)
+      y.z += grp[l * ROW + g * DIM + 2];
+  }
+  M.pislot[M.slot_pos[q]] = y;
+}
+
+// Model::computePowerIterationTimeStep (Model.C:942-1009) for a single model,
+// as one cooperative kernel: each iteration is an element phase (K v into the
+// slots), a grid barrier, a node phase (v_new = (v + sum of the node's slots in
+// element order) / m, block maxima of |v_new|), a grid barrier and the
+// convergence test |fmax - fmax_prev| / fmax < 1e-4, at most 1000 iterations.
+// v is kept unnormalised between iterations (scale = 1 / fmax).  Runs only
+// when the time step is due (or forced at the start).
+template <int NPE>
+__global__ void __launch_bounds__(TILE) k_power_iteration(DevModel M, int force)
+{
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  __shared__ double sh[TILE * ROW];
+  __shared__ double red[TILE / 32];
+  Ctl *C = M.ctl;
+  if (!(force || (C->active && C->due)))
+    return;
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  const int t = threadIdx.x, lane = t & 31;
+  const int g = lane & (NPE - 1), base = lane & ~(NPE - 1);
+  const int nTiles = (M.nE * NPE + TILE - 1) / TILE;
+  double *v = M.pv, *vn = M.pv2;
+  double scale = 1.0, fprev = C->pi_fmax, fmx = 0.0;
+  int it = 0;
+  bool ok = false;
+  while (!ok)
+  {
+    it++;
+    for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x)
+    {
+      const int q = tile * TILE + t, e = q / NPE;
+      const bool act = e < M.nE;
+      const unsigned amask = __ballot_sync(0xffffffffu, act);
+      if (act)
+        element_Kv<NPE>(M, q, e, g, base, amask, v, scale, sh + t * ROW, sh + (t - g) * ROW);
+      __syncwarp();
+    }
+    grid.sync();
+    double lmax = 0.0;
+    for (int i = blockIdx.x * blockDim.x + t; i < M.nN; i += gridDim.x * blockDim.x)
+    {
+      double acc[3] = {v[3 * i] * scale, v[3 * i + 1] * scale, v[3 * i + 2] * scale};
+      for (int k = M.csr_off[i]; k < M.csr_off[i + 1]; k++)
+      {
+        const double4 y = M.pislot[k];
+        acc[0] += y.x;
+        acc[1] += y.y;
+        acc[2] += y.z;
+      }
+      const double m = M.mass[i];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+      {
+        const double val = (c < DIM) ? acc[c] / m : 0.0;
+        vn[3 * i + c] = val;
+        lmax = fmax(lmax, fabs(val));
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
+    if (lane == 0)
+      red[t / 32] = lmax;
+    __syncthreads();
+    if (t == 0)
+    {
+      double b = 0.0;
+      for (int w = 0; w < TILE / 32; w++)
+        b = fmax(b, red[w]);
+      M.blockmax[blockIdx.x] = b;
+    }
+    grid.sync();
+    fmx = 0.0;
+    for (int b = 0; b < (int)gridDim.x; b++)
+      fmx = fmax(fmx, M.blockmax[b]);
+    ok = fabs(fmx - fprev) / fmx < 1e-4;
+    fprev = fmx;
+    scale = 1.0 / fmx;
+    double *tmp = v;
+    v = vn;
+    vn = tmp;
+    if (it > 1000 && !ok)
+    {
+      if (blockIdx.x == 0 && t == 0)
+        raise_status(C, DNL_ERR_POWER_ITERATION, it);
+      return;
+    }
+  }
+  // keep the normalised vector and the frequency for the next call (warm start)
+  for (int i = blockIdx.x * blockDim.x + t; i < 3 * M.nN; i += gridDim.x * blockDim.x)
+    M.pv[i] = v[i] * scale;
+  if (blockIdx.x == 0 && t == 0)
+  {
+    C->pi_fmax = fmx;
+    C->pi_omega = sqrt(fmx);
+    C->pi_iters += it;
+  }
+}
+
 // ---------------------------------------------------------------- control
 
 enum
@@ -1088,9 +1311,15 @@ __device__ __forceinline__ void begin_increment(Ctl &c)
 
 __device__ __forceinline__ void apply_courant(Ctl &c)
 {
-  // Solver::computeTimeStep (Solver.C:205-226): omega_max = 2 / dt_crit
-  const double crit = __longlong_as_double((long long)c.min_bits);
-  c.dt = c.safety * c.omegaS / (2.0 / crit);
+  // Solver::computeTimeStep (Solver.C:205-226): omega_max = 2 / dt_crit, or
+  // the power-iteration omega_max (Model.C:1008)
+  if (c.ts_method == DNL_TS_POWER_ITERATION)
+    c.dt = c.safety * c.omegaS / c.pi_omega;
+  else
+  {
+    const double crit = __longlong_as_double((long long)c.min_bits);
+    c.dt = c.safety * c.omegaS / (2.0 / crit);
+  }
   c.min_bits = INF_BITS;
 }
 

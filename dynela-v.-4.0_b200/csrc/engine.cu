@@ -54,6 +54,8 @@ struct dnl_engine
   double variantMs[8] = {0};
   int *derr = nullptr;      // bulk-copy wait failure flag
   int numSMs = 0;
+  bool powerIteration = false;
+  int piGrid = 0;
   std::string err;
 };
 
@@ -125,9 +127,8 @@ int check_desc(const dnl_model_desc *d, int idx)
     return fail(nullptr, DNL_ERR_ARG, "model %d: empty mesh", idx);
   if (d->n_materials <= 0 || !d->materials)
     return fail(nullptr, DNL_ERR_ARG, "model %d: no material", idx);
-  if (d->ts_method != DNL_TS_COURANT)
-    return fail(nullptr, DNL_ERR_UNSUPPORTED, "model %d: only the Courant time step is available on the GPU path",
-                idx);
+  if (d->ts_method != DNL_TS_COURANT && d->ts_method != DNL_TS_POWER_ITERATION)
+    return fail(nullptr, DNL_ERR_UNSUPPORTED, "model %d: unknown time-step method %d", idx, d->ts_method);
   if (d->precision != DNL_PREC_FP64 && d->precision != DNL_PREC_MIXED)
     return fail(nullptr, DNL_ERR_ARG, "model %d: unknown precision %d", idx, d->precision);
   const int npe = npe_of(d->elem_type);
@@ -347,13 +348,39 @@ int launch_bc_prep(dnl_engine *h)
   return DNL_OK;
 }
 
+// Power-iteration time step: one cooperative launch (grid barriers inside).
+int launch_pi(dnl_engine *h, int force)
+{
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.gridDim = dim3(h->piGrid);
+  cfg.blockDim = dim3(TILE);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = h->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (h->npe == 8)
+    CK(cudaLaunchKernelEx(&cfg, k_power_iteration<8>, h->M, force));
+  else
+    CK(cudaLaunchKernelEx(&cfg, k_power_iteration<4>, h->M, force));
+  h->launches++;
+  return DNL_OK;
+}
+
+int launch_timestep(dnl_engine *h, int force)
+{
+  return h->powerIteration ? launch_pi(h, force) : launch_courant(h, force);
+}
+
 // One increment: the kernels of the graph.
 int enqueue_step(dnl_engine *h)
 {
   launch_bc_prep(h);
   launch_element_any(h, 0);
   launch_nodal(h);
-  launch_courant(h, 0);
+  launch_timestep(h, 0);
   launch_control(h, CTL_FINISH);
   return DNL_OK;
 }
@@ -428,6 +455,8 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
       return rc;
     if (descs[i]->elem_type != descs[0]->elem_type || descs[i]->precision != descs[0]->precision)
       return fail(nullptr, DNL_ERR_ARG, "all models of a batch share the element type and precision");
+    if (n > 1 && descs[i]->ts_method == DNL_TS_POWER_ITERATION)
+      return fail(nullptr, DNL_ERR_UNSUPPORTED, "the power-iteration time step is available for single models only");
   }
   if (dnl_device_count() == 0)
     return fail(nullptr, DNL_ERR_NO_DEVICE, "no CUDA device visible");
@@ -627,6 +656,37 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
   cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream);
   h->variant = 0;
+  h->powerIteration = (descs[0]->ts_method == DNL_TS_POWER_ITERATION);
+  if (h->powerIteration)
+  {
+    // Model::computePowerIterationTimeStep start vector: linear from 1 to -1
+    // over the degrees of freedom (Model.C:967-972)
+    const int d = h->dim;
+    const long ndof = (long)d * h->nN;
+    std::vector<double> pv((size_t)3 * h->nN, 0.0);
+    double prev = 1.0;
+    for (long i = 0; i < ndof; i++)
+    {
+      const double val = (i == 0) ? 1.0 : prev - 2. / (ndof - 1);
+      pv[3 * (i / d) + (i % d)] = val;
+      prev = val;
+    }
+    int perSM = 0;
+    if (h->npe == 8)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_power_iteration<8>, TILE, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_power_iteration<4>, TILE, 0);
+    const int tiles = (h->nIP + TILE - 1) / TILE;
+    h->piGrid = std::max(1, std::min(tiles, std::max(perSM, 1) * h->numSMs));
+    if ((rc = upload(h, &M.pv, pv)) || (rc = upload(h, &M.pv2, pv)) || (rc = dalloc(h, &M.pislot, h->nIP)) ||
+        (rc = dalloc(h, &M.blockmax, h->piGrid)))
+    {
+      std::string e = h->err;
+      dnl_engine_destroy(h);
+      snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+      return rc;
+    }
+  }
   if (cudaMallocHost((void **)&h->hctl, sizeof(Ctl) * h->nInst) != cudaSuccess)
   {
     dnl_engine_destroy(h);
@@ -675,7 +735,7 @@ int dnl_engine_init(dnl_engine *h)
   launch_element_any(h, 1);
   launch_gather(h, 0);
   // Solver::computeTimeStep(true) (Explicit.C:156-158)
-  launch_courant(h, 1);
+  launch_timestep(h, 1);
   launch_control(h, CTL_INIT_DT);
   // first element pass at t_start (Explicit.C:161-181)
   launch_element_any(h, 0);
@@ -733,7 +793,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
         CK(cudaEventRecord(e[1], h->stream));
         launch_nodal(h);
         CK(cudaEventRecord(e[2], h->stream));
-        launch_courant(h, 0);
+        launch_timestep(h, 0);
         launch_control(h, CTL_FINISH);
         CK(cudaEventRecord(e[3], h->stream));
         CK(cudaEventSynchronize(e[3]));
@@ -1115,7 +1175,7 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps)
       launch_element_any(h, 0);
       CK(cudaEventRecord(e1, h->stream));
       launch_nodal(h);
-      launch_courant(h, 0);
+      launch_timestep(h, 0);
       launch_control(h, CTL_FINISH);
       CK(cudaEventSynchronize(e1));
       float t = 0;

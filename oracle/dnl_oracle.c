@@ -61,6 +61,9 @@ struct orc_model
   int ts_method, ts_freq;
   double safety, alphaM, beta, gamma, omegaS;
   int status, bad;
+  double *pv;          /* power-iteration vector [nN*dim] (Model::_powerIterationEV) */
+  double pfmax;        /* Model::_powerIterationFreqMax */
+  long piters;         /* total power iterations run */
 };
 
 /* ---------------------------------------------------------------- tables */
@@ -237,6 +240,7 @@ void orc_destroy(orc_model *m)
   for (int f = 0; f < m->nfunc; f++) { free(m->fx[f]); free(m->fy[f]); }
   free(m->fnp); free(m->fx); free(m->fy);
   free(m->ip); free(m->detJ); free(m->radius); free(m->dNdx); free(m->rot); free(m->dE);
+  free(m->pv);
   free(m);
 }
 
@@ -937,17 +941,184 @@ int orc_element_lengths(orc_model *m, double *len, double *wave)
   return DNL_OK;
 }
 
+/* Elastic stiffness matrix of one element (ElementPlane.C:182-292,
+ * Element3D.C:303-399) with the Hooke matrices of Material.C:98-152
+ * (axisymmetric 4x4 rr, zz, rz, tt / 3-D 6x6 xx, yy, zz, xy, yz, xz; the
+ * shear terms are E/(1+nu)), on the dN/dx of the current Jacobian. */
+static void stiffness(orc_model *m, long e, double *K /* [nd*nd] */)
+{
+  const dnl_material *mt = &m->mat[m->emat[e]];
+  const double E = mt->young, nu = mt->poisson;
+  const double f = E / ((1 + nu) * (1 - 2 * nu));
+  int npe = m->npe, d = m->dim, nd = npe * d;
+  double C[6][6] = {{0}};
+  if (m->dim == 2)
+  {
+    C[0][0] = C[1][1] = C[3][3] = (1 - nu) * f;
+    C[2][2] = (1 - 2 * nu) * f;
+    C[1][0] = C[0][1] = C[3][0] = C[0][3] = C[3][1] = C[1][3] = nu * f;
+  }
+  else
+  {
+    C[0][0] = C[1][1] = C[2][2] = (1 - nu) * f;
+    C[3][3] = C[4][4] = C[5][5] = (1 - 2 * nu) * f;
+    C[0][1] = C[1][0] = C[0][2] = C[2][0] = C[1][2] = C[2][1] = nu * f;
+  }
+  memset(K, 0, sizeof(double) * nd * nd);
+  double CB[6][24];
+  for (int g = 0; g < npe; g++)
+  {
+    long q = e * npe + g;
+    const double *dn = m->dNdx + q * npe * 3;
+    double WxdJ = m->w[g] * m->detJ[q], R = m->radius[q];
+    if (m->dim == 2)
+    {
+      WxdJ *= TWO_PI * R;
+      for (int i = 0; i < npe; i++)
+      {
+        double dNx = dn[3 * i], dNy = dn[3 * i + 1], NoR = m->N[g][i] / R;
+        int I = 2 * i;
+        for (int r = 0; r < 4; r++)
+        {
+          CB[r][I] = C[r][0] * dNx + C[r][2] * dNy + C[r][3] * NoR;
+          CB[r][I + 1] = C[r][1] * dNy + C[r][2] * dNx;
+        }
+      }
+      for (int i = 0; i < npe; i++)
+      {
+        double dNx = dn[3 * i], dNy = dn[3 * i + 1], NoR = m->N[g][i] / R;
+        for (int j = 0; j < npe; j++)
+        {
+          int I = 2 * i, J = 2 * j;
+          K[I * nd + J] += (dNx * CB[0][J] + dNy * CB[2][J]) * WxdJ;
+          K[I * nd + J + 1] += (dNx * CB[0][J + 1] + dNy * CB[2][J + 1]) * WxdJ;
+          K[(I + 1) * nd + J] += (dNy * CB[1][J] + dNx * CB[2][J]) * WxdJ;
+          K[(I + 1) * nd + J + 1] += (dNy * CB[1][J + 1] + dNx * CB[2][J + 1]) * WxdJ;
+          K[I * nd + J] += CB[3][J] * NoR * WxdJ;
+          K[I * nd + J + 1] += CB[3][J + 1] * NoR * WxdJ;
+        }
+      }
+    }
+    else
+    {
+      for (int i = 0; i < npe; i++)
+      {
+        double dNx = dn[3 * i], dNy = dn[3 * i + 1], dNz = dn[3 * i + 2];
+        int I = 3 * i;
+        for (int r = 0; r < 6; r++)
+        {
+          CB[r][I] = C[r][0] * dNx + C[r][3] * dNy + C[r][5] * dNz;
+          CB[r][I + 1] = C[r][1] * dNy + C[r][3] * dNx + C[r][4] * dNz;
+          CB[r][I + 2] = C[r][2] * dNz + C[r][4] * dNy + C[r][5] * dNx;
+        }
+      }
+      for (int i = 0; i < npe; i++)
+      {
+        double dNx = dn[3 * i], dNy = dn[3 * i + 1], dNz = dn[3 * i + 2];
+        for (int j = 0; j < npe; j++)
+          for (int c = 0; c < 3; c++)
+          {
+            int I = 3 * i, J = 3 * j + c;
+            K[I * nd + J] += (dNx * CB[0][J] + dNy * CB[3][J] + dNz * CB[5][J]) * WxdJ;
+            K[(I + 1) * nd + J] += (dNy * CB[1][J] + dNx * CB[3][J] + dNz * CB[4][J]) * WxdJ;
+            K[(I + 2) * nd + J] += (dNz * CB[2][J] + dNy * CB[4][J] + dNx * CB[5][J]) * WxdJ;
+          }
+      }
+    }
+  }
+}
+
+/* Model::computePowerIterationTimeStep (Model.C:942-1009): the largest
+ * eigenvalue of M^-1 K by power iteration, warm-started from the previous
+ * vector and frequency.  As in the reference, the assembled K v is added to
+ * the old vector (Vector::gatherFrom adds, Vector.C:893-915). */
+static int power_iteration(orc_model *m, double *omega)
+{
+  int d = m->dim, npe = m->npe, nd = npe * d;
+  long ndof = m->nN * d;
+  if (!m->pv)
+  {
+    m->pv = (double *)xcalloc(ndof, sizeof(double));
+    m->pv[0] = 1.0;
+    for (long i = 1; i < ndof; i++)
+      m->pv[i] = m->pv[i - 1] - 2. / (ndof - 1);
+  }
+  double *Ks = (double *)xcalloc((size_t)m->nE * nd * nd, sizeof(double));
+  for (long e = 0; e < m->nE; e++)
+    stiffness(m, e, Ks + (size_t)e * nd * nd);
+  double *v0 = (double *)xcalloc(ndof, sizeof(double));
+  double loc[24], y[24], fmax = 0.0;
+  long it = 0;
+  int ok = 0;
+  while (!ok)
+  {
+    it++;
+    memcpy(v0, m->pv, ndof * sizeof(double));
+    for (long e = 0; e < m->nE; e++)
+    {
+      const int32_t *cn = m->conn + e * npe;
+      for (int n = 0; n < npe; n++)
+        for (int c = 0; c < d; c++)
+          loc[n * d + c] = v0[cn[n] * d + c];
+      const double *K = Ks + (size_t)e * nd * nd;
+      for (int i = 0; i < nd; i++)
+      {
+        double acc = 0.0;
+        for (int j = 0; j < nd; j++)
+          acc += K[i * nd + j] * loc[j];
+        y[i] = acc;
+      }
+      for (int n = 0; n < npe; n++)
+        for (int c = 0; c < d; c++)
+          m->pv[cn[n] * d + c] += y[n * d + c];
+    }
+    fmax = 0.0;
+    for (long i = 0; i < ndof; i++)
+    {
+      m->pv[i] /= m->mass[i / d];
+      if (fabs(m->pv[i]) > fmax)
+        fmax = fabs(m->pv[i]);
+    }
+    for (long i = 0; i < ndof; i++)
+      m->pv[i] /= fmax;
+    double conv = fabs(fmax - m->pfmax) / fmax;
+    if (conv < 1e-4)
+      ok = 1;
+    m->pfmax = fmax;
+    if (it > 1000)
+    {
+      free(Ks);
+      free(v0);
+      m->status = DNL_ERR_POWER_ITERATION;
+      return DNL_ERR_POWER_ITERATION;
+    }
+  }
+  m->piters += it;
+  free(Ks);
+  free(v0);
+  *omega = sqrt(fmax);
+  return DNL_OK;
+}
+
 /* Solver::computeTimeStep (Solver.C:196-244). */
 static int compute_time_step(orc_model *m, int force)
 {
   if (force || (m->inc % m->ts_freq == 0))
   {
-    if (m->ts_method != DNL_TS_COURANT)
+    double fmax;
+    if (m->ts_method == DNL_TS_COURANT)
+      fmax = 2.0 / orc_courant(m);
+    else if (m->ts_method == DNL_TS_POWER_ITERATION)
     {
-      set_err("only the Courant time step is restated");
+      int rc = power_iteration(m, &fmax);
+      if (rc)
+        return rc;
+    }
+    else
+    {
+      set_err("unknown time-step method %d", m->ts_method);
       return DNL_ERR_UNSUPPORTED;
     }
-    double fmax = 2.0 / orc_courant(m);
     m->dt = m->safety * m->omegaS / fmax;
   }
   return DNL_OK;

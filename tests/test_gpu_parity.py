@@ -240,3 +240,38 @@ def test_element_variants_agree_and_autotune_keeps_state(precision):
         assert e.control()["increment"] == before[2]["increment"]
         e.run(max_incs=20)
         assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), results[0][0]) < xtol
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_power_iteration_taylor_axi_sample(precision):
+    """The reference's Taylor-Axi sample with its power-iteration time step
+    (Samples/Taylor/Taylor-Axi/Taylor.py:115-118) against the compiled
+    reference's final height, radius and plastic strain."""
+    rows = np.load(os.path.join(helpers.GOLDEN, "taylor_axi_sample.npz"))["rows"]
+    row = rows[rows[:, 0] == _abi.TS_POWER_ITERATION][0]
+    d = meshes.taylor_axi(nr=5, nz=50, radius=3.2, length=32.4, speed=287000.0, mat=meshes.STEEL_42CRMO4,
+                          t_end=80e-6, ts_method=_abi.TS_POWER_ITERATION, ts_freq=1, precision=precision)
+    with engine(d) as e:
+        e.init()
+        n = e.run()
+        c = e.nodes(_abi.NODE_COORDS)
+        epsp = e.ips()[_abi.IP_EPSP].reshape(-1, 4).mean(1).max()
+    if precision == _abi.PREC_FP64:
+        assert n == int(row[2])
+        assert abs(c[5, 0] - row[3]) < 1e-9 * row[3] and abs(c[d.n_nodes - 6, 1] - row[4]) < 1e-9 * row[4]
+        assert abs(epsp - row[5]) < 1e-8
+    else:
+        assert abs(c[5, 0] - row[3]) < 1e-4 * row[3] and abs(c[d.n_nodes - 6, 1] - row[4]) < 1e-4 * row[4]
+        assert abs(epsp - row[5]) < 1e-3 * row[5]
+
+
+def test_power_iteration_hex_vs_oracle():
+    desc = helpers.case_hex_small().copy(ts_method=_abi.TS_POWER_ITERATION, ts_freq=2)
+    with oracle.OracleModel(desc) as o, engine(desc) as e:
+        o.init()
+        e.init()
+        assert abs(e.control()["time_step"] - o.control()["time_step"]) < 1e-12 * o.control()["time_step"]
+        o.run(max_incs=30)
+        e.run(max_incs=30)
+        assert abs(e.control()["time_step"] - o.control()["time_step"]) < 1e-11 * o.control()["time_step"]
+        assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), o.nodes(_abi.NODE_COORDS)) < 1e-12

@@ -203,3 +203,37 @@ def test_reference_bulk_model_building_is_equivalent():
         finally:
             del os.environ["DNL_REF_BULK_MIN_ELEMS"]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_oracle_power_iteration_time_step_matches_reference():
+    """Model::computePowerIterationTimeStep (Model.C:942-1009) restated: a hex
+    block run with the power-iteration time step recomputed every 2 increments."""
+    desc = helpers.case_hex_small().copy(ts_method=_abi.TS_POWER_ITERATION, ts_freq=2)
+    with ref.RefModel(desc) as r:
+        r.init()
+        c0 = r.control()
+        r.run(max_incs=30)
+        x_r, ip_r, c_r = r.nodes(_abi.NODE_COORDS), r.ips(), r.control()
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        assert abs(o.control()["time_step"] - c0["time_step"]) < 1e-13 * c0["time_step"]
+        o.run(max_incs=30)
+        assert abs(o.control()["time_step"] - c_r["time_step"]) < 1e-12 * c_r["time_step"]
+        assert helpers.rel_err(o.nodes(_abi.NODE_COORDS), x_r) < 1e-12
+        assert helpers.field_errors(o.ips(), ip_r).max() < 1e-8
+
+
+def test_oracle_power_iteration_reproduces_taylor_axi_sample():
+    rows = np.load(os.path.join(helpers.GOLDEN, "taylor_axi_sample.npz"))["rows"]
+    row = rows[rows[:, 0] == _abi.TS_POWER_ITERATION][0]
+    d = meshes.taylor_axi(nr=5, nz=50, radius=3.2, length=32.4, speed=287000.0, mat=meshes.STEEL_42CRMO4,
+                          t_end=80e-6, ts_method=_abi.TS_POWER_ITERATION, ts_freq=1)
+    with oracle.OracleModel(d) as o:
+        o.init()
+        n = o.run()
+        c = o.nodes(_abi.NODE_COORDS)
+        ip = o.ips()
+    assert n == int(row[2])
+    assert abs(c[5, 0] - row[3]) < 1e-9 and abs(c[d.n_nodes - 6, 1] - row[4]) < 1e-9
+    assert abs(ip[_abi.IP_EPSP].reshape(-1, 4).mean(1).max() - row[5]) < 1e-9
