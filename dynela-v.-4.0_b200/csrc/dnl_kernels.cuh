@@ -42,6 +42,7 @@ struct __align__(128) Ctl
   int elem_begin, elem_end, node_begin, node_end;
   int ts_method, pi_iters, pad0, pad1;
   double pi_fmax, pi_omega; // power iteration: Model::_powerIterationFreqMax, last omega_max
+  double dt_last;           // time step of the last completed increment
 };
 
 static constexpr unsigned long long INF_BITS = 0x7ff0000000000000ull;
@@ -1335,6 +1336,7 @@ __global__ void k_control(DevModel M, int phase, double t_stop, long long max_in
     {
       // Explicit::endStep (Explicit.C:539-552): time, then the nodal field swap
       c.t = c.t_new;
+      c.dt_last = c.dt_eff;
       c.f0 ^= 1;
       if (c.due)
         apply_courant(c);

@@ -949,6 +949,7 @@ int dnl_engine_control(const dnl_engine *h, int32_t i, dnl_control *out)
   out->bad_index = c.bad;
   out->done = c.t >= c.t_end;
   out->fp64_resolves = c.resolves;
+  out->last_time_step = (c.inc - ((c.prepared && c.active) ? 1 : 0)) > 0 ? c.dt_last : c.dt;
   return DNL_OK;
 }
 

@@ -97,7 +97,7 @@ class ModelDescC(ctypes.Structure):
 class Control(ctypes.Structure):
     _fields_ = [("time", ctypes.c_double), ("time_step", ctypes.c_double), ("t_end", ctypes.c_double),
                 ("increment", ctypes.c_int64), ("status", ctypes.c_int32), ("bad_index", ctypes.c_int32),
-                ("done", ctypes.c_int32), ("fp64_resolves", ctypes.c_int32)]
+                ("done", ctypes.c_int32), ("fp64_resolves", ctypes.c_int32), ("last_time_step", ctypes.c_double)]
 
 
 def _ptr(a, ctype):

@@ -56,7 +56,8 @@ class Engine:
         c = _abi.Control()
         self._check(self._lib.dnl_engine_control(self.h, int(instance), ctypes.byref(c)))
         return dict(time=c.time, time_step=c.time_step, t_end=c.t_end, increment=c.increment,
-                    status=c.status, bad_index=c.bad_index, done=bool(c.done), fp64_resolves=c.fp64_resolves)
+                    status=c.status, bad_index=c.bad_index, done=bool(c.done), fp64_resolves=c.fp64_resolves,
+                    last_time_step=c.last_time_step)
 
     def offsets(self, instance):
         n0, e0, q0 = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()

@@ -180,3 +180,30 @@ def hex_block(nx, ny, nz, size=(1.0, 1.0, 1.0), mat=COPPER, t_end=1e-6, speed=0.
 
 def nodes_per_element_ratio(desc):
     return desc.n_nodes / desc.n_elems
+
+
+def taylor_batch(n=256, seed=20261203, elems=(2000, 60000), speed=(150000.0, 300000.0), jc_scale=(0.8, 1.2),
+                 t_end=80e-6, precision=_abi.PREC_MIXED, ts_freq=10):
+    """Batch of independent 3-D copper Taylor bars of uneven size and parameters:
+    element counts log-uniform in `elems`, impact speed uniform in `speed`
+    (mm/s), and Johnson-Cook A, B, n, C, m each scaled by a factor uniform in
+    `jc_scale`, all drawn from `seed`.  Each bar is taylor_3d with its
+    cross-section and layer count scaled so that the elements keep the shape
+    of the 153,600-element bar."""
+    rng = np.random.default_rng(seed)
+    descs = []
+    for _ in range(n):
+        target = float(np.exp(rng.uniform(np.log(elems[0]), np.log(elems[1]))))
+        v = float(rng.uniform(*speed))
+        f = rng.uniform(jc_scale[0], jc_scale[1], 5)
+        mat = dict(COPPER)
+        for k, s in zip(("A", "B", "n", "C", "m"), f):
+            mat[k] = COPPER[k] * float(s)
+        s = (target / 153600.0) ** (1.0 / 3.0)
+        n_core = max(2, int(round(12 * s)))
+        n_ring = max(2, int(round(17 * s)))
+        per_layer = n_core * n_core + 4 * n_core * n_ring
+        n_axial = max(4, int(round(target / per_layer)))
+        descs.append(taylor_3d(n_core=n_core, n_ring=n_ring, n_axial=n_axial, speed=v, mat=mat, t_end=t_end,
+                               ts_freq=ts_freq, precision=precision))
+    return descs

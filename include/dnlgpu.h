@@ -135,6 +135,8 @@ typedef struct dnl_control {
   int32_t bad_index;  /* element (negative detJ) or integration point (Newton) that failed */
   int32_t done;       /* time >= t_end */
   int32_t fp64_resolves; /* mixed path: points re-solved in FP64 during the last run call */
+  double last_time_step; /* time step of the last completed increment (Solver::timeStep as the
+                            history files see it in Explicit::endStep, Explicit.C:539-552) */
 } dnl_control;
 
 typedef struct dnl_engine dnl_engine;
