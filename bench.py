@@ -46,6 +46,10 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--variant", type=int, default=-1,
                    help="element-pass variant (0-3); default: chosen by the autotuner")
+    p.add_argument("--no-accuracy", action="store_true", help="skip the whole-run mixed/FP64 comparison")
+    p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
+    p.add_argument("--batch-fp64-sample", type=int, default=32,
+                   help="instances of the batch timed one by one on the FP64 path")
     p.add_argument("--axial", type=int, default=160,
                    help="axial element layers (160 = the measured workload; fewer for profiling captures)")
     return p.parse_args()
@@ -213,6 +217,95 @@ def cpu_baseline(desc):
     return {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
 
+# ------------------------------------------------- whole runs and batches
+
+def bar_results(desc, coords, ips):
+    """Final bar length (highest node), foot radius (largest distance to the
+    axis on the impact face), maximum equivalent plastic strain."""
+    import numpy as np
+    from dnlPython import _abi
+    face = desc.coords[:, 1] == 0.0
+    foot = np.sqrt(coords[face, 0] ** 2 + coords[face, 2] ** 2).max()
+    return float(coords[:, 1].max()), float(foot), float(ips[_abi.IP_EPSP].max())
+
+
+def accuracy_run():
+    """The measured bar run to its end time on the mixed and the FP64 path:
+    final length, foot radius and max plastic strain, with the mixed path's
+    relative error against the FP64 path."""
+    from dnlPython import _abi
+    from dnlPython.engine import Engine
+    res = {}
+    for name in ("fp64", "mixed"):
+        d = workload(name)
+        with Engine(d) as e:
+            e.init()
+            e.autotune(steps=6)
+            e.run()
+            c = e.control()
+            L, R, ep = bar_results(d, e.nodes(_abi.NODE_COORDS), e.ips())
+            res[name] = {"increments": c["increment"], "time_s": c["time"], "status": c["status"],
+                         "run_ms": e.timings()["run_ms"], "length_mm": L, "foot_radius_mm": R, "max_epsp": ep,
+                         "fp64_resolves": c["fp64_resolves"]}
+    m, f = res["mixed"], res["fp64"]
+    res["rel_err_mixed_vs_fp64"] = {"length": abs(m["length_mm"] - f["length_mm"]) / f["length_mm"],
+                                    "foot_radius": abs(m["foot_radius_mm"] - f["foot_radius_mm"]) / f["foot_radius_mm"],
+                                    "max_epsp": abs(m["max_epsp"] - f["max_epsp"]) / f["max_epsp"]}
+    res["whole_run_mixed_over_fp64"] = f["run_ms"] / m["run_ms"]
+    res["reference"] = "FP64 GPU path (held to the FP64 oracle on the smaller cases of the test suite)"
+    return res
+
+
+def batch_run(sample):
+    """256 independent copper Taylor bars (element counts log-uniform in
+    2k-60k, speed U(150,300) m/s, Johnson-Cook A, B, n, C, m scaled by
+    U(0.8,1.2), seed 20261203) advanced together to 80 us on the mixed path,
+    against a size-stratified sample of the same bars run one by one on the
+    FP64 path."""
+    import numpy as np
+    from dnlPython import meshes, _abi
+    from dnlPython.engine import Engine
+    descs = meshes.taylor_batch()
+    elems = np.array([d.n_elems for d in descs], dtype=np.float64)
+    t0 = time.perf_counter()
+    with Engine(descs) as b:
+        b.init()
+        variant, _ = b.autotune(steps=6)
+        setup = time.perf_counter() - t0
+        replays = b.run(check=False)
+        ms = b.timings()["run_ms"]
+        launches = b.launch_count()
+        ctl = [b.control(i) for i in range(len(descs))]
+    incs = np.array([c["increment"] for c in ctl], dtype=np.float64)
+    failed = [i for i, c in enumerate(ctl) if c["status"] != 0]
+    steps = float((elems * incs).sum())
+    out = {"instances": len(descs), "elements": int(elems.sum()), "seed": 20261203, "precision": "mixed",
+           "replays": int(replays), "run_ms": ms, "sims_per_s": len(descs) / (ms / 1e3),
+           "elem_steps_per_s": steps / (ms / 1e3), "increments_min_max": [int(incs.min()), int(incs.max())],
+           "stopped_on_error": {str(i): _abi.ERRORS.get(ctl[i]["status"], ctl[i]["status"]) + f" at t={ctl[i]['time']:.3e}"
+                                for i in failed},
+           "element_variant": int(variant), "gpu_launches": launches, "setup_s": setup}
+    if sample > 0:
+        order = np.argsort(elems, kind="stable")
+        pick = order[np.linspace(0, len(order) - 1, min(sample, len(order))).astype(int)]
+        t_ms, s_steps, s_elems = 0.0, 0.0, 0.0
+        for i in pick:
+            d = descs[i].copy(precision=_abi.PREC_FP64)
+            with Engine(d) as e:
+                e.init()
+                n = e.run(check=False)
+                t_ms += e.timings()["run_ms"]
+                s_steps += d.n_elems * e.control()["increment"]
+        rate = s_steps / (t_ms / 1e3)
+        est_s = steps / rate
+        out["fp64_one_by_one"] = {"instances_timed": int(len(pick)), "elem_steps_per_s": rate,
+                                  "est_seconds_all": est_s, "est_sims_per_s": len(descs) / est_s,
+                                  "how": "every instance of a size-ordered stride timed alone to its end time; "
+                                         "all-instance time extrapolated by elem-steps"}
+        out["batched_mixed_over_one_by_one_fp64"] = out["elem_steps_per_s"] / rate
+    return out
+
+
 # ------------------------------------------------------------------ arms
 
 def run_reference_arm(args, rank):
@@ -359,6 +452,11 @@ def run_engine_arm(args, rank, world, dist):
         out["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(desc)
+    # whole runs and the batch hold one GPU for a few minutes: single-GPU runs only
+    if world == 1 and AXIAL == 160 and not args.no_accuracy:
+        out["accuracy_whole_run"] = accuracy_run()
+    if world == 1 and not args.no_batch:
+        out["batched"] = batch_run(args.batch_fp64_sample)
     print(json.dumps(out))
 
 

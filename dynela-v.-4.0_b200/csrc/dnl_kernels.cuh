@@ -766,13 +766,31 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
     bulk_g2s(state[b], reinterpret_cast<const R *>(M.ip) + (size_t)tile * DNL_IP_NCOMP * TILE, STATE_BYTES, &bar[b]);
     bulk_g2s(conn[b], M.conn + (size_t)tile * TILE, CONN_BYTES, &bar[b]);
   };
-  int tile = blockIdx.x;
+  // Tiles whose instances have all stopped are neither copied nor computed.
+  // The active flags do not change during the pass, so every thread of the
+  // block walks the same sequence of tiles.
+  auto live = [&](int tl) {
+    if (M.nInst == 1)
+      return M.ctl[0].active != 0;
+    const int e0 = tl * (TILE / NPE), e1 = min(M.nE - 1, e0 + TILE / NPE - 1);
+    const int i1 = find_segment(M.inst_elem_begin, M.nInst, e1);
+    for (int i = find_segment(M.inst_elem_begin, M.nInst, e0); i <= i1; i++)
+      if (M.ctl[i].active)
+        return true;
+    return false;
+  };
+  auto next_live = [&](int tl) {
+    while (tl < nTiles && !live(tl))
+      tl += gridDim.x;
+    return tl;
+  };
+  int tile = next_live(blockIdx.x);
   if (t == 0 && tile < nTiles)
     issue(tile, 0);
   uint32_t phase[2] = {0, 0};
-  for (int b = 0; tile < nTiles; tile += gridDim.x, b ^= 1)
+  for (int b = 0, next; tile < nTiles; tile = next, b ^= 1)
   {
-    const int next = tile + gridDim.x;
+    next = next_live(tile + gridDim.x);
     if (t == 0 && next < nTiles)
       issue(next, b ^ 1);
     if (!mbar_wait(&bar[b], phase[b]))

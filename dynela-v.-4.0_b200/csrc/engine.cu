@@ -843,13 +843,11 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
       }
       if ((rc = sync_ctl(h)))
         return rc;
-      bool any = false, bad = false;
+      // an instance that fails stops alone; the others of a batch go on
+      bool any = false;
       for (int i = 0; i < h->nInst; i++)
-      {
         any = any || h->hctl[i].active;
-        bad = bad || h->hctl[i].status;
-      }
-      if (!any || bad)
+      if (!any)
         break;
     }
   }

@@ -26,6 +26,7 @@ PREC_MIXED = 1
 BC_FREE, BC_RESTRAIN, BC_SPEED = 0, 1, 2
 
 DNL_OK = 0
+DNL_ERR_NEG_JACOBIAN, DNL_ERR_NEWTON = -3, -4
 ERRORS = {
     -1: "invalid argument",
     -2: "CUDA error",

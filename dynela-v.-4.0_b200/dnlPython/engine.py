@@ -44,9 +44,13 @@ class Engine:
         self._check(self._lib.dnl_engine_init(self.h))
         return self
 
-    def run(self, t_pause=np.inf, max_incs=0):
+    def run(self, t_pause=np.inf, max_incs=0, check=True):
+        """Advance to t_pause / max_incs.  check=False leaves a failed
+        instance's error in control(i)['status'] instead of raising (batches)."""
         done = ctypes.c_int64()
-        self._check(self._lib.dnl_engine_run(self.h, float(t_pause), int(max_incs), ctypes.byref(done)))
+        rc = self._lib.dnl_engine_run(self.h, float(t_pause), int(max_incs), ctypes.byref(done))
+        if check or rc not in (_abi.DNL_ERR_NEG_JACOBIAN, _abi.DNL_ERR_NEWTON):
+            self._check(rc)
         return done.value
 
     def element_pass(self, dt):

@@ -168,7 +168,11 @@ int dnl_engine_init(dnl_engine *h);
  * or max_incs increments have been run in this call (max_incs <= 0: no limit).
  * Replaces the increment loop of Explicit::solve (Explicit.C:184-256).
  * *incs_done (may be NULL) receives the largest number of increments run by
- * one instance in this call. */
+ * one instance in this call.  An instance whose increment fails (negative
+ * Jacobian, radial return without convergence) stops there with the error in
+ * its dnl_control.status, where the reference would abort the whole solve;
+ * the other instances of a batch go on, and once every instance has stopped
+ * the call returns the error of the lowest-numbered failed instance. */
 int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *incs_done);
 
 /* Kernel-level entry point: one element pass (strains, pressure, radial
