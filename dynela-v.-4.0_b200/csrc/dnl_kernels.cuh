@@ -18,6 +18,9 @@
 #pragma once
 
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
+
+#include <cstring>
 
 #include "dnl_math.cuh"
 #include "dnlgpu.h"
@@ -78,6 +81,13 @@ struct DevModel
   double *pv, *pv2;        // [nN*3] iteration vectors (dof = 3 node + component)
   double4 *pislot;         // [nE*npe] element K v contributions, node order
   double *blockmax;        // [gridDim] per-block max |v|
+  // element-pass modes (learned initial guess, Newton statistics, training pairs)
+  const void *mlp_image;   // network image (dnl_mlp.cuh)
+  unsigned long long *stats; // [0] yield-function evaluations, [1] yielding points, [2] guesses used
+  float *harvest;          // pairs of DNL_MLP_PAIR_WORDS floats
+  unsigned long long *harvest_count;
+  long long harvest_cap;
+  int harvest_stride, pad1;
 };
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
@@ -446,6 +456,16 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
     H[8] = Vr / radius;
 }
 
+// What the first half of an element update hands to the second: the strain
+// increment, the Jacobian terms and the point state loaded for the return (the
+// rotation and J^-1 wait in the lane's shared-memory row).
+template <typename R> struct Front
+{
+  R detJ, WxdJ, radius;
+  R dE[6];
+  ReturnState<R> st;
+};
+
 // One increment's work at one Gauss point (Explicit.C:204-226 + the density of
 // Explicit::computeDensity; Element.C:1103-1256 with the Jacobian of
 // ElementPlane.C:46-102 / Element3D.C:64-115 on the current coordinates):
@@ -453,40 +473,38 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
 // radial return, final rotation, density, and the element's nodal forces,
 // summed over its points through shared memory and stored in node order.
 // `row` is this lane's shared-memory row, `grp` the row of the element's first lane.
+// element_front runs up to the start of the return, element_back from the
+// return on; a kernel may run block-wide work (the learned guess) in between.
 template <typename R, int NPE, class Src, class Io>
-__device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int e, int g, int base, unsigned amask,
-                                               int node, const Src &old, R *row, R *grp)
+__device__ __forceinline__ void element_front(const Io &io, Ctl *C, int e, int g, int base, unsigned amask, int node,
+                                              const Src &old, R *row, Front<R> &f)
 {
-  constexpr int DIM = ElemShape<NPE>::DIM;
   constexpr bool AXI = ElemShape<NPE>::AXI;
-  constexpr int ROW = ElemShape<NPE>::ROW;
-  using R4 = typename V4<R>::type;
-  const double dt = C->dt_eff;
   const MatDev &mp = io.mat(e);
   const double4 X = io.x(node);
   const double4 U = io.u(node);
 
-  R detJ, inv[3][3], radius, dE[6], Rot[9];
+  R inv[3][3], Rot[9];
   {
     R H[9];
-    kinematics<R, NPE>(amask, g, base, X, U, detJ, inv, radius, H);
-    polar_lnU<R>(H, dE, Rot);
+    kinematics<R, NPE>(amask, g, base, X, U, f.detJ, inv, f.radius, H);
+    polar_lnU<R>(H, f.dE, Rot);
   }
-  if (detJ < R(0))
+  if (f.detJ < R(0))
     raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
-  R WxdJ = detJ; // Gauss weight 1
+  f.WxdJ = f.detJ; // Gauss weight 1
   if constexpr (AXI)
-    WxdJ *= R(6.28318530717958647692) * radius;
+    f.WxdJ *= R(6.28318530717958647692) * f.radius;
 
   // element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
-  const R trSum = group_sum<NPE>(amask, dE[0] + dE[3] + dE[5]);
+  const R trSum = group_sum<NPE>(amask, f.dE[0] + f.dE[3] + f.dE[5]);
 
   // total strain: Strain += dE, then the final rotation (Element.C:1116-1161)
   {
     R strain[6];
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      strain[c] = old(DNL_IP_STRAIN + c) + dE[c];
+      strain[c] = old(DNL_IP_STRAIN + c) + f.dE[c];
     rotate_sym<R>(Rot, strain);
 #pragma unroll
     for (int c = 0; c < 6; c++)
@@ -501,8 +519,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
     row[9 + k] = inv[k / 3][k % 3];
   }
 
-  // J2 radial return with Johnson-Cook hardening (Element.C:407-622)
-  ReturnState<R> st;
+  ReturnState<R> &st = f.st;
 #pragma unroll
   for (int c = 0; c < 6; c++)
     st.s[c] = old(DNL_IP_STRESS + c);
@@ -515,11 +532,30 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   st.eint = old(DNL_IP_EINT);
   st.einel = old(DNL_IP_EINEL);
   st.pressure = (st.s[0] + st.s[3] + st.s[5]) / R(3) + R(mp.K) * (trSum / R(NPE));
+}
+
+// Second half: J2 radial return with Johnson-Cook hardening (Element.C:407-622)
+// from gamma0 (< 0: the reference's warm start), final rotation, density,
+// write-back and the element forces.  Returns the yield-function evaluations
+// of the return (0 for an elastic point).
+template <typename R, int NPE, class Src, class Io>
+__device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, int g, unsigned amask,
+                                            const Src &old, R *row, R *grp, Front<R> &f, R gamma0 = R(-1))
+{
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  constexpr bool AXI = ElemShape<NPE>::AXI;
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  using R4 = typename V4<R>::type;
+  const double dt = C->dt_eff;
+  const MatDev &mp = io.mat(e);
+  ReturnState<R> &st = f.st;
+  const R *dE = f.dE;
+  int iters;
   {
     JC<R> jc;
     jc.load(mp);
     bool ok;
-    radial_return<R>(jc, R(mp.twoG), R(mp.heatFrac), R(1.0 / mp.rho0), dE, R(dt), st, ok);
+    iters = radial_return<R>(jc, R(mp.twoG), R(mp.heatFrac), R(1.0 / mp.rho0), dE, R(dt), st, ok, gamma0);
     if (!ok)
     {
       if constexpr (sizeof(R) == 4)
@@ -549,6 +585,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
 
   // final rotation of the plastic strain (PlasticStrain += gamma s*/|s*|,
   // Element.C:587) and of the stress, state write-back
+  R Rot[9];
 #pragma unroll
   for (int k = 0; k < 9; k++)
     Rot[k] = row[k];
@@ -564,9 +601,9 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
       io.put(DNL_IP_PLASTIC_STRAIN + c, ep[c]);
   }
   rotate_sym<R>(Rot, st.s);
-  R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
+  R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / f.detJ; // Element::computeDensity (Element.C:1243-1256)
   if constexpr (AXI)
-    rho /= radius;
+    rho /= f.radius;
 #pragma unroll
   for (int c = 0; c < 6; c++)
     io.put(DNL_IP_STRESS + c, st.s[c]);
@@ -593,11 +630,11 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
 #pragma unroll
       for (int j = 0; j < DIM; j++)
         s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
-      P[k][i] = -WxdJ * s;
+      P[k][i] = -f.WxdJ * s;
     }
   const R a = R(0.57735026918962576451);
   const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
-  const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
+  const R hoop = AXI ? st.s[5] / f.radius * f.WxdJ : R(0);
   ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
   __syncwarp(amask);
   R4 fs;
@@ -611,6 +648,16 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
       fs.z += grp[l * ROW + g * DIM + 2];
   }
   io.slot(fs);
+  return iters;
+}
+
+template <typename R, int NPE, class Src, class Io>
+__device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int e, int g, int base, unsigned amask,
+                                               int node, const Src &old, R *row, R *grp)
+{
+  Front<R> f;
+  element_front<R, NPE>(io, C, e, g, base, amask, node, old, row, f);
+  element_back<R, NPE>(io, C, q, e, g, amask, old, row, grp, f);
 }
 
 // Start of the solve: reference Jacobian detJ0 (ElementPlane.C:96-100,
@@ -723,15 +770,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
   return ok != 0;
 }
 
-// Bounded wait for the phase `parity` of a bulk-copy barrier; false when it
-// did not complete within the limit (the caller flags an error and stops).
+// Bounded wait for the phase `parity` of an mbarrier (bulk copies, tensor-core
+// commits); false when it did not complete within about two seconds of SM
+// clock (the caller flags an error and goes on without the data).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
-  for (int i = 0; i < (1 << 24); i++)
-    if (mbar_try_wait(bar, parity))
-      return true;
-  return false;
+  const long long start = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - start > (1ll << 32))
+      return false;
+  return true;
 }
+
+#include "dnl_mlp.cuh"
 
 // Element pass as a persistent kernel over tiles of TILE Gauss points: while a
 // block computes one tile, the bulk-copy engine brings the next tile's point
@@ -815,6 +866,125 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
     }
     __syncthreads(); // the buffer is refilled two tiles later
   }
+}
+
+// ------------------------------------------------ element pass with modes
+
+enum
+{
+  MODE_STATS = 1,   // Newton iterations counted
+  MODE_HARVEST = 2, // + (trial state, converged gamma) pairs kept
+  MODE_GUESS = 3    // + the network's guess as the first iterate
+};
+
+// Element pass (mixed precision) with the Newton iterations of the return
+// counted, and, per MODE, training pairs harvested from the converged returns
+// or the learned initial guess evaluated on the tensor cores for each tile of
+// TILE points between the two halves of the update.  Persistent over tiles.
+template <int NPE, int MODE>
+__global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles, int *err)
+{
+  using R = float;
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  __shared__ R sh[TILE * ROW];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tslot;
+  extern __shared__ __align__(1024) unsigned char dyn[];
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  const int g = lane & (NPE - 1);
+  const int base = lane & ~(NPE - 1);
+  mlp::Tile net;
+  if constexpr (MODE == MODE_GUESS)
+    mlp::tile_setup(net, dyn, M.mlp_image, &bar, &tslot, err);
+  unsigned long long nEval = 0, nPlastic = 0, nGuess = 0;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x)
+  {
+    const int q = tile * TILE + t;
+    const int e = q / NPE;
+    const bool valid = e < M.nE;
+    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
+    Ctl *C = M.ctl + inst;
+    const bool act = valid && C->active;
+    const unsigned amask = __ballot_sync(0xffffffffu, act);
+    R *row = sh + t * ROW, *grp = sh + (t - g) * ROW;
+    GlobalState<R> old{M, q};
+    EngineIo<R> io{M, q, act ? C->f0 : 0};
+    Front<R> f;
+    float x[mlp::NIN] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    float gmax = 0.f;
+    bool plastic = false;
+    if (act)
+    {
+      element_front<R, NPE>(io, C, e, g, base, amask, M.conn[q], old, row, f);
+      const MatDev &mp = io.mat(e);
+      JC<R> jc;
+      jc.load(mp);
+      const R dt = R(C->dt_eff), twoG = R(mp.twoG);
+      R Strial, y0;
+      trial_state<R>(jc, twoG, f.dE, f.st, dt, Strial, y0);
+      plastic = Strial > y0;
+      if (plastic)
+      {
+        gmax = (Strial - y0) / (R(1.2247448713915890491) * twoG);
+        mlp::features(Strial, f.st.epsp, f.st.depsp, f.st.T, twoG, dt, mp, x);
+      }
+    }
+    R gamma0 = R(-1);
+    if constexpr (MODE == MODE_GUESS)
+    {
+      __syncwarp();
+      if (__syncthreads_or(plastic))
+      {
+        const float y = net.forward(t, x);
+        if (plastic)
+        {
+          gamma0 = fminf(fmaxf(y, 0.f), 2.f) * gmax;
+          nGuess++;
+        }
+      }
+    }
+    if (act)
+    {
+      const int evals = element_back<R, NPE>(io, C, q, e, g, amask, old, row, grp, f, gamma0);
+      if (evals > 0)
+      {
+        nEval += evals;
+        nPlastic++;
+      }
+      if constexpr (MODE == MODE_HARVEST)
+      {
+        const unsigned h = (unsigned)q * 2654435761u ^ (unsigned)C->inc * 40503u;
+        if (plastic && evals > 0 && gmax > 0.f && (h >> 7) % (unsigned)M.harvest_stride == 0u)
+        {
+          const unsigned long long k = atomicAdd(M.harvest_count, 1ull);
+          if ((long long)k < M.harvest_cap)
+          {
+            float4 *o = reinterpret_cast<float4 *>(M.harvest + k * DNL_MLP_PAIR_WORDS);
+            o[0] = make_float4(x[0], x[1], x[2], x[3]);
+            o[1] = make_float4(x[4], f.st.gamma / gmax, f.st.gamma, gmax);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // per-warp totals
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    nEval += __shfl_xor_sync(0xffffffffu, nEval, o);
+    nPlastic += __shfl_xor_sync(0xffffffffu, nPlastic, o);
+    nGuess += __shfl_xor_sync(0xffffffffu, nGuess, o);
+  }
+  if (lane == 0 && nPlastic)
+  {
+    atomicAdd(M.stats + 0, nEval);
+    atomicAdd(M.stats + 1, nPlastic);
+    atomicAdd(M.stats + 2, nGuess);
+  }
+  if constexpr (MODE == MODE_GUESS)
+    mlp::tile_release(net);
 }
 
 // ------------------------------------------------------------ nodal update

@@ -326,15 +326,43 @@ template <typename R> struct ReturnState
   R kplast; // out: plastic strain increment / deviator of the new stress (0 if elastic)
 };
 
+// Trial equivalent stress sqrt(3/2)|dev(sigma_old) + 2G dev(dE)| and the yield
+// stress the return starts from (with the reference's lazy first evaluation at
+// gamma = 1e-8, Element.C:458-463): the inputs of the learned initial guess.
+template <typename R>
+__device__ __forceinline__ void trial_state(const JC<R> &jc, R twoG, const R dE[6], const ReturnState<R> &st, R dt,
+                                            R &Strial, R &yield0)
+{
+  R p0 = (st.s[0] + st.s[3] + st.s[5]) / R(3), pe = (dE[0] + dE[3] + dE[5]) / R(3);
+  R d[6];
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    d[c] = st.s[c] + twoG * dE[c];
+  d[0] -= p0 + twoG * pe;
+  d[3] -= p0 + twoG * pe;
+  d[5] -= p0 + twoG * pe;
+  Strial = R(1.2247448713915890491) * sym_norm(d);
+  yield0 = st.yield;
+  if (yield0 == R(0))
+  {
+    R dummy;
+    jc.eval(R(1e-8), R(1e-8) / dt, st.T, dt, yield0, dummy, false);
+  }
+}
+
 // Element::computeStress (Element.C:407-622) for one integration point.  The
 // Newton-bisection iteration on gamma is the reference's; tolNR = 1e-8 and
 // itMax = 250 for FP64.  For FP32 the step tolerance is widened to a few ulp
 // of gamma and `ok` is cleared when the iteration fails to converge in 60
 // steps or the final residual test |f| <= 1e-5 Strial + 2 f' tol fails; the
 // caller then re-solves the point in FP64.
+// A non-negative gamma0 replaces the warm start (the previous increment's gamma)
+// as the first iterate; the bracket and the stopping tests are unchanged.
+// Returns the number of yield-function evaluations of the iteration (0 for an
+// elastic point).
 template <typename R>
 __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac, R inv_rho0, const R dE[6], R dt,
-                                             ReturnState<R> &st, bool &ok)
+                                             ReturnState<R> &st, bool &ok, R gamma0 = R(-1))
 {
   const R SQ32 = R(1.2247448713915890491), SQ23 = R(0.81649658092772603273);
   const R gammaInitial = R(1e-8);
@@ -381,6 +409,8 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
     gamma = st.gamma;
     if (epsp0 == R(0))
       gamma = SQ32 * gammaInitial;
+    if (gamma0 >= R(0))
+      gamma = gamma0;
     R depsp = SQ23 * gamma / dt;
     R epsp = epsp0 + SQ23 * gamma;
     T = T0 + R(0.5) * gamma * heatFrac * (SQ23 * yield + Snorm0);
@@ -413,7 +443,7 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
       if (iterate > itMax || !(gamma == gamma))
       {
         ok = false;
-        return iterate;
+        return iterate + 1;
       }
     }
     // FP32 acceptance: the last residual is the one before the final Newton
@@ -421,8 +451,9 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
     if (!fp64 && !(Num<R>::abs_(fun) <= R(1e-5) * Strial + R(2) * dfun * tol))
     {
       ok = false;
-      return iterate;
+      return iterate + 1;
     }
+    iterate += 1;
     const R invS = R(1) / Snorm;
     const R scale = R(1) - twoG * gamma * invS;
     // plastic strain increment gamma dev*/Snorm = kplast * (scale dev*)

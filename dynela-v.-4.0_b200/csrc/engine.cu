@@ -56,6 +56,9 @@ struct dnl_engine
   int numSMs = 0;
   bool powerIteration = false;
   int piGrid = 0;
+  int mode = DNL_MODE_PLAIN;          // element-pass mode (DNL_MODE_*)
+  void *mlpImage = nullptr;           // learned-guess network image
+  unsigned long long *dstats = nullptr; // Newton statistics [3] + harvest count
   std::string err;
 };
 
@@ -218,6 +221,36 @@ template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
   return DNL_OK;
 }
 
+template <int NPE, int MODE> int launch_mode(dnl_engine *h)
+{
+  const size_t smem = MODE == MODE_GUESS ? mlp::SMEM_BYTES : 0;
+  static int perSM = -1; // per instantiation
+  if (perSM < 0)
+  {
+    if (smem)
+      CK(cudaFuncSetAttribute(k_element_mode<NPE, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_mode<NPE, MODE>, TILE, smem));
+    if (perSM < 1)
+      perSM = 1;
+  }
+  // the blocks resident on one SM must find their tensor-memory columns free
+  if (MODE == MODE_GUESS && perSM * (int)mlp::TMEM_COLS > 512)
+    return fail(h, DNL_ERR_CUDA, "guess kernel: %d blocks per SM exceed the tensor memory", perSM);
+  const int grid = std::min(h->nTiles, perSM * h->numSMs);
+  k_element_mode<NPE, MODE><<<grid, TILE, smem, h->stream>>>(h->M, h->nTiles, h->derr);
+  return DNL_OK;
+}
+
+template <int NPE> int launch_mode_any(dnl_engine *h)
+{
+  switch (h->mode)
+  {
+  case DNL_MODE_STATS: return launch_mode<NPE, MODE_STATS>(h);
+  case DNL_MODE_HARVEST: return launch_mode<NPE, MODE_HARVEST>(h);
+  default: return launch_mode<NPE, MODE_GUESS>(h);
+  }
+}
+
 template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
 {
   const Variant &vv = variant_of(h, v);
@@ -262,6 +295,8 @@ int launch_element_any(dnl_engine *h, int mode)
         k_element_start<double, 4><<<blocks, TILE, 0, h->stream>>>(h->M);
     }
   }
+  else if (h->mode != DNL_MODE_PLAIN)
+    rc = h->npe == 8 ? launch_mode_any<8>(h) : launch_mode_any<4>(h);
   else if (h->npe == 4)
   {
     // the axisymmetric models are small: one plain variant
@@ -655,6 +690,17 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.slot = slot;
   cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
   cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream);
+  if ((rc = dalloc(h, &h->dstats, 4)))
+  {
+    std::string e = h->err;
+    dnl_engine_destroy(h);
+    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+    return rc;
+  }
+  cudaMemsetAsync(h->dstats, 0, 4 * sizeof(unsigned long long), h->stream);
+  M.stats = h->dstats;
+  M.harvest_count = h->dstats + 3;
+  M.harvest_stride = 1;
   h->variant = 0;
   h->powerIteration = (descs[0]->ts_method == DNL_TS_POWER_ITERATION);
   if (h->powerIteration)
@@ -1255,5 +1301,94 @@ int dnl_engine_timings(const dnl_engine *h, double out[4])
 }
 
 int64_t dnl_engine_launch_count(const dnl_engine *h) { return h ? h->launches : 0; }
+
+namespace
+{
+void drop_graph(dnl_engine *h)
+{
+  if (h->graphExec)
+  {
+    cudaGraphExecDestroy(h->graphExec);
+    cudaGraphDestroy(h->graph);
+    h->graphExec = nullptr;
+    h->graph = nullptr;
+  }
+}
+} // namespace
+
+int dnl_engine_set_mode(dnl_engine *h, int32_t mode)
+{
+  if (!h || mode < DNL_MODE_PLAIN || mode > DNL_MODE_GUESS)
+    return DNL_ERR_ARG;
+  if (mode != DNL_MODE_PLAIN && h->precision != DNL_PREC_MIXED)
+    return fail(h, DNL_ERR_UNSUPPORTED, "element-pass modes run on the mixed-precision path");
+  if (mode == DNL_MODE_GUESS && !h->mlpImage)
+    return fail(h, DNL_ERR_ARG, "no guess network: call dnl_engine_set_guess_network first");
+  if (mode == DNL_MODE_HARVEST && !h->M.harvest)
+    return fail(h, DNL_ERR_ARG, "no harvest buffer: call dnl_engine_set_harvest first");
+  h->mode = mode;
+  drop_graph(h);
+  return DNL_OK;
+}
+
+int dnl_engine_set_guess_network(dnl_engine *h, const dnl_mlp *net)
+{
+  if (!h || !net)
+    return DNL_ERR_ARG;
+  std::vector<unsigned char> img(mlp::IMAGE_BYTES);
+  mlp::build_image(*net, img.data());
+  if (!h->mlpImage)
+  {
+    int rc = dalloc(h, reinterpret_cast<unsigned char **>(&h->mlpImage), mlp::IMAGE_BYTES);
+    if (rc)
+      return rc;
+  }
+  CK(cudaMemcpyAsync(h->mlpImage, img.data(), mlp::IMAGE_BYTES, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->M.mlp_image = h->mlpImage;
+  drop_graph(h);
+  return DNL_OK;
+}
+
+int dnl_engine_set_harvest(dnl_engine *h, float *d_pairs, int64_t capacity, int32_t stride)
+{
+  if (!h || (!d_pairs && capacity > 0) || capacity < 0 || stride < 1)
+    return DNL_ERR_ARG;
+  h->M.harvest = d_pairs;
+  h->M.harvest_cap = capacity;
+  h->M.harvest_stride = stride;
+  CK(cudaMemsetAsync(h->dstats + 3, 0, sizeof(unsigned long long), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  drop_graph(h);
+  return DNL_OK;
+}
+
+int dnl_engine_harvest_count(dnl_engine *h, int64_t *count)
+{
+  if (!h || !count)
+    return DNL_ERR_ARG;
+  unsigned long long n = 0;
+  CK(cudaMemcpyAsync(&n, h->dstats + 3, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *count = (int64_t)std::min<unsigned long long>(n, (unsigned long long)h->M.harvest_cap);
+  return DNL_OK;
+}
+
+int dnl_engine_newton_stats(dnl_engine *h, int64_t out[3], int32_t reset)
+{
+  if (!h || !out)
+    return DNL_ERR_ARG;
+  unsigned long long v[3];
+  CK(cudaMemcpyAsync(v, h->dstats, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < 3; k++)
+    out[k] = (int64_t)v[k];
+  if (reset)
+  {
+    CK(cudaMemsetAsync(h->dstats, 0, sizeof(v), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return DNL_OK;
+}
 
 } // extern "C"

@@ -191,6 +191,41 @@ class ModelDesc:
         return c
 
 
+MLP_IN, MLP_HIDDEN, MLP_PAIR_WORDS = 5, 64, 8
+MODE_PLAIN, MODE_STATS, MODE_HARVEST, MODE_GUESS = 0, 1, 2, 3
+
+
+class Mlp(ctypes.Structure):
+    """dnl_mlp: the learned initial guess of the radial return (FP32 weights)."""
+    _fields_ = [("w1", (ctypes.c_float * 16) * MLP_HIDDEN), ("b1", ctypes.c_float * MLP_HIDDEN),
+                ("w2", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b2", ctypes.c_float * MLP_HIDDEN),
+                ("w3", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b3", ctypes.c_float * MLP_HIDDEN),
+                ("w4", ctypes.c_float * MLP_HIDDEN), ("b4", ctypes.c_float),
+                ("in_mean", ctypes.c_float * MLP_IN), ("in_scale", ctypes.c_float * MLP_IN)]
+
+    NPARAM = 64 * 16 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
+    _LAYOUT = (("w1", (64, 16)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)), ("w3", (64, 64)),
+               ("b3", (64,)), ("w4", (64,)), ("b4", ()), ("in_mean", (5,)), ("in_scale", (5,)))
+
+    def to_dict(self):
+        import numpy as np
+        a = np.frombuffer(bytes(self), dtype=np.float32)
+        out, off = {}, 0
+        for name, shape in self._LAYOUT:
+            n = int(np.prod(shape)) if shape else 1
+            out[name] = a[off:off + n].reshape(shape).copy() if shape else np.float32(a[off])
+            off += n
+        return out
+
+    @classmethod
+    def from_dict(cls, d):
+        import numpy as np
+        buf = np.concatenate([np.asarray(d[k], dtype=np.float32).ravel() for k, _ in cls._LAYOUT])
+        m = cls()
+        ctypes.memmove(ctypes.addressof(m), buf.ctypes.data, buf.nbytes)
+        return m
+
+
 def material(young, poisson, density, heat_capacity, taylor_quinney, T0, A, B, C, n, m, depsp0, Tm, Tref):
     return dict(young=young, poisson=poisson, density=density, heat_capacity=heat_capacity,
                 taylor_quinney=taylor_quinney, T0=T0, A=A, B=B, C=C, n=n, m=m, depsp0=depsp0, Tm=Tm, Tref=Tref)
@@ -237,6 +272,16 @@ def load_library():
         "dnl_engine_set_variant": (ctypes.c_int, [vp, i32]),
         "dnl_element_pass_static": (ctypes.c_int, [i32, i32, i32, vp, vp, vp, ctypes.POINTER(Material),
                                                    dbl, vp, vp, vp]),
+        "dnl_engine_set_mode": (ctypes.c_int, [vp, i32]),
+        "dnl_engine_set_guess_network": (ctypes.c_int, [vp, ctypes.POINTER(Mlp)]),
+        "dnl_engine_set_harvest": (ctypes.c_int, [vp, vp, i64, i32]),
+        "dnl_engine_harvest_count": (ctypes.c_int, [vp, ctypes.POINTER(i64)]),
+        "dnl_engine_newton_stats": (ctypes.c_int, [vp, ctypes.POINTER(i64), i32]),
+        "dnl_mlp_forward": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, i64, vp, vp]),
+        "dnl_mlp_gradients": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, vp, i64, ctypes.POINTER(Mlp),
+                                             ctypes.POINTER(ctypes.c_float), vp]),
+        "dnl_mlp_train": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, vp, i64, i32, i32, ctypes.c_float,
+                                         ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -117,6 +117,29 @@ class Engine:
     def launch_count(self):
         return int(self._lib.dnl_engine_launch_count(self.h))
 
+    # ---- learned initial guess of the radial return
+    def set_mode(self, mode):
+        self._check(self._lib.dnl_engine_set_mode(self.h, int(mode)))
+
+    def set_guess_network(self, net):
+        self._check(self._lib.dnl_engine_set_guess_network(self.h, ctypes.byref(net)))
+
+    def set_harvest(self, d_pairs_ptr, capacity, stride):
+        """d_pairs_ptr: device pointer of capacity*8 float32 (e.g. a torch tensor's data_ptr())."""
+        self._check(self._lib.dnl_engine_set_harvest(self.h, ctypes.c_void_p(d_pairs_ptr), int(capacity),
+                                                     int(stride)))
+
+    def harvest_count(self):
+        n = ctypes.c_int64()
+        self._check(self._lib.dnl_engine_harvest_count(self.h, ctypes.byref(n)))
+        return n.value
+
+    def newton_stats(self, reset=False):
+        """(yield-function evaluations, yielding points, points started from the guess)."""
+        out = (ctypes.c_int64 * 3)()
+        self._check(self._lib.dnl_engine_newton_stats(self.h, out, int(bool(reset))))
+        return tuple(int(v) for v in out)
+
     def close(self):
         if getattr(self, "h", None):
             self._lib.dnl_engine_destroy(self.h)

@@ -207,3 +207,73 @@ def taylor_batch(n=256, seed=20261203, elems=(2000, 60000), speed=(150000.0, 300
         descs.append(taylor_3d(n_core=n_core, n_ring=n_ring, n_axial=n_axial, speed=v, mat=mat, t_end=t_end,
                                ts_freq=ts_freq, precision=precision))
     return descs
+
+
+def _pull_end(coords, length, speed, t_end, ramp_frac):
+    """Symmetry plane y = 0 restrained along y; the end y = length pulled at
+    `speed` along y, ramped linearly from 0 over the first ramp_frac of the run
+    (a DiscreteFunction on the imposed speed, Boundary::setFunction)."""
+    nN = coords.shape[0]
+    bc = np.zeros((nN, 3), np.int8)
+    val = np.zeros((nN, 3))
+    fun = -np.ones((nN, 3), np.int32)
+    bc[coords[:, 1] <= 1e-9, 1] = _abi.BC_RESTRAIN
+    top = coords[:, 1] >= length - 1e-9
+    bc[top, 1] = _abi.BC_SPEED
+    val[top, 1] = speed
+    fun[top, 1] = 0
+    ramp = (np.array([0.0, ramp_frac * t_end, 2.0 * t_end]), np.array([0.0, 1.0, 1.0]))
+    return dict(bc_code=bc, bc_value=val, bc_func=fun, functions=[ramp], v_init=np.zeros((nN, 3)))
+
+
+def necking_end_time(elongation, speed, ramp_frac):
+    """Time at which an end pulled at `speed`, ramped over the first ramp_frac
+    of the run, has moved by `elongation`."""
+    return elongation / (speed * (1.0 - 0.5 * ramp_frac))
+
+
+def bar_necking(n_core=24, n_ring=34, n_axial=312, radius=6.413, length=26.667, reduction=0.01, speed=5000.0,
+                elongation=7.0, ramp_frac=0.1, mat=STEEL_NECKING, precision=_abi.PREC_MIXED, ts_freq=10):
+    """Round bar in tension, half of it (y >= 0, symmetry plane y = 0): an
+    O-grid cross-section extruded along y, the radius reduced by `reduction`
+    at y = 0 and tapered back to `radius` at y = length / 3 (the notch zone of
+    Samples/BarNecking/BarNecking-3D/BarNecking.py).  The end is pulled at
+    `speed` (mm/s), ramped over the first ramp_frac of the run, up to
+    `elongation` mm.  Defaults: 3,840 x 312 = 1,198,080 elements."""
+    pts, quads = ogrid_section(1.0, n_core, n_ring)
+    coords, conn = _extrude(pts, quads, n_axial, length)
+    zone = length / 3.0
+    r = radius * (1.0 - reduction * np.clip(1.0 - coords[:, 1] / zone, 0.0, 1.0))
+    coords[:, 0] *= r
+    coords[:, 2] *= r
+    t_end = necking_end_time(elongation, speed, ramp_frac)
+    return _abi.ModelDesc(_abi.ELHEX8N3D, coords, conn, [mat], t_end=t_end, ts_freq=ts_freq, precision=precision,
+                          **_pull_end(coords, length, speed, t_end, ramp_frac))
+
+
+def _block(nx, ny, nz, x0, x1, y0, y1, z0, z1):
+    """Structured hex8 block (vectorised), nodes x fastest then z then y
+    (layer by layer along y)."""
+    xs, ys, zs = np.linspace(x0, x1, nx + 1), np.linspace(y0, y1, ny + 1), np.linspace(z0, z1, nz + 1)
+    gy, gz, gx = np.meshgrid(ys, zs, xs, indexing="ij")
+    coords = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+    idx = np.arange(coords.shape[0]).reshape(ny + 1, nz + 1, nx + 1)
+    j, k, i = np.meshgrid(np.arange(ny), np.arange(nz), np.arange(nx), indexing="ij")
+    j, k, i = j.ravel(), k.ravel(), i.ravel()
+    conn = np.stack([idx[j, k, i], idx[j, k, i + 1], idx[j, k + 1, i + 1], idx[j, k + 1, i],
+                     idx[j + 1, k, i], idx[j + 1, k, i + 1], idx[j + 1, k + 1, i + 1], idx[j + 1, k + 1, i]], axis=1)
+    return coords, _fix_hex_orientation(coords, conn)
+
+
+def plate_necking(nx=128, nz=12, ny=320, width=10.0, thickness=1.0, length=25.0, reduction=0.01, speed=5000.0,
+                  elongation=7.0, ramp_frac=0.1, mat=STEEL_NECKING, precision=_abi.PREC_MIXED, ts_freq=10):
+    """Flat plate in tension, half of it (y >= 0, symmetry plane y = 0),
+    width x thickness cross-section centred on the y axis, the width reduced
+    by `reduction` at y = 0 and tapered back at y = length / 3; end pulled as
+    in bar_necking.  Defaults: 128 x 12 x 320 = 491,520 elements."""
+    coords, conn = _block(nx, ny, nz, -0.5 * width, 0.5 * width, 0.0, length, -0.5 * thickness, 0.5 * thickness)
+    zone = length / 3.0
+    coords[:, 0] *= 1.0 - reduction * np.clip(1.0 - coords[:, 1] / zone, 0.0, 1.0)
+    t_end = necking_end_time(elongation, speed, ramp_frac)
+    return _abi.ModelDesc(_abi.ELHEX8N3D, coords, conn, [mat], t_end=t_end, ts_freq=ts_freq, precision=precision,
+                          **_pull_end(coords, length, speed, t_end, ramp_frac))

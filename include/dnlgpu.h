@@ -251,6 +251,74 @@ int dnl_element_pass_static(int32_t elem_type, int32_t n_nodes, int32_t n_elems,
                             const double *d_du, const int32_t *d_conn, const dnl_material *material,
                             double time_step, double *d_ips, double *d_force, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Learned Newton initial guess of the radial return.  No counterpart in the
+ * reference (its return starts from the previous increment's gamma,
+ * Element.C:507-515).  A 5 -> 64 -> 64 -> 64 -> 1 SiLU network maps the trial
+ * state of a yielding Gauss point to r = gamma / gamma_max, with gamma_max =
+ * (sigma_trial - sigma_y) / (sqrt(3/2) 2G) the upper end of the bracket the
+ * return starts with (a yield stress that falls during the increment can take
+ * gamma past it).  The return starts from min(max(r, 0), 2) * gamma_max and
+ * keeps its own bracket and stopping tests, so it converges to the same root
+ * (the network only changes the iterations).
+ * Inputs, computed in FP32 from the point state before the return:
+ *   x0 = sigma_trial / A, x1 = eps_p, x2 = ln(1 + depsp / depsp0),
+ *   x3 = T / Tm, x4 = ln(3 G dt depsp0 / A)
+ * and normalised as (x - in_mean) * in_scale.  The hidden layers run as BF16
+ * tensor-core products with FP32 accumulation; the output layer in FP32.
+ * Weights are FP32 here and rounded to BF16 on the device. */
+#define DNL_MLP_IN 5
+#define DNL_MLP_HIDDEN 64
+typedef struct dnl_mlp {
+  float w1[DNL_MLP_HIDDEN][16]; /* inputs 5..15 unused (zero) */
+  float b1[DNL_MLP_HIDDEN];
+  float w2[DNL_MLP_HIDDEN][DNL_MLP_HIDDEN];
+  float b2[DNL_MLP_HIDDEN];
+  float w3[DNL_MLP_HIDDEN][DNL_MLP_HIDDEN];
+  float b3[DNL_MLP_HIDDEN];
+  float w4[DNL_MLP_HIDDEN];
+  float b4;
+  float in_mean[DNL_MLP_IN];
+  float in_scale[DNL_MLP_IN];
+} dnl_mlp;
+
+/* One training pair as harvested from the radial return: the 5 raw inputs,
+ * the target r, the converged gamma and gamma_max. */
+#define DNL_MLP_PAIR_WORDS 8
+
+/* Element-pass mode of the engine (mixed precision, hex8 and axisymmetric):
+ * DNL_MODE_PLAIN the tuned variants; DNL_MODE_STATS the same return with its
+ * Newton iterations counted; DNL_MODE_HARVEST counting + training pairs
+ * written to the buffer of dnl_engine_set_harvest; DNL_MODE_GUESS counting +
+ * the network of dnl_engine_set_guess_network as the first iterate. */
+enum { DNL_MODE_PLAIN = 0, DNL_MODE_STATS = 1, DNL_MODE_HARVEST = 2, DNL_MODE_GUESS = 3 };
+int dnl_engine_set_mode(dnl_engine *h, int32_t mode);
+int dnl_engine_set_guess_network(dnl_engine *h, const dnl_mlp *net);
+/* d_pairs: caller-owned device array of capacity*DNL_MLP_PAIR_WORDS floats; one
+ * yielding point in `stride` (chosen by a hash of point and increment) is kept
+ * until the buffer is full.  Resets the pair count. */
+int dnl_engine_set_harvest(dnl_engine *h, float *d_pairs, int64_t capacity, int32_t stride);
+int dnl_engine_harvest_count(dnl_engine *h, int64_t *count);
+/* Since the last reset: [0] yield-function evaluations of the returns,
+ * [1] yielding points, [2] points that started from the network's guess. */
+int dnl_engine_newton_stats(dnl_engine *h, int64_t out[3], int32_t reset);
+
+/* Network kernels (BF16 tensor-core products, FP32 accumulation), on
+ * caller-owned device arrays, on `stream` (NULL: default), synchronous.
+ * d_x [n*5] raw inputs, d_y [n] outputs. */
+int dnl_mlp_forward(const dnl_mlp *net, const float *d_x, int64_t n, float *d_y, void *stream);
+/* Gradient of the mean squared error (1/n) sum (y - t)^2 over n samples
+ * (d_t [n]) with respect to every weight and bias, into *grad (host); *loss
+ * receives the mean squared error.  in_mean / in_scale are not trained. */
+int dnl_mlp_gradients(const dnl_mlp *net, const float *d_x, const float *d_t, int64_t n, dnl_mlp *grad,
+                      float *loss, void *stream);
+/* Adam training (FP32 master weights, BF16 products) on n pairs d_x / d_t:
+ * `epochs` passes over a seeded shuffle in minibatches of batch_tiles*128
+ * pairs.  *net is the initial network on entry and the trained one on return;
+ * loss_history [epochs] (host, may be NULL) receives each epoch's mean loss. */
+int dnl_mlp_train(dnl_mlp *net, const float *d_x, const float *d_t, int64_t n, int32_t epochs, int32_t batch_tiles,
+                  float learning_rate, uint64_t seed, float *loss_history, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

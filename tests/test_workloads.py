@@ -117,3 +117,62 @@ def test_taylor3d_whole_run_mixed_against_fp64():
     assert abs(L - L64) <= 1e-4 * L64 and abs(R - R64) <= 1e-4 * R64
     assert abs(ep - ep64) <= 1e-3 * ep64
     assert L64 < 0.7 * 32.4 and R64 > 1.8 * 3.2  # a mushroomed bar
+
+
+def test_necking_generators():
+    b = meshes.bar_necking(n_core=6, n_ring=8, n_axial=30)
+    assert b.n_elems == (36 + 4 * 6 * 8) * 30
+    face = b.coords[:, 1] == 0.0
+    r0 = np.sqrt(b.coords[face, 0] ** 2 + b.coords[face, 2] ** 2).max()
+    top = b.coords[:, 1] == b.coords[:, 1].max()
+    r1 = np.sqrt(b.coords[top, 0] ** 2 + b.coords[top, 2] ** 2).max()
+    assert abs(r0 - 0.99 * 6.413) < 1e-9 and abs(r1 - 6.413) < 1e-9
+    assert np.all(b.bc_code[face, 1] == _abi.BC_RESTRAIN) and np.all(b.bc_code[top, 1] == _abi.BC_SPEED)
+    # 7 mm of elongation at 5 m/s after a ramp over the first 10% of the run
+    assert abs(b.t_end - 7.0 / (5000.0 * 0.95)) < 1e-15
+    fx, fy = b.functions[0]
+    assert np.interp(0.05 * b.t_end, fx, fy) == pytest.approx(0.5) and np.interp(0.5 * b.t_end, fx, fy) == 1.0
+    p = meshes.plate_necking(nx=16, nz=2, ny=40)
+    assert p.n_elems == 16 * 2 * 40
+    pf = p.coords[:, 1] == 0.0
+    assert abs(p.coords[pf, 0].max() - 0.99 * 5.0) < 1e-12
+    assert abs(p.coords[:, 2].max() - 0.5) < 1e-12
+
+
+def neck_radius(desc, coords):
+    face = desc.coords[:, 1] == 0.0
+    return np.sqrt(coords[face, 0] ** 2 + coords[face, 2] ** 2).max()
+
+
+@pytest.mark.gpu
+def test_bar_necking_matches_oracle():
+    """The pulled bar (imposed speed ramped by a discrete function) against the
+    oracle over its first increments, FP64."""
+    import oracle
+    d = meshes.bar_necking(n_core=4, n_ring=4, n_axial=20, precision=_abi.PREC_FP64)
+    with oracle.OracleModel(d) as o, engine(d) as e:
+        o.init()
+        e.init()
+        o.run(max_incs=40)
+        e.run(max_incs=40)
+        assert e.control()["increment"] == o.control()["increment"] == 40
+        assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), o.nodes(_abi.NODE_COORDS)) < 1e-12
+        assert helpers.field_errors(e.ips(), o.ips()).max() < 1e-8
+
+
+@pytest.mark.gpu
+def test_bar_necking_whole_run_mixed_against_fp64():
+    """A 13,680-element bar pulled by 7 mm: the mixed path's neck radius and
+    maximum plastic strain against the FP64 path's."""
+    out = {}
+    for prec in (_abi.PREC_FP64, _abi.PREC_MIXED):
+        d = meshes.bar_necking(n_core=6, n_ring=8, n_axial=60, precision=prec)
+        with engine(d) as e:
+            e.init()
+            e.run()
+            c = e.control()
+            assert c["status"] == 0 and c["time"] == pytest.approx(d.t_end, rel=1e-12)
+            out[prec] = (neck_radius(d, e.nodes(_abi.NODE_COORDS)), e.ips()[_abi.IP_EPSP].max())
+    (r64, ep64), (r, ep) = out[_abi.PREC_FP64], out[_abi.PREC_MIXED]
+    assert r64 < 0.99 * 6.413  # the bar has thinned at the notch
+    assert abs(r - r64) <= 1e-4 * r64 and abs(ep - ep64) <= 1e-3 * ep64
