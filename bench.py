@@ -48,6 +48,7 @@ def parse():
                    help="element-pass variant (0-3); default: chosen by the autotuner")
     p.add_argument("--no-accuracy", action="store_true", help="skip the whole-run mixed/FP64 comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
+    p.add_argument("--no-guess", action="store_true", help="skip the learned Newton initial guess block")
     p.add_argument("--batch-fp64-sample", type=int, default=32,
                    help="instances of the batch timed one by one on the FP64 path")
     p.add_argument("--axial", type=int, default=160,
@@ -306,6 +307,32 @@ def batch_run(sample):
     return out
 
 
+def guess_run():
+    """The learned Newton initial guess: pairs harvested from the first-yield
+    returns of the 256-bar batch (its first 1,500 increments), the network
+    trained on ln(gamma / gamma_max) by the engine's tensor-core kernels, then
+    the same increments run from the same state with the reference's start
+    and with the network's, on the first-yield window of the 3-D bar
+    (increments 0-400) and of the necking plate (491,520 elements,
+    increments 6,000-8,000)."""
+    from dnlPython import _abi, guess, meshes
+    t0 = time.perf_counter()
+    pairs, st = guess.harvest(meshes.taylor_batch(), capacity=10_000_000, stride=1, max_incs=1500,
+                              scope=_abi.GUESS_FIRST_YIELD)
+    t1 = time.perf_counter()
+    net, hist = guess.train(pairs, epochs=20, batch_tiles=128, learning_rate=1e-3, log_target=True)
+    t2 = time.perf_counter()
+    out = {"pairs": int(pairs.shape[0]), "harvest_s": t1 - t0, "train_s": t2 - t1,
+           "loss_first_last": [hist[0], hist[-1]], "scope": "first yield (eps_p = 0)",
+           "harvest_plain_evals_per_first_yield_point": st[3] / max(st[2], 1)}
+    del pairs
+    for name, desc, warm, incs in (("taylor3d_153600", workload("mixed"), 0, 400),
+                                   ("plate_necking_491520", meshes.plate_necking(), 6000, 2000)):
+        out[name] = guess.compare(desc, net, warm, incs, scope=_abi.GUESS_FIRST_YIELD)
+        out[name]["window"] = [warm, warm + incs]
+    return out
+
+
 # ------------------------------------------------------------------ arms
 
 def run_reference_arm(args, rank):
@@ -457,6 +484,8 @@ def run_engine_arm(args, rank, world, dist):
         out["accuracy_whole_run"] = accuracy_run()
     if world == 1 and not args.no_batch:
         out["batched"] = batch_run(args.batch_fp64_sample)
+    if world == 1 and AXIAL == 160 and not args.no_guess:
+        out["learned_guess"] = guess_run()
     print(json.dumps(out))
 
 

@@ -43,7 +43,7 @@ struct __align__(128) Ctl
   int status, bad, resolves, ts_freq;
   double safety, omegaS, alphaM, beta, gammaN;
   int elem_begin, elem_end, node_begin, node_end;
-  int ts_method, pi_iters, pad0, pad1;
+  int ts_method, pi_iters, direct, pad1; // direct: one-step return (Element::computeStressDirect)
   double pi_fmax, pi_omega; // power iteration: Model::_powerIterationFreqMax, last omega_max
   double dt_last;           // time step of the last completed increment
 };
@@ -83,11 +83,13 @@ struct DevModel
   double *blockmax;        // [gridDim] per-block max |v|
   // element-pass modes (learned initial guess, Newton statistics, training pairs)
   const void *mlp_image;   // network image (dnl_mlp.cuh)
-  unsigned long long *stats; // [0] yield-function evaluations, [1] yielding points, [2] guesses used
+  unsigned long long *stats; // [0] yield-function evaluations and [1] yielding points, [2] and [3] the same
+                             // over the points of the guess scope
   float *harvest;          // pairs of DNL_MLP_PAIR_WORDS floats
   unsigned long long *harvest_count;
   long long harvest_cap;
-  int harvest_stride, pad1;
+  int harvest_stride;
+  int guess_scope;         // DNL_GUESS_ALL or DNL_GUESS_FIRST_YIELD
 };
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
@@ -555,7 +557,8 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
     JC<R> jc;
     jc.load(mp);
     bool ok;
-    iters = radial_return<R>(jc, R(mp.twoG), R(mp.heatFrac), R(1.0 / mp.rho0), dE, R(dt), st, ok, gamma0);
+    iters = radial_return<R>(jc, R(mp.twoG), R(mp.heatFrac), R(1.0 / mp.rho0), dE, R(dt), st, ok, gamma0,
+                             C->direct != 0);
     if (!ok)
     {
       if constexpr (sizeof(R) == 4)
@@ -897,7 +900,7 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
   mlp::Tile net;
   if constexpr (MODE == MODE_GUESS)
     mlp::tile_setup(net, dyn, M.mlp_image, &bar, &tslot, err);
-  unsigned long long nEval = 0, nPlastic = 0, nGuess = 0;
+  unsigned long long nEval = 0, nPlastic = 0, nScope = 0, nScopeEval = 0;
   for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x)
   {
     const int q = tile * TILE + t;
@@ -913,7 +916,7 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
     Front<R> f;
     float x[mlp::NIN] = {0.f, 0.f, 0.f, 0.f, 0.f};
     float gmax = 0.f;
-    bool plastic = false;
+    bool plastic = false, scope = false;
     if (act)
     {
       element_front<R, NPE>(io, C, e, g, base, amask, M.conn[q], old, row, f);
@@ -924,6 +927,8 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
       R Strial, y0;
       trial_state<R>(jc, twoG, f.dE, f.st, dt, Strial, y0);
       plastic = Strial > y0;
+      // first yield: no previous gamma to start from (Element.C:507-515)
+      scope = plastic && (M.guess_scope == DNL_GUESS_ALL || f.st.epsp == R(0));
       if (plastic)
       {
         gmax = (Strial - y0) / (R(1.2247448713915890491) * twoG);
@@ -934,14 +939,11 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
     if constexpr (MODE == MODE_GUESS)
     {
       __syncwarp();
-      if (__syncthreads_or(plastic))
+      if (__syncthreads_or(scope))
       {
         const float y = net.forward(t, x);
-        if (plastic)
-        {
-          gamma0 = fminf(fmaxf(y, 0.f), 2.f) * gmax;
-          nGuess++;
-        }
+        if (scope)
+          gamma0 = fminf(fmaxf(mlp::ratio(net, y), 0.f), 2.f) * gmax;
       }
     }
     if (act)
@@ -951,11 +953,16 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
       {
         nEval += evals;
         nPlastic++;
+        if (scope)
+        {
+          nScopeEval += evals;
+          nScope++;
+        }
       }
       if constexpr (MODE == MODE_HARVEST)
       {
         const unsigned h = (unsigned)q * 2654435761u ^ (unsigned)C->inc * 40503u;
-        if (plastic && evals > 0 && gmax > 0.f && (h >> 7) % (unsigned)M.harvest_stride == 0u)
+        if (scope && evals > 0 && gmax > 0.f && (h >> 7) % (unsigned)M.harvest_stride == 0u)
         {
           const unsigned long long k = atomicAdd(M.harvest_count, 1ull);
           if ((long long)k < M.harvest_cap)
@@ -975,13 +982,15 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
   {
     nEval += __shfl_xor_sync(0xffffffffu, nEval, o);
     nPlastic += __shfl_xor_sync(0xffffffffu, nPlastic, o);
-    nGuess += __shfl_xor_sync(0xffffffffu, nGuess, o);
+    nScope += __shfl_xor_sync(0xffffffffu, nScope, o);
+    nScopeEval += __shfl_xor_sync(0xffffffffu, nScopeEval, o);
   }
   if (lane == 0 && nPlastic)
   {
     atomicAdd(M.stats + 0, nEval);
     atomicAdd(M.stats + 1, nPlastic);
-    atomicAdd(M.stats + 2, nGuess);
+    atomicAdd(M.stats + 2, nScope);
+    atomicAdd(M.stats + 3, nScopeEval);
   }
   if constexpr (MODE == MODE_GUESS)
     mlp::tile_release(net);

@@ -360,9 +360,13 @@ __device__ __forceinline__ void trial_state(const JC<R> &jc, R twoG, const R dE[
 // as the first iterate; the bracket and the stopping tests are unchanged.
 // Returns the number of yield-function evaluations of the iteration (0 for an
 // elastic point).
+// direct: Element::computeStressDirect (Element.C:625-850) instead, one step
+// gamma = (|s*| - sqrt(2/3) sigma_y) / (2G (1 + h / (3G))) with the slope h at
+// the previous plastic strain (or 1e-8) and rate and the initial temperature,
+// then the yield stress at the new state (1 evaluation).
 template <typename R>
 __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac, R inv_rho0, const R dE[6], R dt,
-                                             ReturnState<R> &st, bool &ok, R gamma0 = R(-1))
+                                             ReturnState<R> &st, bool &ok, R gamma0 = R(-1), bool direct = false)
 {
   const R SQ32 = R(1.2247448713915890491), SQ23 = R(0.81649658092772603273);
   const R gammaInitial = R(1e-8);
@@ -402,7 +406,28 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
     jc.eval(gammaInitial, gammaInitial / dt, T, dt, yield, dummy, false);
     st.yield = yield;
   }
-  if (Strial > yield)
+  if (Strial > yield && direct)
+  {
+    R dummy, hard;
+    jc.eval(epsp0 > R(0) ? epsp0 : gammaInitial, st.depsp, T0, dt, dummy, hard, true);
+    gamma = (Snorm - SQ23 * yield) / (twoG * (R(1) + hard / (R(1.5) * twoG)));
+    const R depsp = SQ23 * gamma / dt, epsp = epsp0 + SQ23 * gamma;
+    T = T0 + R(0.5) * gamma * heatFrac * (SQ23 * yield + Snorm0);
+    jc.eval(epsp, depsp, T, dt, yield, dummy, false);
+    const R invS = R(1) / Snorm;
+    const R scale = R(1) - twoG * gamma * invS;
+    st.kplast = gamma * invS / scale;
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      dev[c] *= scale;
+    st.epsp = epsp;
+    st.depsp = depsp;
+    st.gamma = gamma;
+    st.gcum += gamma;
+    st.yield = yield;
+    iterate = 1;
+  }
+  else if (Strial > yield)
   {
     R gammaMin = R(0);
     R gammaMax = (Strial - yield) / twoG32;

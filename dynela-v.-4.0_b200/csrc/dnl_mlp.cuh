@@ -30,7 +30,7 @@ constexpr uint32_t OFF_B1 = OFF_W3 + H * H * 2;   // fp32 biases
 constexpr uint32_t OFF_B2 = OFF_B1 + H * 4;
 constexpr uint32_t OFF_B3 = OFF_B2 + H * 4;
 constexpr uint32_t OFF_W4 = OFF_B3 + H * 4;       // fp32 output weights
-constexpr uint32_t OFF_MISC = OFF_W4 + H * 4;     // b4, in_mean[5], in_scale[5], pad
+constexpr uint32_t OFF_MISC = OFF_W4 + H * 4;     // b4, in_mean[5], in_scale[5], out_exp, pad
 constexpr uint32_t IMAGE_BYTES = OFF_MISC + 16 * 4;
 // training adds the transposed hidden weights (for dh = dz W), after the image
 constexpr uint32_t OFF_W2T = 0, OFF_W3T = H * H * 2, TRANS_BYTES = 2 * H * H * 2;
@@ -270,6 +270,13 @@ struct Tile
   }
 };
 
+// r = gamma / gamma_max from the network's output (linear, or exp of a
+// network trained on ln r)
+__device__ __forceinline__ float ratio(const Tile &T, float y)
+{
+  return reinterpret_cast<const float *>(T.smem + OFF_MISC)[11] != 0.0f ? __expf(fminf(y, 1.0f)) : y;
+}
+
 // Block set-up: the image into shared memory by one bulk copy, the mbarrier,
 // the tensor-memory columns.  Returns false (and flags err) when the copy did
 // not land in time.
@@ -356,6 +363,7 @@ inline void build_image(const dnl_mlp &n, unsigned char *img)
     misc[1 + i] = n.in_mean[i];
     misc[6 + i] = n.in_scale[i];
   }
+  misc[11] = n.out_exp;
   memcpy(img + OFF_MISC, misc, sizeof(misc));
 }
 

@@ -58,7 +58,7 @@ struct dnl_engine
   int piGrid = 0;
   int mode = DNL_MODE_PLAIN;          // element-pass mode (DNL_MODE_*)
   void *mlpImage = nullptr;           // learned-guess network image
-  unsigned long long *dstats = nullptr; // Newton statistics [3] + harvest count
+  unsigned long long *dstats = nullptr; // Newton statistics [4] + harvest count
   std::string err;
 };
 
@@ -132,6 +132,9 @@ int check_desc(const dnl_model_desc *d, int idx)
     return fail(nullptr, DNL_ERR_ARG, "model %d: no material", idx);
   if (d->ts_method != DNL_TS_COURANT && d->ts_method != DNL_TS_POWER_ITERATION)
     return fail(nullptr, DNL_ERR_UNSUPPORTED, "model %d: unknown time-step method %d", idx, d->ts_method);
+  if (d->stress_method != DNL_STRESS_NEWTON && d->stress_method != DNL_STRESS_DIRECT)
+    return fail(nullptr, DNL_ERR_UNSUPPORTED, "model %d: unknown stress computation method %d", idx,
+                d->stress_method);
   if (d->precision != DNL_PREC_FP64 && d->precision != DNL_PREC_MIXED)
     return fail(nullptr, DNL_ERR_ARG, "model %d: unknown precision %d", idx, d->precision);
   const int npe = npe_of(d->elem_type);
@@ -189,9 +192,13 @@ struct Variant
   int tma;
   int minb;
 };
-const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4}, {"tma/5", 1, 5}};
-const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2}, {"tma/3", 1, 3}};
-constexpr int kNumVariants = 4;
+// each precision: two plain budgets, then persistent staged tiles from the most
+// blocks per SM (fewest registers, most spilled) to the fewest (no spills)
+const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4},
+                                {"tma/5", 1, 5},   {"tma/3", 1, 3},   {"tma/2", 1, 2}};
+const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2},
+                                {"tma/3", 1, 3},   {"plain/2", 0, 2}, {"tma/1", 1, 1}};
+constexpr int kNumVariants = DNL_NUM_VARIANTS;
 
 const Variant &variant_of(const dnl_engine *h, int v)
 {
@@ -253,7 +260,6 @@ template <int NPE> int launch_mode_any(dnl_engine *h)
 
 template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
 {
-  const Variant &vv = variant_of(h, v);
   if (sizeof(R) == 4)
   {
     switch (v)
@@ -261,16 +267,19 @@ template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
     case 0: return launch_plain<R, NPE, 6>(h);
     case 1: return launch_plain<R, NPE, 8>(h);
     case 2: return launch_tma<R, NPE, 4>(h);
-    default: return launch_tma<R, NPE, 5>(h);
+    case 3: return launch_tma<R, NPE, 5>(h);
+    case 4: return launch_tma<R, NPE, 3>(h);
+    default: return launch_tma<R, NPE, 2>(h);
     }
   }
-  (void)vv;
   switch (v)
   {
   case 0: return launch_plain<R, NPE, 4>(h);
   case 1: return launch_plain<R, NPE, 3>(h);
   case 2: return launch_tma<R, NPE, 2>(h);
-  default: return launch_tma<R, NPE, 3>(h);
+  case 3: return launch_tma<R, NPE, 3>(h);
+  case 4: return launch_plain<R, NPE, 2>(h);
+  default: return launch_tma<R, NPE, 1>(h);
   }
 }
 
@@ -588,6 +597,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     c.safety = d->ts_safety > 0 ? d->ts_safety : 0.9;
     c.ts_freq = d->ts_freq > 0 ? d->ts_freq : 10;
     c.ts_method = d->ts_method;
+    c.direct = d->stress_method == DNL_STRESS_DIRECT;
     c.t = d->t_start;
     c.t_end = d->t_end;
     c.t_stop = d->t_end;
@@ -690,17 +700,18 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.slot = slot;
   cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
   cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream);
-  if ((rc = dalloc(h, &h->dstats, 4)))
+  if ((rc = dalloc(h, &h->dstats, 5)))
   {
     std::string e = h->err;
     dnl_engine_destroy(h);
     snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
     return rc;
   }
-  cudaMemsetAsync(h->dstats, 0, 4 * sizeof(unsigned long long), h->stream);
+  cudaMemsetAsync(h->dstats, 0, 5 * sizeof(unsigned long long), h->stream);
   M.stats = h->dstats;
-  M.harvest_count = h->dstats + 3;
+  M.harvest_count = h->dstats + 4;
   M.harvest_stride = 1;
+  M.guess_scope = DNL_GUESS_ALL;
   h->variant = 0;
   h->powerIteration = (descs[0]->ts_method == DNL_TS_POWER_ITERATION);
   if (h->powerIteration)
@@ -1256,7 +1267,7 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps)
   return check_status(h);
 }
 
-int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[4])
+int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[DNL_NUM_VARIANTS])
 {
   if (!h)
     return DNL_ERR_ARG;
@@ -1357,7 +1368,7 @@ int dnl_engine_set_harvest(dnl_engine *h, float *d_pairs, int64_t capacity, int3
   h->M.harvest = d_pairs;
   h->M.harvest_cap = capacity;
   h->M.harvest_stride = stride;
-  CK(cudaMemsetAsync(h->dstats + 3, 0, sizeof(unsigned long long), h->stream));
+  CK(cudaMemsetAsync(h->dstats + 4, 0, sizeof(unsigned long long), h->stream));
   CK(cudaStreamSynchronize(h->stream));
   drop_graph(h);
   return DNL_OK;
@@ -1368,20 +1379,29 @@ int dnl_engine_harvest_count(dnl_engine *h, int64_t *count)
   if (!h || !count)
     return DNL_ERR_ARG;
   unsigned long long n = 0;
-  CK(cudaMemcpyAsync(&n, h->dstats + 3, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(&n, h->dstats + 4, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   *count = (int64_t)std::min<unsigned long long>(n, (unsigned long long)h->M.harvest_cap);
   return DNL_OK;
 }
 
-int dnl_engine_newton_stats(dnl_engine *h, int64_t out[3], int32_t reset)
+int dnl_engine_set_guess_scope(dnl_engine *h, int32_t scope)
+{
+  if (!h || (scope != DNL_GUESS_ALL && scope != DNL_GUESS_FIRST_YIELD))
+    return DNL_ERR_ARG;
+  h->M.guess_scope = scope;
+  drop_graph(h);
+  return DNL_OK;
+}
+
+int dnl_engine_newton_stats(dnl_engine *h, int64_t out[4], int32_t reset)
 {
   if (!h || !out)
     return DNL_ERR_ARG;
-  unsigned long long v[3];
+  unsigned long long v[4];
   CK(cudaMemcpyAsync(v, h->dstats, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int k = 0; k < 3; k++)
+  for (int k = 0; k < 4; k++)
     out[k] = (int64_t)v[k];
   if (reset)
   {

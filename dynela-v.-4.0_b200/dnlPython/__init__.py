@@ -405,6 +405,7 @@ class DynELA:
         self.parallel = Parallel()
         self.saveTimes = (0.0, 0.0, 0.0)
         self.precision = _abi.PREC_MIXED if os.environ.get("DNL_PRECISION", "fp64") == "mixed" else _abi.PREC_FP64
+        self.stress_method = _abi.STRESS_NEWTON
         self._engine = None
         self._cache = {}
         self._node_index = {}
@@ -484,8 +485,14 @@ class DynELA:
         self.saveTimes = (float(start), float(end), float(inc))
 
     def setStressComputation(self, method):
-        if str(method) not in ("NR", "Newton", "NewtonRaphson", "StressIntNR"):
-            raise NotImplementedError("only the Newton-Raphson radial return is available on the accelerated path")
+        """DynELA::setStressComputation (DynELA.C:1407-1431): "NewtonRaphson"
+        or "Direct" (the one-step return of Element::computeStressDirect)."""
+        if str(method) == "Direct":
+            self.stress_method = _abi.STRESS_DIRECT
+        elif str(method) == "NewtonRaphson":
+            self.stress_method = _abi.STRESS_NEWTON
+        else:
+            raise ValueError(f"Unknown setStressComputation method : {method}")
 
     def setPrecision(self, precision):
         """Extension: 'fp64' (default, the reference's arithmetic) or 'mixed'
@@ -562,7 +569,7 @@ class DynELA:
                               bc_value=bcv, bc_func=bcf, functions=funcs, t_start=t0, t_end=t1,
                               ts_method=s.timeStepMethod, ts_freq=s.computeTimeStepFrequency,
                               ts_safety=s.timeStepSafetyFactor, rho_b=s.dissipation,
-                              precision=self.precision), node_nums, elem_nums
+                              precision=self.precision, stress_method=self.stress_method), node_nums, elem_nums
 
     # ---- solve (DynELA.C:727-773 -> Explicit::solve on the engine)
     def solve(self):

@@ -19,6 +19,8 @@ ELHEX8N3D = 2
 NODES_PER_ELEMENT = {ELQUA4NAX: 4, ELHEX8N3D: 8}
 DIMS = {ELQUA4NAX: 2, ELHEX8N3D: 3}
 
+STRESS_NEWTON, STRESS_DIRECT = 0, 1
+NUM_VARIANTS = 6  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)
 TS_COURANT = 0
 TS_POWER_ITERATION = 1
 PREC_FP64 = 0
@@ -91,7 +93,7 @@ class ModelDescC(ctypes.Structure):
         ("ts_safety", ctypes.c_double),
         ("rho_b", ctypes.c_double),
         ("precision", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("stress_method", ctypes.c_int32),
     ]
 
 
@@ -115,7 +117,8 @@ class ModelDesc:
 
     def __init__(self, elem_type, coords, conn, materials, elem_mat=None, v_init=None,
                  bc_code=None, bc_value=None, bc_func=None, functions=(), t_start=0.0, t_end=1.0,
-                 ts_method=TS_COURANT, ts_freq=10, ts_safety=0.9, rho_b=0.8182, precision=PREC_FP64):
+                 ts_method=TS_COURANT, ts_freq=10, ts_safety=0.9, rho_b=0.8182, precision=PREC_FP64,
+                 stress_method=STRESS_NEWTON):
         self.elem_type = int(elem_type)
         npe = NODES_PER_ELEMENT[self.elem_type]
         self.coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
@@ -133,6 +136,7 @@ class ModelDesc:
         self.ts_method, self.ts_freq = int(ts_method), int(ts_freq)
         self.ts_safety, self.rho_b = float(ts_safety), float(rho_b)
         self.precision = int(precision)
+        self.stress_method = int(stress_method)
         self._c = None
 
     @property
@@ -157,7 +161,7 @@ class ModelDesc:
                   bc_code=self.bc_code, bc_value=self.bc_value, bc_func=self.bc_func,
                   functions=self.functions, t_start=self.t_start, t_end=self.t_end,
                   ts_method=self.ts_method, ts_freq=self.ts_freq, ts_safety=self.ts_safety,
-                  rho_b=self.rho_b, precision=self.precision)
+                  rho_b=self.rho_b, precision=self.precision, stress_method=self.stress_method)
         kw.update(changes)
         return ModelDesc(**kw)
 
@@ -187,12 +191,14 @@ class ModelDesc:
         c.ts_method, c.ts_freq = self.ts_method, self.ts_freq
         c.ts_safety, c.rho_b = self.ts_safety, self.rho_b
         c.precision = self.precision
+        c.stress_method = self.stress_method
         self._c = c
         return c
 
 
 MLP_IN, MLP_HIDDEN, MLP_PAIR_WORDS = 5, 64, 8
 MODE_PLAIN, MODE_STATS, MODE_HARVEST, MODE_GUESS = 0, 1, 2, 3
+GUESS_ALL, GUESS_FIRST_YIELD = 0, 1
 
 
 class Mlp(ctypes.Structure):
@@ -201,11 +207,12 @@ class Mlp(ctypes.Structure):
                 ("w2", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b2", ctypes.c_float * MLP_HIDDEN),
                 ("w3", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b3", ctypes.c_float * MLP_HIDDEN),
                 ("w4", ctypes.c_float * MLP_HIDDEN), ("b4", ctypes.c_float),
-                ("in_mean", ctypes.c_float * MLP_IN), ("in_scale", ctypes.c_float * MLP_IN)]
+                ("in_mean", ctypes.c_float * MLP_IN), ("in_scale", ctypes.c_float * MLP_IN),
+                ("out_exp", ctypes.c_float)]
 
     NPARAM = 64 * 16 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
     _LAYOUT = (("w1", (64, 16)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)), ("w3", (64, 64)),
-               ("b3", (64,)), ("w4", (64,)), ("b4", ()), ("in_mean", (5,)), ("in_scale", (5,)))
+               ("b3", (64,)), ("w4", (64,)), ("b4", ()), ("in_mean", (5,)), ("in_scale", (5,)), ("out_exp", ()))
 
     def to_dict(self):
         import numpy as np
@@ -220,7 +227,7 @@ class Mlp(ctypes.Structure):
     @classmethod
     def from_dict(cls, d):
         import numpy as np
-        buf = np.concatenate([np.asarray(d[k], dtype=np.float32).ravel() for k, _ in cls._LAYOUT])
+        buf = np.concatenate([np.asarray(d.get(k, 0.0), dtype=np.float32).ravel() for k, _ in cls._LAYOUT])
         m = cls()
         ctypes.memmove(ctypes.addressof(m), buf.ctypes.data, buf.nbytes)
         return m
@@ -277,6 +284,7 @@ def load_library():
         "dnl_engine_set_harvest": (ctypes.c_int, [vp, vp, i64, i32]),
         "dnl_engine_harvest_count": (ctypes.c_int, [vp, ctypes.POINTER(i64)]),
         "dnl_engine_newton_stats": (ctypes.c_int, [vp, ctypes.POINTER(i64), i32]),
+        "dnl_engine_set_guess_scope": (ctypes.c_int, [vp, i32]),
         "dnl_mlp_forward": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, i64, vp, vp]),
         "dnl_mlp_gradients": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, vp, i64, ctypes.POINTER(Mlp),
                                              ctypes.POINTER(ctypes.c_float), vp]),

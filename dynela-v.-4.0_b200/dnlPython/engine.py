@@ -107,7 +107,7 @@ class Engine:
 
     def variant(self):
         v = ctypes.c_int32()
-        ms = np.zeros(4)
+        ms = np.zeros(_abi.NUM_VARIANTS)
         self._check(self._lib.dnl_engine_variant(self.h, ctypes.byref(v), _pd(ms)))
         return v.value, ms
 
@@ -134,9 +134,13 @@ class Engine:
         self._check(self._lib.dnl_engine_harvest_count(self.h, ctypes.byref(n)))
         return n.value
 
+    def set_guess_scope(self, scope):
+        self._check(self._lib.dnl_engine_set_guess_scope(self.h, int(scope)))
+
     def newton_stats(self, reset=False):
-        """(yield-function evaluations, yielding points, points started from the guess)."""
-        out = (ctypes.c_int64 * 3)()
+        """(yield-function evaluations, yielding points, yielding points of the
+        guess scope, their evaluations)."""
+        out = (ctypes.c_int64 * 4)()
         self._check(self._lib.dnl_engine_newton_stats(self.h, out, int(bool(reset))))
         return tuple(int(v) for v in out)
 

@@ -25,16 +25,17 @@ def _torch():
     return torch
 
 
-def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf):
+def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf, scope=_abi.GUESS_ALL):
     """Run `descs` (one model or a batch) with the plain return and keep one
-    yielding point in `stride` as a (5 inputs, r = gamma / gamma_max, gamma,
-    gamma_max) pair.  Returns a device tensor [n, 8] and the Newton statistics
-    (evaluations, yielding points, guesses) of the run."""
+    yielding point of `scope` in `stride` as a (5 inputs, r = gamma /
+    gamma_max, gamma, gamma_max) pair.  Returns a device tensor [n, 8] and the Newton statistics
+    of the run (Engine.newton_stats)."""
     torch = _torch()
     buf = torch.zeros((int(capacity), _abi.MLP_PAIR_WORDS), dtype=torch.float32, device="cuda")
     with Engine(descs) as e:
         e.init()
         e.set_harvest(buf.data_ptr(), buf.shape[0], stride)
+        e.set_guess_scope(scope)
         e.set_mode(_abi.MODE_HARVEST)
         e.run(t_pause=t_pause, max_incs=max_incs, check=False)
         n = e.harvest_count()
@@ -58,19 +59,30 @@ def initial_network(x, r, seed=1):
     return _abi.Mlp.from_dict(d)
 
 
-def train(pairs, epochs=8, batch_tiles=128, learning_rate=1e-3, seed=20261203, net=None):
+def first_yield(pairs):
+    """The pairs of points yielding for the first time (eps_p = 0): the
+    points the reference starts from gamma = 1e-8."""
+    return pairs[pairs[:, 1] == 0.0]
+
+
+def train(pairs, epochs=8, batch_tiles=128, learning_rate=1e-3, seed=20261203, net=None, log_target=False):
     """Adam training of the network on harvested pairs (device tensor [n, 8])
-    by the engine's kernels.  Returns the trained dnl_mlp and the per-epoch
-    mean squared error."""
+    by the engine's kernels, on r = gamma / gamma_max (log_target: on ln r,
+    for points whose r spans decades, such as first-yield points).  Returns
+    the trained dnl_mlp and the per-epoch mean squared error."""
     torch = _torch()
     lib = _abi.load_library()
     x = pairs[:, :_abi.MLP_IN].contiguous()
-    r = pairs[:, 5].contiguous()
+    # r past 2 (a yield stress that fell a long way during the increment) is
+    # rare and heavy-tailed; the guess is clamped to [0, 2] gamma_max anyway
+    r = pairs[:, 5].clamp(1e-6 if log_target else 0.0, 2.0)
+    r = (torch.log(r) if log_target else r).contiguous()
     n = x.shape[0]
     if net is None:
         g = torch.Generator(device=pairs.device).manual_seed(int(seed) % (2 ** 63))
-        sub = pairs[torch.randperm(n, device=pairs.device, generator=g)[:200000]].cpu().numpy()
-        net = initial_network(sub[:, :_abi.MLP_IN], sub[:, 5])
+        pick = torch.randperm(n, device=pairs.device, generator=g)[:200000]
+        net = initial_network(x[pick].cpu().numpy(), r[pick].cpu().numpy())
+    net.out_exp = 1.0 if log_target else 0.0
     hist = (ctypes.c_float * max(1, epochs))()
     rc = lib.dnl_mlp_train(ctypes.byref(net), x.data_ptr(), r.data_ptr(), n, int(epochs), int(batch_tiles),
                            float(learning_rate), int(seed), hist, None)
@@ -91,13 +103,14 @@ def predict(net, x):
     return y
 
 
-def compare(desc, net, warm_incs, incs):
+def compare(desc, net, warm_incs, incs, scope=_abi.GUESS_ALL):
     """Run `desc` to increment warm_incs with the plain return, then `incs`
     more increments once with the warm start (counted) and once from the
-    network's guess, from the same state.  Returns, per mode, the Newton
-    evaluations per yielding point, the FP64 re-solves and the element-pass
-    time per increment, and the relative differences of the guessed run's
-    stress, plastic strain and coordinates from the plain run's."""
+    network's guess (for the points of `scope`), from the same state.
+    Returns, per mode, the Newton evaluations per yielding point and per point
+    of the scope, the FP64 re-solves and the element-pass time per increment,
+    and the relative differences of the guessed run's stress, plastic strain
+    and coordinates from the plain run's."""
     out, ref = {}, None
     for name, mode in (("plain", _abi.MODE_STATS), ("guess", _abi.MODE_GUESS)):
         with Engine(desc) as e:
@@ -105,14 +118,16 @@ def compare(desc, net, warm_incs, incs):
             if warm_incs:
                 e.run(max_incs=warm_incs)
             e.set_guess_network(net)
+            e.set_guess_scope(scope)
             e.set_mode(mode)
             e.newton_stats(reset=True)
             e.set_timing(True)
             e.run(max_incs=incs)
             tm = e.timings()
-            ev, pl, gu = e.newton_stats()
+            ev, pl, sc, sev = e.newton_stats()
             c = e.control()
-            out[name] = dict(evals_per_point=ev / max(pl, 1), yielding_points=pl, guessed=gu,
+            out[name] = dict(evals_per_point=ev / max(pl, 1), yielding_points=pl, scope_points=sc,
+                             evals_per_scope_point=sev / max(sc, 1),
                              fp64_resolve_rate=c["fp64_resolves"] / max(pl, 1),
                              element_ms=tm["element_ms"] / max(incs, 1))
             ips = e.ips()

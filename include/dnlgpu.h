@@ -122,8 +122,13 @@ typedef struct dnl_model_desc {
   double ts_safety;            /* Solver::setTimeStepSafetyFactor (default 0.9) */
   double rho_b;                /* Explicit::setDissipation (default 0.8182) */
   int32_t precision;           /* DNL_PREC_* */
-  int32_t reserved;
+  int32_t stress_method;       /* DNL_STRESS_*: DynELA::setStressComputation (DynELA.C:1407-1431) */
 } dnl_model_desc;
+
+/* Radial return of Model::computeStress (Model.C:840-851): the
+ * Newton-Raphson iteration of Element::computeStress (Element.C:407-622) or
+ * the one-step return of Element::computeStressDirect (Element.C:625-850). */
+enum { DNL_STRESS_NEWTON = 0, DNL_STRESS_DIRECT = 1 };
 
 /* Solver state of one instance. */
 typedef struct dnl_control {
@@ -221,9 +226,10 @@ int64_t dnl_engine_launch_count(const dnl_engine *h);
  * and restores the state.  No counterpart in the reference (its element loop
  * has one implementation). */
 int dnl_engine_autotune(dnl_engine *h, int32_t steps);
+#define DNL_NUM_VARIANTS 6
 /* Variant in use and the element-pass time (ms) the autotuner measured for each. */
-int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[4]);
-/* Force an element-pass variant (0..3). */
+int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[DNL_NUM_VARIANTS]);
+/* Force an element-pass variant (0 .. DNL_NUM_VARIANTS-1). */
 int dnl_engine_set_variant(dnl_engine *h, int32_t variant);
 
 /* Element pass that allocates no device memory.  No counterpart in the
@@ -280,6 +286,7 @@ typedef struct dnl_mlp {
   float b4;
   float in_mean[DNL_MLP_IN];
   float in_scale[DNL_MLP_IN];
+  float out_exp; /* 0: r = output; 1: r = exp(output) (a network trained on ln r) */
 } dnl_mlp;
 
 /* One training pair as harvested from the radial return: the 5 raw inputs,
@@ -295,13 +302,22 @@ enum { DNL_MODE_PLAIN = 0, DNL_MODE_STATS = 1, DNL_MODE_HARVEST = 2, DNL_MODE_GU
 int dnl_engine_set_mode(dnl_engine *h, int32_t mode);
 int dnl_engine_set_guess_network(dnl_engine *h, const dnl_mlp *net);
 /* d_pairs: caller-owned device array of capacity*DNL_MLP_PAIR_WORDS floats; one
- * yielding point in `stride` (chosen by a hash of point and increment) is kept
- * until the buffer is full.  Resets the pair count. */
+ * yielding point of the guess scope (dnl_engine_set_guess_scope) in `stride`
+ * (chosen by a hash of point and increment) is kept until the buffer is full.
+ * Resets the pair count. */
 int dnl_engine_set_harvest(dnl_engine *h, float *d_pairs, int64_t capacity, int32_t stride);
 int dnl_engine_harvest_count(dnl_engine *h, int64_t *count);
-/* Since the last reset: [0] yield-function evaluations of the returns,
- * [1] yielding points, [2] points that started from the network's guess. */
-int dnl_engine_newton_stats(dnl_engine *h, int64_t out[3], int32_t reset);
+/* Which yielding points start from the network in DNL_MODE_GUESS:
+ * DNL_GUESS_ALL every one, DNL_GUESS_FIRST_YIELD only those without a
+ * previous gamma to start from (eps_p = 0, where the reference starts from
+ * gamma = 1e-8); the others keep the warm start. */
+enum { DNL_GUESS_ALL = 0, DNL_GUESS_FIRST_YIELD = 1 };
+int dnl_engine_set_guess_scope(dnl_engine *h, int32_t scope);
+/* Since the last reset (counting modes): [0] yield-function evaluations of
+ * the returns and [1] yielding points; [2] yielding points of the guess scope
+ * and [3] their evaluations (in DNL_MODE_GUESS, the points that started from
+ * the network). */
+int dnl_engine_newton_stats(dnl_engine *h, int64_t out[4], int32_t reset);
 
 /* Network kernels (BF16 tensor-core products, FP32 accumulation), on
  * caller-owned device arrays, on `stream` (NULL: default), synchronous.

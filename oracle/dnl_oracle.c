@@ -58,7 +58,7 @@ struct orc_model
   double N[8][8], dNdxi[8][8][3], w[8];          /* Gauss tables [ip][node] */
   double t, dt, t_end, up_to;
   long inc;
-  int ts_method, ts_freq;
+  int ts_method, ts_freq, stress_method;
   double safety, alphaM, beta, gamma, omegaS;
   int status, bad;
   double *pv;          /* power-iteration vector [nN*dim] (Model::_powerIterationEV) */
@@ -222,6 +222,7 @@ orc_model *orc_create(const dnl_model_desc *d)
   m->gamma = 1.5 - m->alphaM;
   m->omegaS = sqrt((12.0 * pow(1.0 + rb, 3) * (2.0 - rb)) / (10.0 + 15.0 * rb - rb * rb + pow(rb, 3) - pow(rb, 4)));
   m->ts_method = d->ts_method;
+  m->stress_method = d->stress_method;
   m->ts_freq = d->ts_freq > 0 ? d->ts_freq : 10;
   m->safety = d->ts_safety > 0 ? d->ts_safety : 0.9;
   m->t = d->t_start;
@@ -422,10 +423,16 @@ double orc_jc_hardening(const dnl_material *p, double epsp, double depsp, double
 
 /* -------------------------------------------------------- radial return */
 
+int orc_radial_return_method(const dnl_material *mat, const double dE[6], double dt, double *st, int direct);
+
 enum { RS_S = 0, RS_EP = 6, RS_EPSP = 12, RS_DEPSP, RS_GAMMA, RS_GCUM, RS_YIELD, RS_T, RS_P, RS_EINT, RS_EINEL, RS_N };
 
-/* Element::computeStress (Element.C:407-622) for one integration point. */
-int orc_radial_return(const dnl_material *mat, const double dE[6], double dt, double *st)
+/* Element::computeStress (Element.C:407-622) for one integration point, or
+ * with direct != 0 Element::computeStressDirect (Element.C:625-850): one
+ * step gamma = (|s*| - sqrt(2/3) sigma_y) / (2G (1 + h / (3G))) with the
+ * slope h at the previous plastic strain and rate and the initial temperature,
+ * then the yield stress at the new state. */
+int orc_radial_return_method(const dnl_material *mat, const double dE[6], double dt, double *st, int direct)
 {
   const double gammaInitial = 1e-8, tolNR = 1e-8;
   const int itMax = 250;
@@ -458,7 +465,26 @@ int orc_radial_return(const dnl_material *mat, const double dE[6], double dt, do
     yield = orc_jc_yield(mat, gammaInitial, gammaInitial / dt, T);
     st[RS_YIELD] = yield;
   }
-  if (Strial > yield)
+  if (Strial > yield && direct)
+  {
+    double hard = orc_jc_hardening(mat, plasticStrain > 0.0 ? plasticStrain : gammaInitial, plasticStrainRate, T, dt);
+    gamma = (Snorm - SQRT23 * yield) / (TwoG * (1.0 + hard / (1.5 * TwoG)));
+    plasticStrainRate = SQRT23 * gamma / dt;
+    plasticStrain = st[RS_EPSP] + SQRT23 * gamma;
+    T = T0 + 0.5 * gamma * heatFrac * (SQRT23 * yield + Snorm0);
+    yield = orc_jc_yield(mat, plasticStrain, plasticStrainRate, T);
+    for (int c = 0; c < 6; c++)
+      st[RS_EP + c] += gamma * dev[c] / Snorm;
+    double scale = 1.0 - TwoG * gamma / Snorm;
+    for (int c = 0; c < 6; c++)
+      dev[c] *= scale;
+    st[RS_EPSP] += SQRT23 * gamma;
+    st[RS_DEPSP] = SQRT23 * gamma / dt;
+    st[RS_GAMMA] = gamma;
+    st[RS_GCUM] += gamma;
+    st[RS_YIELD] = yield;
+  }
+  else if (Strial > yield)
   {
     double gammaMin = 0.0;
     double gammaMax = (Strial - yield) / TwoG32;
@@ -519,6 +545,11 @@ int orc_radial_return(const dnl_material *mat, const double dE[6], double dt, do
     st[RS_T] += heatFrac * plWorkInc;
   }
   return iterate;
+}
+
+int orc_radial_return(const dnl_material *mat, const double dE[6], double dt, double *st)
+{
+  return orc_radial_return_method(mat, dE, dt, st, 0);
 }
 
 /* ----------------------------------------------------------- element pass */
@@ -692,7 +723,7 @@ static int stress(orc_model *m, double dt)
       st[RS_P] = IPV(m, DNL_IP_PRESSURE, q);
       st[RS_EINT] = IPV(m, DNL_IP_EINT, q);
       st[RS_EINEL] = IPV(m, DNL_IP_EINEL, q);
-      if (orc_radial_return(mt, m->dE + q * 6, dt, st) < 0)
+      if (orc_radial_return_method(mt, m->dE + q * 6, dt, st, m->stress_method == DNL_STRESS_DIRECT) < 0)
       {
         m->status = DNL_ERR_NEWTON;
         m->bad = (int)q;

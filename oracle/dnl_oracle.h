@@ -43,6 +43,7 @@ void orc_polar_lnU(const double F[9], double lnU[6], double R[9]);
  * [stress 6, plastic strain 6, epsp, depsp, gamma, gammaCum, yield, T, pressure, eint, einel]
  * (21 doubles, updated in place); returns the Newton iteration count or -1. */
 int orc_radial_return(const dnl_material *mat, const double dE[6], double dt, double *state);
+int orc_radial_return_method(const dnl_material *mat, const double dE[6], double dt, double *state, int direct);
 double orc_jc_yield(const dnl_material *mat, double epsp, double depsp, double T);
 double orc_jc_hardening(const dnl_material *mat, double epsp, double depsp, double T, double dt);
 

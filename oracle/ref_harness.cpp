@@ -364,6 +364,9 @@ void *ref_create(const dnl_model_desc *d, const char *workdir)
   if (d->rho_b >= 0.0 && d->rho_b <= 1.0)
     s->setDissipation(d->rho_b);
   s->_reportFrequency = 1 << 30; // keep stdout quiet
+  // DynELA::setStressComputation (DynELA.C:1407-1431)
+  if (d->stress_method == DNL_STRESS_DIRECT)
+    dyn->setStressComputation((char *)"Direct");
   m->solver = s;
   g_model = m;
   return m;

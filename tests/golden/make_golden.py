@@ -82,10 +82,23 @@ def published_case():
     print("taylor_axi_sample", rows)
 
 
+CASES = {
+    "axi_run": lambda: run_case("axi_run", helpers.case_axi_small(), [1, 10, 200]),
+    "hex_run": lambda: run_case("hex_run", helpers.case_hex_small(), [1, 10, 60]),
+    "hex_speed_run": lambda: run_case("hex_speed_run", helpers.case_hex_speed(), [1, 10, 60]),
+    "axi_pass": lambda: pass_case("axi_pass", helpers.case_axi_small(), seed=5),
+    "hex_pass": lambda: pass_case("hex_pass", helpers.case_hex_small(), seed=6),
+    # Element::computeStressDirect (DynELA::setStressComputation("Direct"))
+    "hex_direct_run": lambda: run_case("hex_direct_run", helpers.case_hex_small().copy(stress_method=_abi.STRESS_DIRECT),
+                                       [1, 10, 60]),
+    "hex_direct_pass": lambda: pass_case("hex_direct_pass",
+                                         helpers.case_hex_small().copy(stress_method=_abi.STRESS_DIRECT), seed=7),
+    # the round bar pulled by a ramped end speed (necking workload, small mesh)
+    "bar_necking_run": lambda: run_case("bar_necking_run", helpers.case_bar_necking(), [1, 10, 60]),
+    "taylor_axi_sample": published_case,
+}
+
 if __name__ == "__main__":
-    run_case("axi_run", helpers.case_axi_small(), [1, 10, 200])
-    run_case("hex_run", helpers.case_hex_small(), [1, 10, 60])
-    run_case("hex_speed_run", helpers.case_hex_speed(), [1, 10, 60])
-    pass_case("axi_pass", helpers.case_axi_small(), seed=5)
-    pass_case("hex_pass", helpers.case_hex_small(), seed=6)
-    published_case()
+    # python tests/golden/make_golden.py [case ...]   (all cases by default)
+    for name in (sys.argv[1:] or list(CASES)):
+        CASES[name]()

@@ -38,7 +38,7 @@ def desc_to_npz(desc, prefix=""):
         out[prefix + "func_y"] = np.concatenate([f[1] for f in desc.functions])
         out[prefix + "func_n"] = np.array([len(f[0]) for f in desc.functions])
     out[prefix + "solver"] = np.array([desc.t_start, desc.t_end, desc.ts_method, desc.ts_freq, desc.ts_safety,
-                                       desc.rho_b, desc.precision])
+                                       desc.rho_b, desc.precision, desc.stress_method])
     return out
 
 
@@ -56,7 +56,8 @@ def desc_from_npz(z, prefix="", precision=None):
     return _abi.ModelDesc(int(z[prefix + "elem_type"]), z[prefix + "coords"], z[prefix + "conn"], mats,
                           functions=funcs, t_start=s[0], t_end=s[1], ts_method=int(s[2]), ts_freq=int(s[3]),
                           ts_safety=s[4], rho_b=s[5],
-                          precision=int(s[6]) if precision is None else precision, **opt)
+                          precision=int(s[6]) if precision is None else precision,
+                          stress_method=int(s[7]) if len(s) > 7 else _abi.STRESS_NEWTON, **opt)
 
 
 def random_point_state(desc, ips, seed, stress_scale=200.0):
@@ -146,3 +147,9 @@ def case_hex_speed(precision=_abi.PREC_FP64):
     fun[top, 1] = 0
     ramp = (np.array([0.0, 1e-6, 1.0]), np.array([0.0, 1.0, 1.0]))
     return d.copy(bc_code=bc, bc_value=val, bc_func=fun, functions=[ramp], v_init=np.zeros_like(d.coords))
+
+
+def case_bar_necking(precision=_abi.PREC_FP64):
+    """Round bar of the necking workload on a coarse mesh (4 x 4 O-grid, 20
+    layers), pulled by its ramped end speed."""
+    return meshes.bar_necking(n_core=4, n_ring=4, n_axial=20, precision=precision)

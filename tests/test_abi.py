@@ -53,6 +53,8 @@ def test_invalid_descriptions_are_rejected():
     assert lib.dnl_engine_create(ctypes.byref(c), ctypes.byref(h)) == -1 and not h
     rc, h, msg = _create(d.copy(ts_method=7))
     assert rc == -6
+    rc, h, msg = _create(d.copy(stress_method=5))
+    assert rc == -6 and "stress computation" in msg
 
 
 def test_no_device_means_no_engine():

@@ -284,3 +284,16 @@ def test_api_mixed_precision_taylor(tmp_path):
     _, out = run_api_taylor(tmp_path, precision="mixed")
     assert abs(out["radius"][1][-1, 1] - row[3]) < 1e-4 * row[3]
     assert abs(out["height"][1][-1, 1] - row[4]) < 1e-4 * row[4]
+
+
+def test_stress_computation_method():
+    """DynELA::setStressComputation (DynELA.C:1407-1431): "Direct" selects the
+    one-step return, "NewtonRaphson" the iterated one, anything else is refused."""
+    model, _ = taylor_axi_script(nr=2, nz=4)
+    assert model._description()[0].stress_method == _abi.STRESS_NEWTON
+    model.setStressComputation("Direct")
+    assert model._description()[0].stress_method == _abi.STRESS_DIRECT
+    model.setStressComputation("NewtonRaphson")
+    assert model._description()[0].stress_method == _abi.STRESS_NEWTON
+    with pytest.raises(ValueError):
+        model.setStressComputation("Implicit")

@@ -220,7 +220,7 @@ def test_element_variants_agree_and_autotune_keeps_state(precision):
     leaves the simulation state untouched."""
     d = meshes.taylor_3d(n_core=4, n_ring=3, n_axial=40, precision=precision)
     results = []
-    for v in range(4):
+    for v in range(_abi.NUM_VARIANTS):
         with engine(d) as e:
             e.init()
             e.set_variant(v)
@@ -235,7 +235,7 @@ def test_element_variants_agree_and_autotune_keeps_state(precision):
         e.run(max_incs=5)
         before = (e.nodes(_abi.NODE_COORDS), e.ips(), e.control())
         v, ms = e.autotune(steps=3)
-        assert 0 <= v < 4 and (ms > 0).all()
+        assert 0 <= v < _abi.NUM_VARIANTS and (ms > 0).all()
         assert np.array_equal(e.nodes(_abi.NODE_COORDS), before[0]) and np.array_equal(e.ips(), before[1])
         assert e.control()["increment"] == before[2]["increment"]
         e.run(max_incs=20)
