@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-accuracy", action="store_true", help="skip the whole-run mixed/FP64 comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
     p.add_argument("--no-guess", action="store_true", help="skip the learned Newton initial guess block")
+    p.add_argument("--no-necking", action="store_true", help="skip the necking workloads block")
     p.add_argument("--batch-fp64-sample", type=int, default=32,
                    help="instances of the batch timed one by one on the FP64 path")
     p.add_argument("--axial", type=int, default=160,
@@ -307,6 +308,32 @@ def batch_run(sample):
     return out
 
 
+def necking_run(incs=300):
+    """Throughput of the two tension workloads on the mixed path (FP64 beside
+    it): the round bar (1,198,080 elements) and the plate (491,520 elements),
+    each pulled by its ramped end speed, `incs` increments after 20, device
+    time of the run."""
+    from dnlPython import _abi, meshes
+    from dnlPython.engine import Engine
+    out = {}
+    for name, make in (("bar_necking_1198080", meshes.bar_necking), ("plate_necking_491520", meshes.plate_necking)):
+        res = {}
+        for prec, pname in ((_abi.PREC_MIXED, "mixed"), (_abi.PREC_FP64, "fp64")):
+            d = make(precision=prec)
+            with Engine(d) as e:
+                e.init()
+                v, _ = e.autotune(steps=4)
+                e.run(max_incs=20)
+                e.run(max_incs=incs)
+                ms = e.timings()["run_ms"]
+                res[pname] = {"elem_steps_per_s": d.n_elems * incs / (ms / 1e3), "ms_per_step": ms / incs,
+                              "variant": int(v)}
+        res["mixed_over_fp64"] = res["mixed"]["elem_steps_per_s"] / res["fp64"]["elem_steps_per_s"]
+        res["elements"] = d.n_elems
+        out[name] = res
+    return out
+
+
 def guess_run():
     """The learned Newton initial guess: pairs harvested from the first-yield
     returns of the 256-bar batch (its first 1,500 increments), the network
@@ -484,6 +511,8 @@ def run_engine_arm(args, rank, world, dist):
         out["accuracy_whole_run"] = accuracy_run()
     if world == 1 and not args.no_batch:
         out["batched"] = batch_run(args.batch_fp64_sample)
+    if world == 1 and not args.no_necking:
+        out["necking"] = necking_run()
     if world == 1 and AXIAL == 160 and not args.no_guess:
         out["learned_guess"] = guess_run()
     print(json.dumps(out))

@@ -458,6 +458,176 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
     H[8] = Vr / radius;
 }
 
+// One increment's work at one Gauss point (Explicit.C:204-226 + the density of
+// Explicit::computeDensity; Element.C:1103-1256 with the Jacobian of
+// ElementPlane.C:46-102 / Element3D.C:64-115 on the current coordinates):
+// strain increment and rotation by polar decomposition, element-mean pressure,
+// radial return, final rotation, density, and the element's nodal forces,
+// summed over its points through shared memory and stored in node order.
+// `row` is this lane's shared-memory row, `grp` the row of the element's first lane.
+// The element-pass modes run the same update split in two (element_front /
+// element_back below); this single body is what the plain variants use (the
+// split costs the plain variants about 10 % in spilled registers).
+template <typename R, int NPE, class Src, class Io>
+__device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int e, int g, int base, unsigned amask,
+                                               int node, const Src &old, R *row, R *grp)
+{
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  constexpr bool AXI = ElemShape<NPE>::AXI;
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  using R4 = typename V4<R>::type;
+  const double dt = C->dt_eff;
+  const MatDev &mp = io.mat(e);
+  const double4 X = io.x(node);
+  const double4 U = io.u(node);
+
+  R detJ, inv[3][3], radius, dE[6], Rot[9];
+  {
+    R H[9];
+    kinematics<R, NPE>(amask, g, base, X, U, detJ, inv, radius, H);
+    polar_lnU<R>(H, dE, Rot);
+  }
+  if (detJ < R(0))
+    raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
+  R WxdJ = detJ; // Gauss weight 1
+  if constexpr (AXI)
+    WxdJ *= R(6.28318530717958647692) * radius;
+
+  // element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
+  const R trSum = group_sum<NPE>(amask, dE[0] + dE[3] + dE[5]);
+
+  // total strain: Strain += dE, then the final rotation (Element.C:1116-1161)
+  {
+    R strain[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      strain[c] = old(DNL_IP_STRAIN + c) + dE[c];
+    rotate_sym<R>(Rot, strain);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      io.put(DNL_IP_STRAIN + c, strain[c]);
+  }
+
+  // the rotation and J^-1 wait in shared memory while the return holds its registers
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+  {
+    row[k] = Rot[k];
+    row[9 + k] = inv[k / 3][k % 3];
+  }
+
+  // J2 radial return with Johnson-Cook hardening (Element.C:407-622)
+  ReturnState<R> st;
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    st.s[c] = old(DNL_IP_STRESS + c);
+  st.epsp = old(DNL_IP_EPSP);
+  st.depsp = old(DNL_IP_DEPSP);
+  st.gamma = old(DNL_IP_GAMMA);
+  st.gcum = old(DNL_IP_GAMMA_CUM);
+  st.yield = old(DNL_IP_YIELD);
+  st.T = old(DNL_IP_T);
+  st.eint = old(DNL_IP_EINT);
+  st.einel = old(DNL_IP_EINEL);
+  JC<R> jc;
+  jc.load(mp);
+  st.pressure = (st.s[0] + st.s[3] + st.s[5]) / R(3) + jc.K() * (trSum / R(NPE));
+  {
+    bool ok;
+    radial_return<R>(jc, jc.twoG(), jc.heatFrac(), jc.invRho0(), dE, R(dt), st, ok, R(-1), C->direct != 0);
+    if (!ok)
+    {
+      if constexpr (sizeof(R) == 4)
+      {
+        atomicAdd(&C->resolves, 1);
+        const Resolved r = resolve_fp64(io.ip32(), q, io.matp(e), dE[0], dE[1], dE[2], dE[3], dE[4], dE[5], dt,
+                                        st.pressure);
+        if (!r.ok)
+          raise_status(C, DNL_ERR_NEWTON, q);
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+          st.s[c] = r.s[c];
+        st.kplast = r.kplast;
+        st.epsp = r.epsp;
+        st.depsp = r.depsp;
+        st.gamma = r.gamma;
+        st.gcum = r.gcum;
+        st.yield = r.yield;
+        st.T = r.T;
+        st.eint = r.eint;
+        st.einel = r.einel;
+      }
+      else
+        raise_status(C, DNL_ERR_NEWTON, q);
+    }
+  }
+
+  // final rotation of the plastic strain (PlasticStrain += gamma s*/|s*|,
+  // Element.C:587) and of the stress, state write-back
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+    Rot[k] = row[k];
+  {
+    R ep[6];
+    const R pn = (st.s[0] + st.s[3] + st.s[5]) / R(3);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      ep[c] = old(DNL_IP_PLASTIC_STRAIN + c) + st.kplast * (st.s[c] - ((c == 0 || c == 3 || c == 5) ? pn : R(0)));
+    rotate_sym<R>(Rot, ep);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      io.put(DNL_IP_PLASTIC_STRAIN + c, ep[c]);
+  }
+  rotate_sym<R>(Rot, st.s);
+  R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
+  if constexpr (AXI)
+    rho /= radius;
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    io.put(DNL_IP_STRESS + c, st.s[c]);
+  io.put(DNL_IP_EPSP, st.epsp);
+  io.put(DNL_IP_DEPSP, st.depsp);
+  io.put(DNL_IP_GAMMA, st.gamma);
+  io.put(DNL_IP_GAMMA_CUM, st.gcum);
+  io.put(DNL_IP_YIELD, st.yield);
+  io.put(DNL_IP_T, st.T);
+  io.put(DNL_IP_PRESSURE, st.pressure);
+  io.put(DNL_IP_EINT, st.eint);
+  io.put(DNL_IP_EINEL, st.einel);
+  io.put(DNL_IP_DENSITY, rho);
+
+  // internal forces f_n = -sum_g dN_n/dx . sigma w detJ (Element.C:362-404):
+  // with P = -w detJ J^-1 sigma, f_n,i = sum_k dN_n/dxi_k P_ki
+  R P[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+    {
+      R s = R(0);
+#pragma unroll
+      for (int j = 0; j < DIM; j++)
+        s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
+      P[k][i] = -WxdJ * s;
+    }
+  const R a = R(0.57735026918962576451);
+  const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
+  const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
+  ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
+  __syncwarp(amask);
+  R4 fs;
+  fs.x = fs.y = fs.z = fs.w = R(0);
+#pragma unroll
+  for (int l = 0; l < NPE; l++)
+  {
+    fs.x += grp[l * ROW + g * DIM];
+    fs.y += grp[l * ROW + g * DIM + 1];
+    if constexpr (DIM == 3)
+      fs.z += grp[l * ROW + g * DIM + 2];
+  }
+  io.slot(fs);
+}
+
 // What the first half of an element update hands to the second: the strain
 // increment, the Jacobian terms and the point state loaded for the return (the
 // rotation and J^-1 wait in the lane's shared-memory row).
@@ -468,15 +638,10 @@ template <typename R> struct Front
   ReturnState<R> st;
 };
 
-// One increment's work at one Gauss point (Explicit.C:204-226 + the density of
-// Explicit::computeDensity; Element.C:1103-1256 with the Jacobian of
-// ElementPlane.C:46-102 / Element3D.C:64-115 on the current coordinates):
-// strain increment and rotation by polar decomposition, element-mean pressure,
-// radial return, final rotation, density, and the element's nodal forces,
-// summed over its points through shared memory and stored in node order.
-// `row` is this lane's shared-memory row, `grp` the row of the element's first lane.
-// element_front runs up to the start of the return, element_back from the
-// return on; a kernel may run block-wide work (the learned guess) in between.
+// The element update of element_update above in two halves, for the
+// element-pass modes: element_front runs up to the start of the return,
+// element_back from the return on; the mode kernel runs block-wide work (the
+// learned guess) in between.  Same arithmetic as element_update.
 template <typename R, int NPE, class Src, class Io>
 __device__ __forceinline__ void element_front(const Io &io, Ctl *C, int e, int g, int base, unsigned amask, int node,
                                               const Src &old, R *row, Front<R> &f)
@@ -652,15 +817,6 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
   }
   io.slot(fs);
   return iters;
-}
-
-template <typename R, int NPE, class Src, class Io>
-__device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int e, int g, int base, unsigned amask,
-                                               int node, const Src &old, R *row, R *grp)
-{
-  Front<R> f;
-  element_front<R, NPE>(io, C, e, g, base, amask, node, old, row, f);
-  element_back<R, NPE>(io, C, q, e, g, amask, old, row, grp, f);
 }
 
 // Start of the solve: reference Jacobian detJ0 (ElementPlane.C:96-100,

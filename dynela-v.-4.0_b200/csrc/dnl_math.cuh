@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dnlgpu.h"
+
 namespace dnl
 {
 
@@ -267,37 +269,87 @@ template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R 
     }
 }
 
-// Johnson-Cook parameters of one material, with the constants the return uses.
+// Johnson-Cook parameters of one material in the precision a return runs in.
+template <typename R> struct JCParams
+{
+  R A, B, C, n, m, depsp0, Tm, Tref, invTmT, thermal; // invTmT = 1/(Tm-Tref), thermal = tq/(rho0 Cp)
+  R twoG, invRho0, K;                                 // 2G, 1/rho0 and the bulk modulus of the return
+};
+
+// Material constants (Material.h, JohnsonCookLaw.C:132-143) with the derived
+// ones the return uses, and the Johnson-Cook block in FP64 and in FP32.
 struct MatDev
 {
   double young, poisson, rho0, cp, tq, T0;
   double A, B, C, n, m, depsp0, Tm, Tref;
   double twoG, K, heatFrac, wave2; // E/(1+nu), E/(3(1-2nu)), tq/(rho0 Cp), E(1-nu)/((1+nu)(1-2nu))
+  JCParams<double> jc64;
+  JCParams<float> jc32;
 };
 
+// Host: the device copy of a material description.
+inline MatDev make_mat(const dnl_material &m)
+{
+  MatDev d;
+  d.young = m.young;
+  d.poisson = m.poisson;
+  d.rho0 = m.density;
+  d.cp = m.heat_capacity;
+  d.tq = m.taylor_quinney;
+  d.T0 = m.T0;
+  d.A = m.A;
+  d.B = m.B;
+  d.C = m.C;
+  d.n = m.n;
+  d.m = m.m;
+  d.depsp0 = m.depsp0;
+  d.Tm = m.Tm;
+  d.Tref = m.Tref;
+  d.twoG = m.young / (1.0 + m.poisson);                          // Material.h:110-114
+  d.K = m.young / (3.0 * (1.0 - 2.0 * m.poisson));               // Material.h:152-156
+  d.heatFrac = m.taylor_quinney / (m.density * m.heat_capacity); // Material.h:165-169
+  d.wave2 = m.young * (1.0 - m.poisson) / ((1.0 + m.poisson) * (1.0 - 2.0 * m.poisson)); // Element.C:358
+  d.jc64 = {d.A, d.B, d.C, d.n, d.m, d.depsp0, d.Tm, d.Tref, 1.0 / (d.Tm - d.Tref), d.heatFrac, d.twoG,
+            1.0 / d.rho0, d.K};
+  d.jc32 = {(float)d.A,    (float)d.B,      (float)d.C,    (float)d.n,           (float)d.m,
+            (float)d.depsp0, (float)d.Tm,   (float)d.Tref, (float)d.jc64.invTmT, (float)d.heatFrac,
+            (float)d.twoG, (float)(1.0 / d.rho0), (float)d.K};
+  return d;
+}
+
+// The Johnson-Cook law as the return calls it.  The parameters are read from
+// the material (global memory, read-only loads) at each use instead of being
+// held in registers through the return: the element pass is limited by
+// registers, and the material is one cached line that every thread shares.
 template <typename R> struct JC
 {
-  R A, B, C, n, m, depsp0, Tm, Tref, invTmT, thermal; // thermal = tq/(rho0 Cp)
+  const JCParams<R> *q;
   __device__ __forceinline__ void load(const MatDev &p)
   {
-    A = R(p.A); B = R(p.B); C = R(p.C); n = R(p.n); m = R(p.m); depsp0 = R(p.depsp0);
-    Tm = R(p.Tm); Tref = R(p.Tref); invTmT = R(1.0 / (p.Tm - p.Tref)); thermal = R(p.heatFrac);
+    if constexpr (sizeof(R) == 4)
+      q = &p.jc32;
+    else
+      q = &p.jc64;
   }
+  __device__ __forceinline__ R twoG() const { return __ldg(&q->twoG); }
+  __device__ __forceinline__ R heatFrac() const { return __ldg(&q->thermal); }
+  __device__ __forceinline__ R invRho0() const { return __ldg(&q->invRho0); }
+  __device__ __forceinline__ R K() const { return __ldg(&q->K); }
   // JohnsonCookLaw::getYieldStress (JohnsonCookLaw.C:146-170) and the analytic
   // total derivative getDerivateYieldStress (JohnsonCookLaw.C:298-339), in one pass.
   __device__ __forceinline__ void eval(R epsp, R depsp, R T, R dt, R &yield, R &hard, bool wantHard) const
   {
-    R pn = Num<R>::pow_(epsp, n); // epsp^n
-    R hard0 = A + B * pn;
-    bool rate = depsp > depsp0;
-    R visc0 = rate ? R(1) + C * Num<R>::log_(depsp / depsp0) : R(1);
+    R pn = Num<R>::pow_(epsp, __ldg(&q->n)); // epsp^n
+    R hard0 = __ldg(&q->A) + __ldg(&q->B) * pn;
+    bool rate = depsp > __ldg(&q->depsp0);
+    R visc0 = rate ? R(1) + __ldg(&q->C) * Num<R>::log_(depsp / __ldg(&q->depsp0)) : R(1);
     R temp0 = R(1), temp1 = R(0);
-    bool hot = T > Tref, melt = !(T < Tm);
+    bool hot = T > __ldg(&q->Tref), melt = !(T < __ldg(&q->Tm));
     if (hot)
     {
       if (!melt)
       {
-        temp1 = Num<R>::pow_((T - Tref) * invTmT, m);
+        temp1 = Num<R>::pow_((T - __ldg(&q->Tref)) * __ldg(&q->invTmT), __ldg(&q->m));
         temp0 = R(1) - temp1;
       }
       else
@@ -306,11 +358,11 @@ template <typename R> struct JC
     yield = hard0 * visc0 * temp0;
     if (wantHard)
     {
-      R h = n * B * (epsp > R(0) ? pn / epsp : R(0)) * visc0 * temp0; // n B epsp^(n-1) ...
+      R h = __ldg(&q->n) * __ldg(&q->B) * (epsp > R(0) ? pn / epsp : R(0)) * visc0 * temp0; // n B epsp^(n-1) ...
       if (rate)
-        h += hard0 * C * temp0 / (depsp * dt);
+        h += hard0 * __ldg(&q->C) * temp0 / (depsp * dt);
       if (hot && !melt)
-        h -= m * thermal * hard0 * hard0 * visc0 * visc0 * temp0 * temp1 / (T - Tref);
+        h -= __ldg(&q->m) * __ldg(&q->thermal) * hard0 * hard0 * visc0 * visc0 * temp0 * temp1 / (T - __ldg(&q->Tref));
       hard = h;
     }
   }

@@ -157,29 +157,6 @@ int check_desc(const dnl_model_desc *d, int idx)
   return DNL_OK;
 }
 
-MatDev make_mat(const dnl_material &m)
-{
-  MatDev d;
-  d.young = m.young;
-  d.poisson = m.poisson;
-  d.rho0 = m.density;
-  d.cp = m.heat_capacity;
-  d.tq = m.taylor_quinney;
-  d.T0 = m.T0;
-  d.A = m.A;
-  d.B = m.B;
-  d.C = m.C;
-  d.n = m.n;
-  d.m = m.m;
-  d.depsp0 = m.depsp0;
-  d.Tm = m.Tm;
-  d.Tref = m.Tref;
-  d.twoG = m.young / (1.0 + m.poisson);                 // Material.h:110-114
-  d.K = m.young / (3.0 * (1.0 - 2.0 * m.poisson));      // Material.h:152-156
-  d.heatFrac = m.taylor_quinney / (m.density * m.heat_capacity); // Material.h:165-169
-  d.wave2 = m.young * (1.0 - m.poisson) / ((1.0 + m.poisson) * (1.0 - 2.0 * m.poisson)); // Element.C:358
-  return d;
-}
 
 // ----------------------------------------------------------------- launches
 

@@ -34,7 +34,8 @@ constexpr size_t OFF_SLOT = 256;
 constexpr size_t OFF_COUNT = OFF_SLOT + sizeof(double4) * MAX_IPS;
 constexpr size_t OFF_CURSOR = OFF_COUNT + sizeof(int) * (MAX_NODES + 1);
 constexpr size_t OFF_LIST = OFF_CURSOR + sizeof(int) * MAX_NODES;
-constexpr size_t SCRATCH_BYTES = OFF_LIST + sizeof(int) * MAX_IPS;
+constexpr size_t OFF_MAT = (OFF_LIST + sizeof(int) * MAX_IPS + 255) / 256 * 256;
+constexpr size_t SCRATCH_BYTES = OFF_MAT + sizeof(MatDev);
 
 // The scratch of every call (about 5.3 MB).  Host code only takes its device
 // address (cudaGetSymbolAddress); the kernels receive that address.
@@ -45,13 +46,14 @@ struct Scratch
   Ctl *ctl;
   double4 *slot;
   int *count, *cursor, *list;
+  MatDev *mat; // the call's material, read by the return from global memory
 };
 
 __host__ __device__ Scratch carve(unsigned char *base)
 {
   return Scratch{reinterpret_cast<Ctl *>(base + OFF_CTL), reinterpret_cast<double4 *>(base + OFF_SLOT),
                  reinterpret_cast<int *>(base + OFF_COUNT), reinterpret_cast<int *>(base + OFF_CURSOR),
-                 reinterpret_cast<int *>(base + OFF_LIST)};
+                 reinterpret_cast<int *>(base + OFF_LIST), reinterpret_cast<MatDev *>(base + OFF_MAT)};
 }
 
 // Caller's arrays: point state component-major [29][n_ips] FP64, nodes [n][3].
@@ -60,7 +62,7 @@ struct StaticIo
   const double *coords, *du;
   double *ip;
   double4 *slots;
-  MatDev mat_;
+  const MatDev *mat_;
   int nIP, q;
   __device__ __forceinline__ double4 x(int n) const
   {
@@ -70,8 +72,8 @@ struct StaticIo
   {
     return make_double4(du[3 * n], du[3 * n + 1], du[3 * n + 2], 0.0);
   }
-  __device__ __forceinline__ const MatDev &mat(int) const { return mat_; }
-  __device__ __forceinline__ const MatDev *matp(int) const { return &mat_; }
+  __device__ __forceinline__ const MatDev &mat(int) const { return *mat_; }
+  __device__ __forceinline__ const MatDev *matp(int) const { return mat_; }
   __device__ __forceinline__ void put(int c, double v) const { ip[(size_t)c * nIP + q] = v; }
   __device__ __forceinline__ void slot(const double4 &v) const { slots[q] = v; }
   __device__ __forceinline__ const float *ip32() const { return nullptr; }
@@ -107,6 +109,7 @@ __global__ void k_sp_clear(Args a)
     c.active = 1;
     c.dt_eff = a.dt;
     *s.ctl = c;
+    *s.mat = a.mat;
   }
   if (i <= a.nN)
     s.count[i] = 0;
@@ -199,7 +202,7 @@ template <int NPE> __global__ void __launch_bounds__(TILE) k_sp_element(Args a)
   if (!act)
     return;
   const int nIP = a.nE * NPE;
-  StaticIo io{a.coords, a.du, a.ip, s.slot, a.mat, nIP, q};
+  StaticIo io{a.coords, a.du, a.ip, s.slot, s.mat, nIP, q};
   PlainState old{a.ip, nIP, q};
   element_update<double, NPE>(io, s.ctl, q, e, g, base, amask, a.conn[q], old, sh + threadIdx.x * ROW,
                               sh + (threadIdx.x - g) * ROW);
@@ -297,25 +300,7 @@ extern "C" int dnl_element_pass_static(int32_t elem_type, int32_t n_nodes, int32
   a.npe = npe;
   a.dt = time_step;
   a.scratch = scratch;
-  MatDev &d = a.mat;
-  d.young = m.young;
-  d.poisson = m.poisson;
-  d.rho0 = m.density;
-  d.cp = m.heat_capacity;
-  d.tq = m.taylor_quinney;
-  d.T0 = m.T0;
-  d.A = m.A;
-  d.B = m.B;
-  d.C = m.C;
-  d.n = m.n;
-  d.m = m.m;
-  d.depsp0 = m.depsp0;
-  d.Tm = m.Tm;
-  d.Tref = m.Tref;
-  d.twoG = m.young / (1.0 + m.poisson);
-  d.K = m.young / (3.0 * (1.0 - 2.0 * m.poisson));
-  d.heatFrac = m.taylor_quinney / (m.density * m.heat_capacity);
-  d.wave2 = m.young * (1.0 - m.poisson) / ((1.0 + m.poisson) * (1.0 - 2.0 * m.poisson));
+  a.mat = make_mat(m);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int nIP = n_elems * npe;
   k_sp_clear<<<(n_nodes + 1 + 255) / 256, 256, 0, st>>>(a);
