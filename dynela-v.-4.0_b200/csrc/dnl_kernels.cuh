@@ -1027,6 +1027,186 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
   }
 }
 
+// ------------------------------------- element pass with staged node data
+
+// 16-byte asynchronous global -> shared copies (no mbarrier), grouped per tile
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Element update I/O for a tile whose node coordinates and increments, force
+// slot positions and element materials were staged in shared memory.
+template <typename R> struct StagedIo
+{
+  using R4 = typename V4<R>::type;
+  const DevModel &M;
+  int q;
+  const double4 *nx, *nu; // this lane's node
+  int spos;
+  const MatDev *mp;
+  __device__ __forceinline__ double4 x(int) const { return *nx; }
+  __device__ __forceinline__ double4 u(int) const { return *nu; }
+  __device__ __forceinline__ const MatDev &mat(int) const { return *mp; }
+  __device__ __forceinline__ const MatDev *matp(int) const { return mp; }
+  __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
+  __device__ __forceinline__ void slot(const R4 &v) const { reinterpret_cast<R4 *>(M.slot)[spos] = v; }
+  __device__ __forceinline__ const float *ip32() const { return reinterpret_cast<const float *>(M.ip); }
+};
+
+// Element pass as a persistent kernel with three pipelines a tile apart: the
+// point state, force-slot positions and element materials of the next tile
+// come by bulk copy (mbarrier), the connectivity two tiles ahead, and the
+// coordinates and increments of the next tile's nodes are gathered by
+// asynchronous copies while the current tile computes, so the update reads
+// every input from shared memory.
+template <typename R, int NPE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nTiles, int *err)
+{
+  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr int EPT = TILE / NPE; // elements per tile
+  constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
+  constexpr uint32_t NODE_BYTES = 2 * TILE * sizeof(double4); // coordinates then increments
+  constexpr uint32_t IDX_BYTES = TILE * sizeof(int);
+  constexpr uint32_t EMAT_BYTES = EPT * sizeof(int);
+  static_assert(EMAT_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
+  // shared memory: state[2] | nodes[2] | (slot positions, materials)[2] | connectivity[3] | rows
+  constexpr uint32_t OFF_NODES = 2 * STATE_BYTES;
+  constexpr uint32_t OFF_IDX = OFF_NODES + 2 * NODE_BYTES;
+  constexpr uint32_t IDX_STRIDE = IDX_BYTES + EMAT_BYTES;
+  constexpr uint32_t OFF_CONN = OFF_IDX + 2 * IDX_STRIDE;
+  constexpr uint32_t OFF_ROWS = OFF_CONN + 3 * IDX_BYTES;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  auto state = [&](int b) { return reinterpret_cast<R *>(smem_raw + b * STATE_BYTES); };
+  auto nodes = [&](int b) { return reinterpret_cast<double4 *>(smem_raw + OFF_NODES + b * NODE_BYTES); };
+  auto spos = [&](int b) { return reinterpret_cast<int *>(smem_raw + OFF_IDX + b * IDX_STRIDE); };
+  auto emat = [&](int b) { return reinterpret_cast<int *>(smem_raw + OFF_IDX + b * IDX_STRIDE + IDX_BYTES); };
+  auto conn = [&](int c) { return reinterpret_cast<int *>(smem_raw + OFF_CONN + c * IDX_BYTES); };
+  R *rows = reinterpret_cast<R *>(smem_raw + OFF_ROWS);
+  __shared__ __align__(8) uint64_t sbar[2], cbar[3];
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  const int g = lane & (NPE - 1);
+  const int base = lane & ~(NPE - 1);
+  if (t == 0)
+  {
+    mbar_init(&sbar[0], 1);
+    mbar_init(&sbar[1], 1);
+    mbar_init(&cbar[0], 1);
+    mbar_init(&cbar[1], 1);
+    mbar_init(&cbar[2], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto live = [&](int tl) {
+    if (M.nInst == 1)
+      return M.ctl[0].active != 0;
+    const int e0 = tl * EPT, e1 = min(M.nE - 1, e0 + EPT - 1);
+    const int i1 = find_segment(M.inst_elem_begin, M.nInst, e1);
+    for (int i = find_segment(M.inst_elem_begin, M.nInst, e0); i <= i1; i++)
+      if (M.ctl[i].active)
+        return true;
+    return false;
+  };
+  auto next_live = [&](int tl) {
+    while (tl < nTiles && !live(tl))
+      tl += gridDim.x;
+    return tl;
+  };
+  auto issue_state = [&](int tl, int b) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&sbar[b], STATE_BYTES + IDX_BYTES + EMAT_BYTES);
+    bulk_g2s(state(b), reinterpret_cast<const R *>(M.ip) + (size_t)tl * DNL_IP_NCOMP * TILE, STATE_BYTES, &sbar[b]);
+    bulk_g2s(spos(b), M.slot_pos + (size_t)tl * TILE, IDX_BYTES, &sbar[b]);
+    bulk_g2s(emat(b), M.emat + (size_t)tl * EPT, EMAT_BYTES, &sbar[b]);
+  };
+  auto issue_conn = [&](int tl, int c) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&cbar[c], IDX_BYTES);
+    bulk_g2s(conn(c), M.conn + (size_t)tl * TILE, IDX_BYTES, &cbar[c]);
+  };
+  // this lane's node of a tile: coordinates and increment of field0 of its instance
+  auto gather = [&](int tl, int c, int b) {
+    const int q = tl * TILE + t;
+    const int e = min(q / NPE, M.nE - 1);
+    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, e) : 0;
+    const int node = conn(c)[t];
+    const char *src_x = reinterpret_cast<const char *>(M.x + node);
+    const char *src_u = reinterpret_cast<const char *>(M.u[M.ctl[inst].f0] + node);
+    char *dst = reinterpret_cast<char *>(nodes(b) + t);
+    cp_async16(dst, src_x);
+    cp_async16(dst + 16, src_x + 16);
+    cp_async16(dst + TILE * sizeof(double4), src_u);
+    cp_async16(dst + TILE * sizeof(double4) + 16, src_u + 16);
+    cp_async_commit();
+  };
+  uint32_t sph = 0, cph = 0; // parity bit of each barrier
+  bool failed = false;
+  auto wait_bar = [&](uint64_t *bar, uint32_t &bits, int k) {
+    if (!failed && !mbar_wait(bar, (bits >> k) & 1u))
+    {
+      atomicExch(err, 1);
+      failed = true;
+    }
+    bits ^= 1u << k;
+  };
+
+  int tile = next_live(blockIdx.x);
+  int next = tile < nTiles ? next_live(tile + gridDim.x) : nTiles;
+  if (t == 0 && tile < nTiles)
+  {
+    issue_conn(tile, 0);
+    issue_state(tile, 0);
+    if (next < nTiles)
+      issue_conn(next, 1);
+  }
+  if (tile < nTiles)
+  {
+    wait_bar(&cbar[0], cph, 0);
+    gather(tile, 0, 0);
+  }
+  for (int b = 0, c = 0; tile < nTiles; b ^= 1, c = (c == 2 ? 0 : c + 1))
+  {
+    const int after = next < nTiles ? next_live(next + gridDim.x) : nTiles;
+    const int c1 = (c == 2 ? 0 : c + 1), c2 = (c1 == 2 ? 0 : c1 + 1);
+    if (t == 0)
+    {
+      if (next < nTiles)
+        issue_state(next, b ^ 1);
+      if (after < nTiles)
+        issue_conn(after, c2);
+    }
+    if (next < nTiles)
+    {
+      wait_bar(&cbar[c1], cph, c1);
+      gather(next, c1, b ^ 1);
+      cp_async_wait<1>(); // this tile's nodes (all but the group just issued)
+    }
+    else
+      cp_async_wait<0>();
+    wait_bar(&sbar[b], sph, b);
+    const int q = tile * TILE + t;
+    const int e = q / NPE;
+    const bool valid = e < M.nE;
+    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
+    Ctl *C = M.ctl + inst;
+    const bool act = valid && C->active && !failed;
+    const unsigned amask = __ballot_sync(0xffffffffu, act);
+    if (act)
+    {
+      SharedTile<R> old{state(b), t};
+      StagedIo<R> io{M, q, nodes(b) + t, nodes(b) + TILE + t, spos(b)[t], M.mat + emat(b)[t / NPE]};
+      element_update<R, NPE>(io, C, q, e, g, base, amask, 0, old, rows + t * ROW, rows + (t - g) * ROW);
+    }
+    __syncthreads(); // the buffers of this tile are refilled from the next iteration on
+    tile = next;
+    next = after;
+  }
+  cp_async_wait<0>();
+}
+
 // ------------------------------------------------ element pass with modes
 
 enum

@@ -171,10 +171,11 @@ struct Variant
 };
 // each precision: two plain budgets, then persistent staged tiles from the most
 // blocks per SM (fewest registers, most spilled) to the fewest (no spills)
-const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4},
-                                {"tma/5", 1, 5},   {"tma/3", 1, 3},   {"tma/2", 1, 2}};
-const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2},
-                                {"tma/3", 1, 3},   {"plain/2", 0, 2}, {"tma/1", 1, 1}};
+// then the fully staged kernel (node gathers one tile ahead as well)
+const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4}, {"tma/5", 1, 5},
+                                {"tma/3", 1, 3},   {"tma/2", 1, 2},   {"stage/3", 2, 3}, {"stage/2", 2, 2}};
+const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2},  {"tma/3", 1, 3},
+                                {"plain/2", 0, 2}, {"tma/1", 1, 1},   {"stage/2", 2, 2}, {"stage/1", 2, 1}};
 constexpr int kNumVariants = DNL_NUM_VARIANTS;
 
 const Variant &variant_of(const dnl_engine *h, int v)
@@ -202,6 +203,25 @@ template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
   }
   const int grid = std::min(h->nTiles, perSM * h->numSMs);
   k_element_tma<R, NPE, MINB><<<grid, TILE, smem, h->stream>>>(h->M, h->nTiles, h->derr);
+  return DNL_OK;
+}
+
+template <typename R, int NPE, int MINB> int launch_stage(dnl_engine *h)
+{
+  constexpr int EPT = TILE / NPE;
+  const size_t smem = 2 * DNL_IP_NCOMP * TILE * sizeof(R) + 2 * 2 * TILE * sizeof(double4) +
+                      2 * (TILE + EPT) * sizeof(int) + 3 * TILE * sizeof(int) +
+                      TILE * ElemShape<NPE>::ROW * sizeof(R);
+  static int perSM = -1; // per instantiation
+  if (perSM < 0)
+  {
+    CK(cudaFuncSetAttribute(k_element_stage<R, NPE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_stage<R, NPE, MINB>, TILE, smem));
+    if (perSM < 1)
+      perSM = 1;
+  }
+  const int grid = std::min(h->nTiles, perSM * h->numSMs);
+  k_element_stage<R, NPE, MINB><<<grid, TILE, smem, h->stream>>>(h->M, h->nTiles, h->derr);
   return DNL_OK;
 }
 
@@ -246,7 +266,9 @@ template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
     case 2: return launch_tma<R, NPE, 4>(h);
     case 3: return launch_tma<R, NPE, 5>(h);
     case 4: return launch_tma<R, NPE, 3>(h);
-    default: return launch_tma<R, NPE, 2>(h);
+    case 5: return launch_tma<R, NPE, 2>(h);
+    case 6: return launch_stage<R, NPE, 3>(h);
+    default: return launch_stage<R, NPE, 2>(h);
     }
   }
   switch (v)
@@ -256,7 +278,9 @@ template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
   case 2: return launch_tma<R, NPE, 2>(h);
   case 3: return launch_tma<R, NPE, 3>(h);
   case 4: return launch_plain<R, NPE, 2>(h);
-  default: return launch_tma<R, NPE, 1>(h);
+  case 5: return launch_tma<R, NPE, 1>(h);
+  case 6: return launch_stage<R, NPE, 2>(h);
+  default: return launch_stage<R, NPE, 1>(h);
   }
 }
 
@@ -614,6 +638,9 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     for (size_t k = 0; k < (size_t)h->nIP; k++)
       pos[k] = fill[conn[k]]++;
   }
+  // whole tiles for the bulk copies of the staged element pass (padding unused)
+  pos.resize((size_t)h->nIPpad, 0);
+  emat.resize((size_t)h->nIPpad / h->npe, 0);
 
   int rc = DNL_OK;
   DevModel &M = h->M;

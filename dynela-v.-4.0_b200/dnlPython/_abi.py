@@ -20,7 +20,7 @@ NODES_PER_ELEMENT = {ELQUA4NAX: 4, ELHEX8N3D: 8}
 DIMS = {ELQUA4NAX: 2, ELHEX8N3D: 3}
 
 STRESS_NEWTON, STRESS_DIRECT = 0, 1
-NUM_VARIANTS = 6  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)
+NUM_VARIANTS = 8  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)
 TS_COURANT = 0
 TS_POWER_ITERATION = 1
 PREC_FP64 = 0

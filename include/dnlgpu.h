@@ -226,7 +226,7 @@ int64_t dnl_engine_launch_count(const dnl_engine *h);
  * and restores the state.  No counterpart in the reference (its element loop
  * has one implementation). */
 int dnl_engine_autotune(dnl_engine *h, int32_t steps);
-#define DNL_NUM_VARIANTS 6
+#define DNL_NUM_VARIANTS 8
 /* Variant in use and the element-pass time (ms) the autotuner measured for each. */
 int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[DNL_NUM_VARIANTS]);
 /* Force an element-pass variant (0 .. DNL_NUM_VARIANTS-1). */

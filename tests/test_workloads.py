@@ -44,7 +44,7 @@ def test_taylor_batch_generator():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", [0, 2], ids=["plain", "bulk-copy"])
+@pytest.mark.parametrize("variant", [0, 2, 6], ids=["plain", "bulk-copy", "staged"])
 def test_batch_failed_instance_stops_alone(variant):
     """An instance whose element inverts stops with its status; the other
     instances of the batch run to their end exactly as they do alone."""
@@ -74,7 +74,7 @@ def test_batch_failed_instance_stops_alone(variant):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", [0, 2], ids=["plain", "bulk-copy"])
+@pytest.mark.parametrize("variant", [0, 2, 6], ids=["plain", "bulk-copy", "staged"])
 def test_batch_of_taylor_bars_matches_single_runs(variant):
     """Bars of uneven size, speed and material in one batch: every instance
     ends bit-identical to its own run (the bars finish at different
