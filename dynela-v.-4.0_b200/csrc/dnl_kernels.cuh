@@ -90,6 +90,7 @@ struct DevModel
   long long harvest_cap;
   int harvest_stride;
   int guess_scope;         // DNL_GUESS_ALL or DNL_GUESS_FIRST_YIELD
+  unsigned *done_count;    // blocks of the fused Courant + end-of-increment kernel that have finished
 };
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
@@ -1340,7 +1341,7 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
 // Model::computeInternalForces, Model.C:881-898), then the Chung-Hulbert
 // corrector and the boundary conditions, then disp += du, coords += du.
 template <typename R, int DIM>
-__global__ void __launch_bounds__(256) k_nodal(DevModel M)
+__global__ void __launch_bounds__(128) k_nodal(DevModel M)
 {
   using R4 = typename V4<R>::type;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1499,6 +1500,100 @@ __global__ void k_gather(DevModel M, int what)
     M.fout[i] = f;
 }
 
+// ---------------------------------------------------------------- control
+
+enum
+{
+  CTL_FINISH = 0,   // end of the increment that ran, then begin the next one
+  CTL_LIMITS = 1,   // new pause time / increment budget, then begin
+  CTL_INIT_DT = 2,  // after the forced Courant pass of the start: dt, then arm the first element pass
+  CTL_POST_INIT = 3 // after the first element pass
+};
+
+__device__ __forceinline__ void begin_increment(Ctl &c)
+{
+  // Explicit::updateTimes (Explicit.C:414-427) for the increment to come
+  const bool go = c.status == 0 && c.t < c.t_end && c.t < c.t_stop && c.inc < c.inc_stop;
+  if (go)
+  {
+    if (c.t + c.dt > c.t_end)
+      c.dt = c.t_end - c.t;
+    c.inc += 1;
+    c.dt_eff = c.dt;
+    c.t_new = c.t + c.dt;
+    // Solver::computeTimeStep runs after the Jacobian when the solve goes on (Explicit.C:239-254, Solver.C:200)
+    c.due = (c.t_new < c.t_end) && (c.inc % c.ts_freq == 0);
+  }
+  else
+    c.due = 0;
+  c.active = go;
+  c.prepared = 1;
+}
+
+__device__ __forceinline__ void apply_courant(Ctl &c)
+{
+  // Solver::computeTimeStep (Solver.C:205-226): omega_max = 2 / dt_crit, or
+  // the power-iteration omega_max (Model.C:1008)
+  if (c.ts_method == DNL_TS_POWER_ITERATION)
+    c.dt = c.safety * c.omegaS / c.pi_omega;
+  else
+  {
+    const double crit = __longlong_as_double((long long)c.min_bits);
+    c.dt = c.safety * c.omegaS / (2.0 / crit);
+  }
+  c.min_bits = INF_BITS;
+}
+
+// end of the increment that ran, then begin the next one
+__device__ __forceinline__ void finish_increment(Ctl &c)
+{
+  if (c.prepared && c.active && c.status == 0)
+  {
+    // Explicit::endStep (Explicit.C:539-552): time, then the nodal field swap
+    c.t = c.t_new;
+    c.dt_last = c.dt_eff;
+    c.f0 ^= 1;
+    if (c.due)
+      apply_courant(c);
+  }
+  c.prepared = 0;
+  c.active = 0;
+  begin_increment(c);
+}
+
+__global__ void k_control(DevModel M, int phase, double t_stop, long long max_incs)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nInst)
+    return;
+  Ctl &c = M.ctl[i];
+  if (phase == CTL_FINISH)
+    finish_increment(c);
+  else if (phase == CTL_LIMITS)
+  {
+    const long long committed = c.inc - ((c.prepared && c.active) ? 1 : 0);
+    c.inc = committed;
+    c.t_stop = t_stop;
+    c.inc_stop = (max_incs > 0) ? committed + max_incs : 0x7fffffffffffffffll;
+    c.prepared = 0;
+    c.active = 0;
+    begin_increment(c);
+  }
+  else if (phase == CTL_INIT_DT)
+  {
+    apply_courant(c);
+    c.dt_eff = c.dt;
+    c.active = (c.status == 0);
+    c.prepared = 0;
+    c.due = 0;
+  }
+  else
+  {
+    c.active = 0;
+    c.prepared = 0;
+  }
+}
+
 // ------------------------------------------------------------- time step
 
 __device__ __forceinline__ double3 d3(const double4 &v) { return make_double3(v.x, v.y, v.z); }
@@ -1549,19 +1644,10 @@ __device__ __forceinline__ double charlen_q4(const double3 P[4])
 // Model::computeCourantTimeStep (Model.C:636-669): min over elements of l_e/c_e
 // with the elongation wave speed of the mean point density (Element.C:343-359).
 // One thread per element, a segmented warp-shuffle min over the lanes of one
-// instance, then one atomicMin per instance and warp.
+// instance, then one atomicMin per instance and warp (called by a full warp).
 template <typename R, int NPE>
-__global__ void __launch_bounds__(256) k_courant(DevModel M, int force)
+__device__ __forceinline__ void courant_warp(const DevModel &M, int e, int lane, int inst, bool act, Ctl *C)
 {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const bool valid = e < M.nE;
-  const int ec = valid ? e : M.nE - 1;
-  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
-  Ctl *C = M.ctl + inst;
-  const bool act = valid && (force || (C->active && C->due));
-  if (__ballot_sync(0xffffffffu, act) == 0)
-    return;
   double ratio = 1e300;
   if (act)
   {
@@ -1595,6 +1681,60 @@ __global__ void __launch_bounds__(256) k_courant(DevModel M, int force)
   const int prev = __shfl_up_sync(0xffffffffu, key, 1);
   if (act && (lane == 0 || prev != key))
     atomicMin(&C->min_bits, (unsigned long long)__double_as_longlong(ratio));
+}
+
+template <typename R, int NPE>
+__global__ void __launch_bounds__(256) k_courant(DevModel M, int force)
+{
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool valid = e < M.nE;
+  const int ec = valid ? e : M.nE - 1;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
+  Ctl *C = M.ctl + inst;
+  const bool act = valid && (force || (C->active && C->due));
+  if (__ballot_sync(0xffffffffu, act) == 0)
+    return;
+  courant_warp<R, NPE>(M, e, lane, inst, act, C);
+}
+
+// The Courant pass of an increment fused with the end of the increment:
+// persistent over elements (it only works every ts_freq increments), and the
+// block that finishes last runs finish_increment for every instance (what
+// k_control(CTL_FINISH) does), one launch instead of two.
+template <typename R, int NPE>
+__global__ void __launch_bounds__(256) k_courant_finish(DevModel M)
+{
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  const int nE32 = (M.nE + 31) & ~31; // whole warps, so every lane takes the same trips
+  const bool any = (M.nInst > 1) || (M.ctl[0].active && M.ctl[0].due);
+  if (any)
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nE32; e += stride)
+    {
+      const bool valid = e < M.nE;
+      const int ec = valid ? e : M.nE - 1;
+      const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
+      Ctl *C = M.ctl + inst;
+      const bool act = valid && C->active && C->due;
+      if (__ballot_sync(0xffffffffu, act) != 0)
+        courant_warp<R, NPE>(M, e, lane, inst, act, C);
+    }
+  // last block done: every block's minima are in memory before it counts itself
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0)
+    last = atomicAdd(M.done_count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last)
+  {
+    __threadfence();
+    for (int i = threadIdx.x; i < M.nInst; i += blockDim.x)
+      finish_increment(M.ctl[i]);
+    if (threadIdx.x == 0)
+      *M.done_count = 0;
+  }
 }
 
 // ------------------------------------------------- power-iteration time step
@@ -1810,96 +1950,6 @@ __global__ void __launch_bounds__(TILE) k_power_iteration(DevModel M, int force)
     C->pi_fmax = fmx;
     C->pi_omega = sqrt(fmx);
     C->pi_iters += it;
-  }
-}
-
-// ---------------------------------------------------------------- control
-
-enum
-{
-  CTL_FINISH = 0,   // end of the increment that ran, then begin the next one
-  CTL_LIMITS = 1,   // new pause time / increment budget, then begin
-  CTL_INIT_DT = 2,  // after the forced Courant pass of the start: dt, then arm the first element pass
-  CTL_POST_INIT = 3 // after the first element pass
-};
-
-__device__ __forceinline__ void begin_increment(Ctl &c)
-{
-  // Explicit::updateTimes (Explicit.C:414-427) for the increment to come
-  const bool go = c.status == 0 && c.t < c.t_end && c.t < c.t_stop && c.inc < c.inc_stop;
-  if (go)
-  {
-    if (c.t + c.dt > c.t_end)
-      c.dt = c.t_end - c.t;
-    c.inc += 1;
-    c.dt_eff = c.dt;
-    c.t_new = c.t + c.dt;
-    // Solver::computeTimeStep runs after the Jacobian when the solve goes on (Explicit.C:239-254, Solver.C:200)
-    c.due = (c.t_new < c.t_end) && (c.inc % c.ts_freq == 0);
-  }
-  else
-    c.due = 0;
-  c.active = go;
-  c.prepared = 1;
-}
-
-__device__ __forceinline__ void apply_courant(Ctl &c)
-{
-  // Solver::computeTimeStep (Solver.C:205-226): omega_max = 2 / dt_crit, or
-  // the power-iteration omega_max (Model.C:1008)
-  if (c.ts_method == DNL_TS_POWER_ITERATION)
-    c.dt = c.safety * c.omegaS / c.pi_omega;
-  else
-  {
-    const double crit = __longlong_as_double((long long)c.min_bits);
-    c.dt = c.safety * c.omegaS / (2.0 / crit);
-  }
-  c.min_bits = INF_BITS;
-}
-
-__global__ void k_control(DevModel M, int phase, double t_stop, long long max_incs)
-{
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= M.nInst)
-    return;
-  Ctl &c = M.ctl[i];
-  if (phase == CTL_FINISH)
-  {
-    if (c.prepared && c.active && c.status == 0)
-    {
-      // Explicit::endStep (Explicit.C:539-552): time, then the nodal field swap
-      c.t = c.t_new;
-      c.dt_last = c.dt_eff;
-      c.f0 ^= 1;
-      if (c.due)
-        apply_courant(c);
-    }
-    c.prepared = 0;
-    c.active = 0;
-    begin_increment(c);
-  }
-  else if (phase == CTL_LIMITS)
-  {
-    const long long committed = c.inc - ((c.prepared && c.active) ? 1 : 0);
-    c.inc = committed;
-    c.t_stop = t_stop;
-    c.inc_stop = (max_incs > 0) ? committed + max_incs : 0x7fffffffffffffffll;
-    c.prepared = 0;
-    c.active = 0;
-    begin_increment(c);
-  }
-  else if (phase == CTL_INIT_DT)
-  {
-    apply_courant(c);
-    c.dt_eff = c.dt;
-    c.active = (c.status == 0);
-    c.prepared = 0;
-    c.due = 0;
-  }
-  else
-  {
-    c.active = 0;
-    c.prepared = 0;
   }
 }
 

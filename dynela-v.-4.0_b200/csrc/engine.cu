@@ -324,7 +324,7 @@ int launch_element_any(dnl_engine *h, int mode)
 
 int launch_nodal(dnl_engine *h)
 {
-  const int threads = 256, blocks = (h->nN + threads - 1) / threads;
+  const int threads = 128, blocks = (h->nN + threads - 1) / threads;
   if (h->precision == DNL_PREC_MIXED)
   {
     if (h->dim == 3)
@@ -419,14 +419,42 @@ int launch_timestep(dnl_engine *h, int force)
   return h->powerIteration ? launch_pi(h, force) : launch_courant(h, force);
 }
 
+// End of an increment: the time-step pass when due and the control update.
+// With the Courant time step both run in one launch (k_courant_finish).
+int launch_step_end(dnl_engine *h)
+{
+  if (h->powerIteration)
+  {
+    launch_pi(h, 0);
+    return launch_control(h, CTL_FINISH);
+  }
+  const int threads = 256;
+  const int blocks = std::max(1, std::min((h->nE + threads - 1) / threads, 2 * h->numSMs));
+  if (h->precision == DNL_PREC_MIXED)
+  {
+    if (h->npe == 8)
+      k_courant_finish<float, 8><<<blocks, threads, 0, h->stream>>>(h->M);
+    else
+      k_courant_finish<float, 4><<<blocks, threads, 0, h->stream>>>(h->M);
+  }
+  else
+  {
+    if (h->npe == 8)
+      k_courant_finish<double, 8><<<blocks, threads, 0, h->stream>>>(h->M);
+    else
+      k_courant_finish<double, 4><<<blocks, threads, 0, h->stream>>>(h->M);
+  }
+  h->launches++;
+  return DNL_OK;
+}
+
 // One increment: the kernels of the graph.
 int enqueue_step(dnl_engine *h)
 {
   launch_bc_prep(h);
   launch_element_any(h, 0);
   launch_nodal(h);
-  launch_timestep(h, 0);
-  launch_control(h, CTL_FINISH);
+  launch_step_end(h);
   return DNL_OK;
 }
 
@@ -712,6 +740,14 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     return rc;
   }
   cudaMemsetAsync(h->dstats, 0, 5 * sizeof(unsigned long long), h->stream);
+  if ((rc = dalloc(h, &M.done_count, 1)))
+  {
+    std::string e = h->err;
+    dnl_engine_destroy(h);
+    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+    return rc;
+  }
+  cudaMemsetAsync(M.done_count, 0, sizeof(unsigned), h->stream);
   M.stats = h->dstats;
   M.harvest_count = h->dstats + 4;
   M.harvest_stride = 1;
@@ -854,8 +890,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
         CK(cudaEventRecord(e[1], h->stream));
         launch_nodal(h);
         CK(cudaEventRecord(e[2], h->stream));
-        launch_timestep(h, 0);
-        launch_control(h, CTL_FINISH);
+        launch_step_end(h);
         CK(cudaEventRecord(e[3], h->stream));
         CK(cudaEventSynchronize(e[3]));
         float t01, t12, t23;
@@ -1235,8 +1270,7 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps)
       launch_element_any(h, 0);
       CK(cudaEventRecord(e1, h->stream));
       launch_nodal(h);
-      launch_timestep(h, 0);
-      launch_control(h, CTL_FINISH);
+      launch_step_end(h);
       CK(cudaEventSynchronize(e1));
       float t = 0;
       cudaEventElapsedTime(&t, e0, e1);
