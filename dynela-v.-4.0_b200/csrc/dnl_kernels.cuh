@@ -43,7 +43,8 @@ struct __align__(128) Ctl
   int status, bad, resolves, ts_freq;
   double safety, omegaS, alphaM, beta, gammaN;
   int elem_begin, elem_end, node_begin, node_end;
-  int ts_method, pi_iters, direct, pad1; // direct: one-step return (Element::computeStressDirect)
+  int ts_method, pi_iters, direct, plane; // direct: one-step return (Element::computeStressDirect);
+                                          // plane: plane-strain quads (no axisymmetric terms)
   double pi_fmax, pi_omega; // power iteration: Model::_powerIterationFreqMax, last omega_max
   double dt_last;           // time step of the last completed increment
 };
@@ -385,10 +386,10 @@ template <typename R> struct SharedTile
 // F33 - 1 = sum N_n du_r,n / r, ElementAxi.C:78-100).
 template <typename R, int NPE>
 __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, const double4 &X, const double4 &U, R &detJ,
-                                           R (&inv)[3][3], R &radius, R (&H)[9])
+                                           R (&inv)[3][3], R &radius, R (&H)[9], bool axi)
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
-  constexpr bool AXI = ElemShape<NPE>::AXI;
+  const bool AXI = ElemShape<NPE>::AXI && axi;
   const double x0 = __shfl_sync(amask, X.x, base), y0 = __shfl_sync(amask, X.y, base),
                z0 = __shfl_sync(amask, X.z, base);
   const double ux0 = __shfl_sync(amask, U.x, base), uy0 = __shfl_sync(amask, U.y, base),
@@ -407,7 +408,7 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
   R Nr = R(0), Vr = R(0);
   GatherJG<R, NPE, 0>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
   radius = R(1);
-  if constexpr (AXI)
+  if (AXI)
   {
     // r = sum N_n x_n (ElementAxi.C:46-59) and sum N_n du_n, from the offsets
     radius = R(x0 + (double)Nr);
@@ -455,7 +456,7 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
         s += G[i][k] * inv[k][j];
       H[3 * i + j] = (i < DIM && j < DIM) ? s : R(0);
     }
-  if constexpr (AXI)
+  if (AXI)
     H[8] = Vr / radius;
 }
 
@@ -474,7 +475,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
                                                int node, const Src &old, R *row, R *grp)
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
-  constexpr bool AXI = ElemShape<NPE>::AXI;
+  const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
   constexpr int ROW = ElemShape<NPE>::ROW;
   using R4 = typename V4<R>::type;
   const double dt = C->dt_eff;
@@ -485,13 +486,13 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   R detJ, inv[3][3], radius, dE[6], Rot[9];
   {
     R H[9];
-    kinematics<R, NPE>(amask, g, base, X, U, detJ, inv, radius, H);
+    kinematics<R, NPE>(amask, g, base, X, U, detJ, inv, radius, H, !C->plane);
     polar_lnU<R>(H, dE, Rot);
   }
   if (detJ < R(0))
     raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
   R WxdJ = detJ; // Gauss weight 1
-  if constexpr (AXI)
+  if (AXI)
     WxdJ *= R(6.28318530717958647692) * radius;
 
   // element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
@@ -581,7 +582,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   }
   rotate_sym<R>(Rot, st.s);
   R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
-  if constexpr (AXI)
+  if (AXI)
     rho /= radius;
 #pragma unroll
   for (int c = 0; c < 6; c++)
@@ -647,7 +648,7 @@ template <typename R, int NPE, class Src, class Io>
 __device__ __forceinline__ void element_front(const Io &io, Ctl *C, int e, int g, int base, unsigned amask, int node,
                                               const Src &old, R *row, Front<R> &f)
 {
-  constexpr bool AXI = ElemShape<NPE>::AXI;
+  const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
   const MatDev &mp = io.mat(e);
   const double4 X = io.x(node);
   const double4 U = io.u(node);
@@ -655,13 +656,13 @@ __device__ __forceinline__ void element_front(const Io &io, Ctl *C, int e, int g
   R inv[3][3], Rot[9];
   {
     R H[9];
-    kinematics<R, NPE>(amask, g, base, X, U, f.detJ, inv, f.radius, H);
+    kinematics<R, NPE>(amask, g, base, X, U, f.detJ, inv, f.radius, H, !C->plane);
     polar_lnU<R>(H, f.dE, Rot);
   }
   if (f.detJ < R(0))
     raise_status(C, DNL_ERR_NEG_JACOBIAN, e);
   f.WxdJ = f.detJ; // Gauss weight 1
-  if constexpr (AXI)
+  if (AXI)
     f.WxdJ *= R(6.28318530717958647692) * f.radius;
 
   // element-mean volumetric increment (Element::computePressure, Element.C:1125-1143)
@@ -711,7 +712,7 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
                                             const Src &old, R *row, R *grp, Front<R> &f, R gamma0 = R(-1))
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
-  constexpr bool AXI = ElemShape<NPE>::AXI;
+  const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
   constexpr int ROW = ElemShape<NPE>::ROW;
   using R4 = typename V4<R>::type;
   const double dt = C->dt_eff;
@@ -771,7 +772,7 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
   }
   rotate_sym<R>(Rot, st.s);
   R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / f.detJ; // Element::computeDensity (Element.C:1243-1256)
-  if constexpr (AXI)
+  if (AXI)
     rho /= f.radius;
 #pragma unroll
   for (int c = 0; c < 6; c++)
@@ -828,7 +829,6 @@ template <typename R, int NPE>
 __global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
 {
   constexpr int ROW = ElemShape<NPE>::ROW;
-  constexpr bool AXI = ElemShape<NPE>::AXI;
   using R4 = typename V4<R>::type;
   __shared__ R sh[TILE * ROW];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -841,14 +841,16 @@ __global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
   if (!act)
     return;
   const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, e) : 0;
+  const bool AXI = ElemShape<NPE>::AXI && !M.ctl[inst].plane;
   const MatDev &mp = M.mat[M.emat[e]];
   const int node = M.conn[q];
   R detJ, inv[3][3], radius, H[9];
-  kinematics<R, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H);
+  kinematics<R, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H,
+                    !M.ctl[inst].plane);
   if (detJ < R(0))
     raise_status(M.ctl + inst, DNL_ERR_NEG_JACOBIAN, e);
   R WxdJ = detJ;
-  if constexpr (AXI)
+  if (AXI)
     WxdJ *= R(6.28318530717958647692) * radius;
   const R rho0 = R(mp.rho0);
 #pragma unroll
@@ -1749,14 +1751,14 @@ __device__ __forceinline__ void element_Kv(const DevModel &M, int q, int e, int 
                                            const double *v, double scale, double *row, double *grp)
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
-  constexpr bool AXI = ElemShape<NPE>::AXI;
+  const bool AXI = ElemShape<NPE>::AXI && !M.ctl[0].plane;
   constexpr int ROW = ElemShape<NPE>::ROW;
   const int node = M.conn[q];
   const MatDev &mp = M.mat[M.emat[e]];
   double detJ, inv[3][3], radius, H[9];
-  kinematics<double, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H);
+  kinematics<double, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H, AXI);
   double WxdJ = detJ;
-  if constexpr (AXI)
+  if (AXI)
     WxdJ *= 6.28318530717958647692 * radius;
   const double vx = v[3 * node] * scale, vy = v[3 * node + 1] * scale, vz = DIM == 3 ? v[3 * node + 2] * scale : 0.0;
   const double a = 0.57735026918962576451;
@@ -1804,7 +1806,8 @@ __device__ __forceinline__ void element_Kv(const DevModel &M, int q, int e, int 
       eps[0] += dNx[n][0] * ux;
       eps[1] += dNx[n][1] * uy;
       eps[2] += dNx[n][1] * ux + dNx[n][0] * uy;
-      eps[3] += Nn / radius * ux;
+      if (AXI)
+        eps[3] += Nn / radius * ux;
     }
   }
   const double E = mp.young, nu = mp.poisson, f = E / ((1 + nu) * (1 - 2 * nu));
@@ -1837,7 +1840,7 @@ __device__ __forceinline__ void element_Kv(const DevModel &M, int q, int e, int 
     }
     else
     {
-      row[n * 2] = (dNx[n][0] * sig[0] + dNx[n][1] * sig[2] + Nv[n] / radius * sig[3]) * WxdJ;
+      row[n * 2] = (dNx[n][0] * sig[0] + dNx[n][1] * sig[2] + (AXI ? Nv[n] / radius * sig[3] : 0.0)) * WxdJ;
       row[n * 2 + 1] = (dNx[n][1] * sig[1] + dNx[n][0] * sig[2]) * WxdJ;
     }
   }
@@ -1969,7 +1972,7 @@ __global__ void k_energies(DevModel M, double *out /* [nInst*3] */, int speed_fi
     const double4 v = M.v[fsel][i];
     ke += M.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0;
   }
-  const double wfac = (NPE == 4) ? 6.28318530717958647692 : 1.0;
+  const double wfac = (NPE == 4 && !c.plane) ? 6.28318530717958647692 : 1.0;
   for (int q = c.elem_begin * NPE + threadIdx.x; q < c.elem_end * NPE; q += blockDim.x)
   {
     const MatDev &mp = M.mat[M.emat[q / NPE]];

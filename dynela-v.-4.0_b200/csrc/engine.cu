@@ -118,7 +118,10 @@ int copy(dnl_engine *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind
   return DNL_OK;
 }
 
-int npe_of(int type) { return type == DNL_ELQUA4NAX ? 4 : (type == DNL_ELHEX8N3D ? 8 : 0); }
+int npe_of(int type)
+{
+  return (type == DNL_ELQUA4NAX || type == DNL_ELQUA4N2D) ? 4 : (type == DNL_ELHEX8N3D ? 8 : 0);
+}
 
 int check_desc(const dnl_model_desc *d, int idx)
 {
@@ -627,6 +630,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     c.ts_freq = d->ts_freq > 0 ? d->ts_freq : 10;
     c.ts_method = d->ts_method;
     c.direct = d->stress_method == DNL_STRESS_DIRECT;
+    c.plane = d->elem_type == DNL_ELQUA4N2D;
     c.t = d->t_start;
     c.t_end = d->t_end;
     c.t_stop = d->t_end;

@@ -17,7 +17,7 @@ hands the model to the engine (include/dnlgpu.h) and writes the history files
 at their save times.  There is no CPU solver behind this module: without the
 engine library or a CUDA device `solve()` raises EngineUnavailable.
 
-Scope of the mirror: the elements ElQua4NAx and ElHex8N3D, the Johnson-Cook
+Scope of the mirror: the elements ElQua4NAx, ElQua4N2D and ElHex8N3D, the Johnson-Cook
 law, BoundaryRestrain / BoundarySpeed (+ DiscreteFunction / RampFunction time
 functions), the Explicit solver with the Courant and power-iteration time
 steps, and HistoryFile.  SvgInterface and the VTK result files are accepted
@@ -60,8 +60,8 @@ class Element:
     ElGeneric = 0
     ElQua4NAx = _abi.ELQUA4NAX
     ElHex8N3D = _abi.ELHEX8N3D
+    ElQua4N2D = _abi.ELQUA4N2D
     # families outside the accelerated path
-    ElQua4N2D = 101
     ElTri3N2D = 102
     ElTet4N3D = 103
     ElTet10N3D = 104
@@ -422,8 +422,8 @@ class DynELA:
     def createElement(self, number, *nodes):
         if self._default_element == Element.ElGeneric:
             raise ValueError("Element type not set")
-        if self._default_element not in (Element.ElQua4NAx, Element.ElHex8N3D):
-            raise NotImplementedError("only ElQua4NAx and ElHex8N3D are available on the accelerated path")
+        if self._default_element not in (Element.ElQua4NAx, Element.ElHex8N3D, Element.ElQua4N2D):
+            raise NotImplementedError("only ElQua4NAx, ElQua4N2D and ElHex8N3D are available on the accelerated path")
         npe = _abi.NODES_PER_ELEMENT[self._default_element]
         if len(nodes) != npe:
             raise ValueError(f"element {number}: {len(nodes)} nodes given, {npe} expected")

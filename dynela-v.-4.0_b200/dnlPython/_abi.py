@@ -16,8 +16,9 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libdnlgpu.so")
 # element families
 ELQUA4NAX = 1
 ELHEX8N3D = 2
-NODES_PER_ELEMENT = {ELQUA4NAX: 4, ELHEX8N3D: 8}
-DIMS = {ELQUA4NAX: 2, ELHEX8N3D: 3}
+ELQUA4N2D = 3
+NODES_PER_ELEMENT = {ELQUA4NAX: 4, ELHEX8N3D: 8, ELQUA4N2D: 4}
+DIMS = {ELQUA4NAX: 2, ELHEX8N3D: 3, ELQUA4N2D: 2}
 
 STRESS_NEWTON, STRESS_DIRECT = 0, 1
 NUM_VARIANTS = 8  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)

@@ -277,3 +277,31 @@ def plate_necking(nx=128, nz=12, ny=320, width=10.0, thickness=1.0, length=25.0,
     t_end = necking_end_time(elongation, speed, ramp_frac)
     return _abi.ModelDesc(_abi.ELHEX8N3D, coords, conn, [mat], t_end=t_end, ts_freq=ts_freq, precision=precision,
                           **_pull_end(coords, length, speed, t_end, ramp_frac))
+
+
+def quad_block(nx, ny, size=(1.0, 1.0), mat=COPPER, t_end=1e-6, speed=0.0, seed=None, distort=0.0,
+               precision=_abi.PREC_FP64, ts_freq=10, elem_type=_abi.ELQUA4N2D):
+    """Structured block of nx*ny 4-node quads in the (x, y) plane (plane strain
+    by default; elem_type=ELQUA4NAX for the axisymmetric element), nodes
+    numbered row by row from y = 0.  With a seed, interior nodes are jittered by
+    `distort` x the cell size and the initial speed is random with magnitude
+    ~speed; y = 0 is restrained along y."""
+    xs, ys = np.linspace(0, size[0], nx + 1), np.linspace(0, size[1], ny + 1)
+    gy, gx = np.meshgrid(ys, xs, indexing="ij")
+    coords = np.zeros(((nx + 1) * (ny + 1), 3))
+    coords[:, 0], coords[:, 1] = gx.ravel(), gy.ravel()
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    n1 = (ii + jj * (nx + 1)).ravel()
+    conn = np.stack([n1, n1 + 1, n1 + nx + 2, n1 + nx + 1], axis=1)
+    rng = np.random.default_rng(seed)
+    if seed is not None and distort > 0:
+        h = min(size[0] / nx, size[1] / ny)
+        inner = (coords[:, 0] > 0) & (coords[:, 0] < size[0]) & (coords[:, 1] > 0) & (coords[:, 1] < size[1])
+        coords[inner, :2] += distort * h * rng.uniform(-1, 1, (inner.sum(), 2))
+    v = np.zeros_like(coords)
+    if speed:
+        v[:, :2] = speed * rng.uniform(-1, 1, (coords.shape[0], 2)) if seed is not None else [0.0, -speed]
+    bc = np.zeros(coords.shape, np.int8)
+    bc[coords[:, 1] <= 1e-12, 1] = _abi.BC_RESTRAIN
+    return _abi.ModelDesc(elem_type, coords, conn, [mat], v_init=v, bc_code=bc, t_end=t_end, precision=precision,
+                          ts_freq=ts_freq)

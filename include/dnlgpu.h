@@ -29,7 +29,8 @@ extern "C" {
 /* Element families on the path (Sources/dnlElements/Element.h type enum). */
 enum {
   DNL_ELQUA4NAX = 1, /* 4-node axisymmetric quad, 4 Gauss points (ElQua4NAx.C:21-240) */
-  DNL_ELHEX8N3D = 2  /* 8-node hexahedron, 8 Gauss points (ElHex8N3D.C:25-535) */
+  DNL_ELHEX8N3D = 2, /* 8-node hexahedron, 8 Gauss points (ElHex8N3D.C:25-535) */
+  DNL_ELQUA4N2D = 3  /* 4-node plane-strain quad, 4 Gauss points (ElQua4N2D.C, Element2D.C:53-99) */
 };
 
 /* Critical time step method (Solver.h Courant / PowerIteration). */
@@ -102,7 +103,7 @@ typedef struct dnl_function {
 
 /* One model (one simulation instance). */
 typedef struct dnl_model_desc {
-  int32_t elem_type;           /* DNL_ELQUA4NAX or DNL_ELHEX8N3D */
+  int32_t elem_type;           /* DNL_ELQUA4NAX, DNL_ELHEX8N3D or DNL_ELQUA4N2D */
   int32_t n_nodes;
   int32_t n_elems;
   const double *coords;        /* [n_nodes*3] */

@@ -39,6 +39,7 @@ const char *orc_last_error(void) { return g_err; }
 struct orc_model
 {
   int type, npe, dim;
+  int axi; /* ElementAxi family (ElQua4NAx); ElQua4N2D is plane strain */
   long nN, nE, nIP;
   double *x, *disp, *mass, *fint;
   double *fu[2], *fv[2], *fa[2]; /* nodal fields; fu[f0] is field0 */
@@ -125,15 +126,16 @@ orc_model *orc_create(const dnl_model_desc *d)
     set_err("invalid model description");
     return NULL;
   }
-  if (d->elem_type != DNL_ELQUA4NAX && d->elem_type != DNL_ELHEX8N3D)
+  if (d->elem_type != DNL_ELQUA4NAX && d->elem_type != DNL_ELHEX8N3D && d->elem_type != DNL_ELQUA4N2D)
   {
     set_err("unknown element type %d", d->elem_type);
     return NULL;
   }
   orc_model *m = (orc_model *)xcalloc(1, sizeof(orc_model));
   m->type = d->elem_type;
-  m->npe = (m->type == DNL_ELQUA4NAX) ? 4 : 8;
-  m->dim = (m->type == DNL_ELQUA4NAX) ? 2 : 3;
+  m->npe = (m->type == DNL_ELHEX8N3D) ? 8 : 4;
+  m->dim = (m->type == DNL_ELHEX8N3D) ? 3 : 2;
+  m->axi = (m->type == DNL_ELQUA4NAX);
   m->nN = d->n_nodes;
   m->nE = d->n_elems;
   m->nIP = m->nE * m->npe;
@@ -614,7 +616,7 @@ static int jacobian(orc_model *m, int reference)
             s += m->dNdxi[g][n][j] * inv[j][k];
           dn[3 * n + k] = s;
         }
-      if (m->type == DNL_ELQUA4NAX)
+      if (m->axi)
       {
         double r = 0.0;
         for (int n = 0; n < npe; n++)
@@ -624,7 +626,7 @@ static int jacobian(orc_model *m, int reference)
       else
         m->radius[q] = 1.0;
       if (reference)
-        IPV(m, DNL_IP_DETJ0, q) = (m->type == DNL_ELQUA4NAX) ? det * m->radius[q] : det;
+        IPV(m, DNL_IP_DETJ0, q) = (m->axi) ? det * m->radius[q] : det;
     }
   }
   return DNL_OK;
@@ -656,7 +658,8 @@ static void strains(orc_model *m)
           F[4] += dn[3 * n + 1] * un[1];
           Vr += m->N[g][n] * un[0];
         }
-        F[8] += Vr / m->radius[q];
+        if (m->axi)
+          F[8] += Vr / m->radius[q];
       }
       else
       {
@@ -779,7 +782,7 @@ static void internal_forces(orc_model *m)
     {
       long q = e * npe + g;
       double WxdJ = m->w[g] * m->detJ[q];
-      if (m->type == DNL_ELQUA4NAX)
+      if (m->axi)
         WxdJ *= TWO_PI * m->radius[q];
       const double *dn = m->dNdx + q * npe * 3;
       for (int n = 0; n < npe; n++)
@@ -787,7 +790,7 @@ static void internal_forces(orc_model *m)
         for (int i = 0; i < d; i++)
           for (int j = 0; j < d; j++)
             fe[n * d + i] -= dn[3 * n + j] * IPV(m, SYM[j][i], q) * WxdJ;
-        if (m->type == DNL_ELQUA4NAX)
+        if (m->axi)
           fe[n * d] -= m->N[g][n] * IPV(m, 5, q) / m->radius[q] * WxdJ;
       }
     }
@@ -820,7 +823,7 @@ static void density(orc_model *m)
     {
       long q = e * m->npe + g;
       double r = mt->density * IPV(m, DNL_IP_DETJ0, q) / m->detJ[q];
-      if (m->type == DNL_ELQUA4NAX)
+      if (m->axi)
         r /= m->radius[q];
       IPV(m, DNL_IP_DENSITY, q) = r;
     }
@@ -841,7 +844,7 @@ static void mass_matrix(orc_model *m)
     {
       long q = e * m->npe + g;
       double WxdJ = m->w[g] * m->detJ[q];
-      if (m->type == DNL_ELQUA4NAX)
+      if (m->axi)
         WxdJ *= TWO_PI * m->radius[q];
       for (int n = 0; n < m->npe; n++)
         me[n] += mt->density * m->N[g][n] * WxdJ;
@@ -946,7 +949,7 @@ static double wave_speed(orc_model *m, long e) /* Element::getElongationWaveSpee
 static double charlen(orc_model *m, long e)
 {
   const int32_t *cn = m->conn + e * m->npe;
-  return (m->type == DNL_ELQUA4NAX) ? charlen_q4(m->x, cn) : charlen_hex(m->x, cn);
+  return (m->dim == 2) ? charlen_q4(m->x, cn) : charlen_hex(m->x, cn);
 }
 
 /* Model::computeCourantTimeStep (Model.C:636-669). */
@@ -983,11 +986,18 @@ static void stiffness(orc_model *m, long e, double *K /* [nd*nd] */)
   const double f = E / ((1 + nu) * (1 - 2 * nu));
   int npe = m->npe, d = m->dim, nd = npe * d;
   double C[6][6] = {{0}};
-  if (m->dim == 2)
+  if (m->dim == 2 && m->axi)
   {
     C[0][0] = C[1][1] = C[3][3] = (1 - nu) * f;
     C[2][2] = (1 - 2 * nu) * f;
     C[1][0] = C[0][1] = C[3][0] = C[0][3] = C[3][1] = C[1][3] = nu * f;
+  }
+  else if (m->dim == 2)
+  {
+    /* Material::getHookeStiffnessMatrix(planeStrain), Material.C:105-113 */
+    C[0][0] = C[1][1] = (1 - nu) * f;
+    C[2][2] = (1 - 2 * nu) * f;
+    C[1][0] = C[0][1] = nu * f;
   }
   else
   {
@@ -1004,10 +1014,11 @@ static void stiffness(orc_model *m, long e, double *K /* [nd*nd] */)
     double WxdJ = m->w[g] * m->detJ[q], R = m->radius[q];
     if (m->dim == 2)
     {
-      WxdJ *= TWO_PI * R;
+      if (m->axi)
+        WxdJ *= TWO_PI * R;
       for (int i = 0; i < npe; i++)
       {
-        double dNx = dn[3 * i], dNy = dn[3 * i + 1], NoR = m->N[g][i] / R;
+        double dNx = dn[3 * i], dNy = dn[3 * i + 1], NoR = m->axi ? m->N[g][i] / R : 0.0;
         int I = 2 * i;
         for (int r = 0; r < 4; r++)
         {
@@ -1017,7 +1028,7 @@ static void stiffness(orc_model *m, long e, double *K /* [nd*nd] */)
       }
       for (int i = 0; i < npe; i++)
       {
-        double dNx = dn[3 * i], dNy = dn[3 * i + 1], NoR = m->N[g][i] / R;
+        double dNx = dn[3 * i], dNy = dn[3 * i + 1], NoR = m->axi ? m->N[g][i] / R : 0.0;
         for (int j = 0; j < npe; j++)
         {
           int I = 2 * i, J = 2 * j;
@@ -1402,7 +1413,7 @@ int orc_energies(orc_model *m, double out[3])
     for (int g = 0; g < m->npe; g++)
     {
       long q = e * m->npe + g;
-      double wgt = mt->density * IPV(m, DNL_IP_DETJ0, q) * m->w[g] * (m->type == DNL_ELQUA4NAX ? TWO_PI : 1.0);
+      double wgt = mt->density * IPV(m, DNL_IP_DETJ0, q) * m->w[g] * (m->axi ? TWO_PI : 1.0);
       ei += wgt * IPV(m, DNL_IP_EINT, q);
       ep += wgt * IPV(m, DNL_IP_EINEL, q);
     }

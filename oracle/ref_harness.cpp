@@ -64,6 +64,7 @@
 #include <BoundarySpeed.h>
 #include <DiscreteFunction.h>
 #include <ElQua4NAx.h>
+#include <ElQua4N2D.h>
 #include <ElHex8N3D.h>
 #include <Timer.h>
 #undef private
@@ -126,7 +127,7 @@ void *ref_create(const dnl_model_desc *d, const char *workdir)
   }
   RefModel *m = new RefModel;
   m->type = d->elem_type;
-  if (d->elem_type == DNL_ELQUA4NAX)
+  if (d->elem_type == DNL_ELQUA4NAX || d->elem_type == DNL_ELQUA4N2D)
   {
     m->npe = 4;
     m->dim = 2;
@@ -165,7 +166,9 @@ void *ref_create(const dnl_model_desc *d, const char *workdir)
     fprintf(stderr, "ref_harness: cannot return to %s\n", cwd);
   DynELA *dyn = m->dyn;
 
-  dyn->setDefaultElement(d->elem_type == DNL_ELQUA4NAX ? Element::ElQua4NAx : Element::ElHex8N3D);
+  dyn->setDefaultElement(d->elem_type == DNL_ELQUA4NAX   ? Element::ElQua4NAx
+                         : d->elem_type == DNL_ELQUA4N2D ? Element::ElQua4N2D
+                                                         : Element::ElHex8N3D);
   long bulkMin = 20000; // meshes from this many elements take the bulk path below
   if (const char *env = getenv("DNL_REF_BULK_MIN_ELEMS"))
     bulkMin = atol(env);
@@ -200,7 +203,9 @@ void *ref_create(const dnl_model_desc *d, const char *workdir)
     model.nodes.compact();
     for (long e = 0; e < m->nE; e++)
     {
-      Element *pel = (m->npe == 4) ? (Element *)new ElQua4NAx(e + 1) : (Element *)new ElHex8N3D(e + 1);
+      Element *pel = d->elem_type == DNL_ELQUA4NAX   ? (Element *)new ElQua4NAx(e + 1)
+                     : d->elem_type == DNL_ELQUA4N2D ? (Element *)new ElQua4N2D(e + 1)
+                                                     : (Element *)new ElHex8N3D(e + 1);
       pel->createIntegrationPoints();
       model.elements << pel;
       const int32_t *c = d->conn + (long)m->npe * e;

@@ -95,6 +95,9 @@ CASES = {
                                          helpers.case_hex_small().copy(stress_method=_abi.STRESS_DIRECT), seed=7),
     # the round bar pulled by a ramped end speed (necking workload, small mesh)
     "bar_necking_run": lambda: run_case("bar_necking_run", helpers.case_bar_necking(), [1, 10, 60]),
+    # plane-strain quads (ElQua4N2D)
+    "plane_run": lambda: run_case("plane_run", helpers.case_plane_small(), [1, 10, 60]),
+    "plane_pass": lambda: pass_case("plane_pass", helpers.case_plane_small(), seed=8),
     "taylor_axi_sample": published_case,
 }
 

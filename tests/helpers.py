@@ -153,3 +153,10 @@ def case_bar_necking(precision=_abi.PREC_FP64):
     """Round bar of the necking workload on a coarse mesh (4 x 4 O-grid, 20
     layers), pulled by its ramped end speed."""
     return meshes.bar_necking(n_core=4, n_ring=4, n_axial=20, precision=precision)
+
+
+def case_plane_small(precision=_abi.PREC_FP64):
+    """Plane-strain block (ElQua4N2D) with a distorted mesh and a random
+    initial speed field."""
+    return meshes.quad_block(4, 6, size=(1.2, 1.8), speed=60000.0, seed=13, distort=0.12, t_end=5e-6,
+                             precision=precision, ts_freq=3)

@@ -154,6 +154,9 @@ def test_boundary_resolution_rules():
     ("Element/Tensile/ElHex8N3D/Tensile.py", _abi.ELHEX8N3D, None),
     ("Element/Radial/ElQua4NAx/Radial.py", _abi.ELQUA4NAX, None),
     ("Element/Torus/ElQua4NAx/Torus.py", _abi.ELQUA4NAX, None),
+    ("PlateNecking/PlateNecking.py", _abi.ELQUA4N2D, None),
+    ("Element/Shear/ElQua4N2D/Shear.py", _abi.ELQUA4N2D, None),
+    ("Element/Tensile/ElQua4N2D/Tensile.py", _abi.ELQUA4N2D, None),
 ])
 def test_reference_samples_parse_unchanged(sample, etype, count, tmp_path, monkeypatch):
     captured = {}

@@ -265,8 +265,10 @@ def test_power_iteration_taylor_axi_sample(precision):
         assert abs(epsp - row[5]) < 1e-3 * row[5]
 
 
-def test_power_iteration_hex_vs_oracle():
-    desc = helpers.case_hex_small().copy(ts_method=_abi.TS_POWER_ITERATION, ts_freq=2)
+@pytest.mark.parametrize("case", ["hex", "plane"])
+def test_power_iteration_vs_oracle(case):
+    base = helpers.case_hex_small() if case == "hex" else helpers.case_plane_small()
+    desc = base.copy(ts_method=_abi.TS_POWER_ITERATION, ts_freq=2)
     with oracle.OracleModel(desc) as o, engine(desc) as e:
         o.init()
         e.init()
