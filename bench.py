@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--variant", type=int, default=-1,
-                   help="element-pass variant (0-3); default: chosen by the autotuner")
+                   help="element-pass variant (0-7); default: chosen by the autotuner")
     p.add_argument("--no-accuracy", action="store_true", help="skip the whole-run mixed/FP64 comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
     p.add_argument("--no-guess", action="store_true", help="skip the learned Newton initial guess block")
@@ -258,35 +258,45 @@ def accuracy_run():
     return res
 
 
-def batch_run(sample):
+def batch_run(sample, dist=None, world=1, rank=0):
     """256 independent copper Taylor bars (element counts log-uniform in
     2k-60k, speed U(150,300) m/s, Johnson-Cook A, B, n, C, m scaled by
     U(0.8,1.2), seed 20261203) advanced together to 80 us on the mixed path,
     against a size-stratified sample of the same bars run one by one on the
-    FP64 path."""
+    FP64 path.  On several GPUs the bars are partitioned over the ranks
+    (dnlPython.parallel.shard_instances, no exchange during the run) and the
+    time is the slowest rank's."""
     import numpy as np
-    from dnlPython import meshes, _abi
+    from dnlPython import meshes, _abi, parallel
     from dnlPython.engine import Engine
-    descs = meshes.taylor_batch()
+    all_descs = meshes.taylor_batch()
+    mine = parallel.shard_instances([parallel.instance_cost(d) for d in all_descs], world)[rank]
+    descs = [all_descs[i] for i in mine]
     elems = np.array([d.n_elems for d in descs], dtype=np.float64)
     t0 = time.perf_counter()
     with Engine(descs) as b:
         b.init()
         variant, _ = b.autotune(steps=6)
         setup = time.perf_counter() - t0
+        if dist is not None:
+            dist.barrier()
         replays = b.run(check=False)
-        ms = b.timings()["run_ms"]
+        ms_rank = b.timings()["run_ms"]
         launches = b.launch_count()
         ctl = [b.control(i) for i in range(len(descs))]
     incs = np.array([c["increment"] for c in ctl], dtype=np.float64)
-    failed = [i for i, c in enumerate(ctl) if c["status"] != 0]
-    steps = float((elems * incs).sum())
-    out = {"instances": len(descs), "elements": int(elems.sum()), "seed": 20261203, "precision": "mixed",
-           "replays": int(replays), "run_ms": ms, "sims_per_s": len(descs) / (ms / 1e3),
-           "elem_steps_per_s": steps / (ms / 1e3), "increments_min_max": [int(incs.min()), int(incs.max())],
-           "stopped_on_error": {str(i): _abi.ERRORS.get(ctl[i]["status"], ctl[i]["status"]) + f" at t={ctl[i]['time']:.3e}"
-                                for i in failed},
-           "element_variant": int(variant), "gpu_launches": launches, "setup_s": setup}
+    failed = [mine[i] for i, c in enumerate(ctl) if c["status"] != 0]
+    steps_rank = float((elems * incs).sum())
+    ms = parallel.reduce_max(ms_rank, dist)
+    steps = parallel.reduce_sum(steps_rank, dist)
+    n_all = len(all_descs)
+    out = {"instances": n_all, "elements": int(sum(d.n_elems for d in all_descs)), "seed": 20261203,
+           "precision": "mixed", "ranks": world, "replays_rank0": int(replays), "run_ms": ms,
+           "sims_per_s": n_all / (ms / 1e3), "elem_steps_per_s": steps / (ms / 1e3),
+           "increments_min_max_rank0": [int(incs.min()), int(incs.max())],
+           "stopped_on_error_rank0": {str(i): _abi.ERRORS.get(ctl[mine.index(i)]["status"], "error")
+                                      + f" at t={ctl[mine.index(i)]['time']:.3e}" for i in failed},
+           "element_variant_rank0": int(variant), "gpu_launches_rank0": launches, "setup_s_rank0": setup}
     if sample > 0:
         order = np.argsort(elems, kind="stable")
         pick = order[np.linspace(0, len(order) - 1, min(sample, len(order))).astype(int)]
@@ -394,12 +404,8 @@ def run_engine_arm(args, rank, world, dist):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from dnlPython import parallel
+        return parallel.reduce_max(x, dist)
 
     desc = workload(args.precision)
     word = 4 if args.precision == "mixed" else 8
@@ -463,14 +469,21 @@ def run_engine_arm(args, rank, world, dist):
     # ---- end to end through the public API, host buffers in and out
     e2e = None
     if not args.no_e2e:
+        # the caller's result buffers, page-locked and allocated once (outside the timing)
+        import torch
+        ips_host = torch.empty((_abi.IP_NCOMP, desc.n_ips), dtype=torch.float64, pin_memory=True).numpy()
+        coords_host = torch.empty((desc.n_nodes, 3), dtype=torch.float64, pin_memory=True).numpy()
         barrier()
         t0 = time.perf_counter()
         e = Engine(desc)
+        ta = time.perf_counter()
         e.init()
         e.set_variant(variant)
+        tb = time.perf_counter()
         e.run(max_incs=args.steps)
-        coords = e.nodes(_abi.NODE_COORDS)
-        ips = e.ips()
+        tc = time.perf_counter()
+        coords = e.nodes(_abi.NODE_COORDS, out=coords_host)
+        ips = e.ips(out=ips_host)
         t1 = time.perf_counter()
         e.close()
         wall = max_over_ranks(t1 - t0)
@@ -478,7 +491,15 @@ def run_engine_arm(args, rank, world, dist):
         d2h = coords.nbytes + ips.nbytes
         e2e = {"value": world * desc.n_elems * args.steps / wall, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "what": "model upload + start of the solve + K increments + coordinates and point state read back"}
+               "what": "model upload + start of the solve + K increments + coordinates and point state read back "
+                       "into page-locked host arrays allocated before the timing",
+               "seconds": {"create_upload": ta - t0, "start": tb - ta, "increments": tc - tb, "read_back": t1 - tc}}
+
+    batched = None
+    if not args.no_batch:
+        # partitioned over the ranks (collective timing: every rank takes part);
+        # the one-by-one FP64 sample on a single GPU only
+        batched = batch_run(args.batch_fp64_sample if world == 1 else 0, dist, world, rank)
 
     if rank != 0:
         return
@@ -509,8 +530,8 @@ def run_engine_arm(args, rank, world, dist):
     # whole runs and the batch hold one GPU for a few minutes: single-GPU runs only
     if world == 1 and AXIAL == 160 and not args.no_accuracy:
         out["accuracy_whole_run"] = accuracy_run()
-    if world == 1 and not args.no_batch:
-        out["batched"] = batch_run(args.batch_fp64_sample)
+    if batched:
+        out["batched"] = batched
     if world == 1 and not args.no_necking:
         out["necking"] = necking_run()
     if world == 1 and AXIAL == 160 and not args.no_guess:

@@ -319,6 +319,139 @@ template <typename R, int NPE, int N> struct ForcesToShared
   }
 };
 
+template <int NPE> struct ElemShape
+{
+  static constexpr int DIM = (NPE == 8) ? 3 : 2;
+  static constexpr bool AXI = (NPE == 4);
+  // shared-memory row per point (padded for bank spread): the element forces
+  // of the transpose, or the rotation and inverse Jacobian parked across the return
+  static constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
+  // the element pass's row: the rotation and J^-1 parked across the return
+  // (the hexahedron's forces need no transpose, the quadrilaterals' 8 fit)
+  static constexpr int PASS_ROW = 19;
+};
+
+// Hexahedron in modal form.  With the node signs of node_sign(),
+// s0 = -chi_3(n), s1 = -chi_2(n), s2 = -chi_4(n), s0 s1 = chi_1(n),
+// s0 s2 = chi_7(n), s1 s2 = chi_6(n), s0 s1 s2 = -chi_5(n), where
+// chi_w(n) = (-1)^popcount(w & n), so that the shape-function derivatives of
+// ElHex8N3D.C:561-632 read
+//   8 dN_n/dxi0 = -chi_3 + chi_1 xi1 + chi_7 xi2 - chi_5 xi1 xi2
+//   8 dN_n/dxi1 = -chi_2 + chi_1 xi0 + chi_6 xi2 - chi_5 xi0 xi2
+//   8 dN_n/dxi2 = -chi_4 + chi_7 xi0 + chi_6 xi1 - chi_5 xi0 xi1.
+// The Jacobian at a Gauss point is then a combination of the Walsh sums
+// W_w = sum_n chi_w(n) x_n of the element's nodes, and the nodal forces are
+// the Walsh transform of the per-point terms summed over the points.  Both
+// run on the element's eight lanes (lane g holds node g and Gauss point g) with
+// butterflies over lane bits instead of per-node loops.
+
+// In place: lane w of the group ends with sum_n chi_w(n) v_n.
+template <typename R, int NC>
+__device__ __forceinline__ void walsh8(unsigned amask, int g, R (&v)[NC])
+{
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+  {
+    const R sg = ((g >> k) & 1) ? R(-1) : R(1); // bit 0: v + p, bit 1: p - v
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      v[c] = sg * v[c] + __shfl_xor_sync(amask, v[c], 1 << k);
+  }
+}
+
+// J (and G) at this lane's Gauss point from the offsets of the element's nodes
+// (this lane's node offset in o[0..2] for x and o[3..5] for the increment).
+template <typename R>
+__device__ __forceinline__ void hex_jacobians(unsigned amask, int g, int base, R xi0, R xi1, R xi2, R (&o)[6],
+                                              R (&J)[3][3], R (&G)[3][3])
+{
+  walsh8<R, 6>(amask, g, o);
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+    o[c] *= R(0.125);
+  const R x01 = xi0 * xi1, x02 = xi0 * xi2, x12 = xi1 * xi2;
+#pragma unroll
+  for (int c = 0; c < 6; c++)
+  {
+    const R w1 = __shfl_sync(amask, o[c], base + 1), w2 = __shfl_sync(amask, o[c], base + 2);
+    const R w3 = __shfl_sync(amask, o[c], base + 3), w4 = __shfl_sync(amask, o[c], base + 4);
+    const R w5 = __shfl_sync(amask, o[c], base + 5), w6 = __shfl_sync(amask, o[c], base + 6);
+    const R w7 = __shfl_sync(amask, o[c], base + 7);
+    R(&T)[3][3] = c < 3 ? J : G;
+    const int i = c < 3 ? c : c - 3;
+    T[i][0] = w1 * xi1 + w7 * xi2 - w5 * x12 - w3;
+    T[i][1] = w1 * xi0 + w6 * xi2 - w5 * x02 - w2;
+    T[i][2] = w7 * xi0 + w6 * xi1 - w5 * x01 - w4;
+  }
+}
+
+// Nodal forces f_n = sum_g sum_k dN_n/dxi_k(xi_g) P_g[k][.] of the element,
+// returned on lane n: the per-point modal terms Z_w, then a reduction over the
+// eight lanes fused with the Walsh transform (at each lane bit the pair of
+// lanes exchanges the half of the terms the partner keeps).
+template <typename R>
+__device__ __forceinline__ void hex_forces(unsigned amask, int g, R xi0, R xi1, R xi2, const R (&P)[3][3], R (&f)[3])
+{
+  const R x01 = xi0 * xi1, x02 = xi0 * xi2, x12 = xi1 * xi2;
+  const R s0 = (g & 1) ? R(-1) : R(1), s1 = (g & 2) ? R(-1) : R(1), s2 = (g & 4) ? R(-1) : R(1);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+  {
+    const R p0 = P[0][i], p1 = P[1][i], p2 = P[2][i];
+    const R z1 = xi1 * p0 + xi0 * p1, z2 = -p1, z3 = -p0, z4 = -p2;
+    const R z5 = -(x12 * p0 + x02 * p1 + x01 * p2);
+    const R z6 = xi2 * p1 + xi1 * p2, z7 = xi2 * p0 + xi0 * p2;
+    // lane bit 0: pairs (z0 = 0, z1), (z2, z3), (z4, z5), (z6, z7)
+    const R a0 = s0 * z1 - __shfl_xor_sync(amask, s0 * z1, 1);
+    const R a1 = (z2 + s0 * z3) + __shfl_xor_sync(amask, z2 - s0 * z3, 1);
+    const R a2 = (z4 + s0 * z5) + __shfl_xor_sync(amask, z4 - s0 * z5, 1);
+    const R a3 = (z6 + s0 * z7) + __shfl_xor_sync(amask, z6 - s0 * z7, 1);
+    // lane bit 1: pairs (a0, a1), (a2, a3)
+    const R b0 = (a0 + s1 * a1) + __shfl_xor_sync(amask, a0 - s1 * a1, 2);
+    const R b1 = (a2 + s1 * a3) + __shfl_xor_sync(amask, a2 - s1 * a3, 2);
+    // lane bit 2
+    f[i] = R(0.125) * ((b0 + s2 * b1) + __shfl_xor_sync(amask, b0 - s2 * b1, 4));
+  }
+}
+
+// The element's nodal forces from this lane's P (and hoop term), returned for
+// this lane's node: modal butterflies for the hexahedron, a shared-memory
+// transpose for the quadrilaterals (row: this lane's row, grp: the element's first).
+template <typename R, int NPE>
+__device__ __forceinline__ typename V4<R>::type element_forces(unsigned amask, int g, const R (&P)[3][3], R hoop,
+                                                               R *row, R *grp)
+{
+  constexpr int DIM = ElemShape<NPE>::DIM;
+  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  static_assert(ROW >= NPE * DIM || NPE == 8, "the transpose needs NPE * DIM values per row");
+  const R a = R(0.57735026918962576451);
+  const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
+  typename V4<R>::type fs;
+  fs.x = fs.y = fs.z = fs.w = R(0);
+  if constexpr (NPE == 8)
+  {
+    R f[3];
+    hex_forces<R>(amask, g, xi0, xi1, xi2, P, f);
+    fs.x = f[0];
+    fs.y = f[1];
+    fs.z = f[2];
+  }
+  else
+  {
+    ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
+    __syncwarp(amask);
+#pragma unroll
+    for (int l = 0; l < NPE; l++)
+    {
+      fs.x += grp[l * ROW + g * DIM];
+      fs.y += grp[l * ROW + g * DIM + 1];
+      if constexpr (DIM == 3)
+        fs.z += grp[l * ROW + g * DIM + 2];
+    }
+  }
+  return fs;
+}
+
 template <typename R, int NPE, int N> struct MassToShared
 {
   static __device__ __forceinline__ void run(R xi0, R xi1, R xi2, R scale, R *row)
@@ -340,14 +473,6 @@ template <typename R, int NPE, int N> struct MassToShared
 #define DNL_ELEM_MINB_F64 4
 #endif
 
-template <int NPE> struct ElemShape
-{
-  static constexpr int DIM = (NPE == 8) ? 3 : 2;
-  static constexpr bool AXI = (NPE == 4);
-  // shared-memory row per point (padded for bank spread): the element forces
-  // of the transpose, or the rotation and inverse Jacobian parked across the return
-  static constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
-};
 
 // How the element update reaches nodes, materials and its outputs in the
 // engine's own arrays (tile-major point state, node-ordered force slots).
@@ -406,7 +531,13 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
     for (int j = 0; j < 3; j++)
       J[i][j] = G[i][j] = R(0);
   R Nr = R(0), Vr = R(0);
-  GatherJG<R, NPE, 0>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
+  if constexpr (NPE == 8)
+  {
+    R o[6] = {rx, ry, rz, urx, ury, urz};
+    hex_jacobians<R>(amask, g, base, xi0, xi1, xi2, o, J, G);
+  }
+  else
+    GatherJG<R, NPE, 0>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
   radius = R(1);
   if (AXI)
   {
@@ -476,7 +607,6 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
   const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
-  constexpr int ROW = ElemShape<NPE>::ROW;
   using R4 = typename V4<R>::type;
   const double dt = C->dt_eff;
   const MatDev &mp = io.mat(e);
@@ -612,22 +742,8 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
         s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
       P[k][i] = -WxdJ * s;
     }
-  const R a = R(0.57735026918962576451);
-  const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
   const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
-  ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
-  __syncwarp(amask);
-  R4 fs;
-  fs.x = fs.y = fs.z = fs.w = R(0);
-#pragma unroll
-  for (int l = 0; l < NPE; l++)
-  {
-    fs.x += grp[l * ROW + g * DIM];
-    fs.y += grp[l * ROW + g * DIM + 1];
-    if constexpr (DIM == 3)
-      fs.z += grp[l * ROW + g * DIM + 2];
-  }
-  io.slot(fs);
+  io.slot(element_forces<R, NPE>(amask, g, P, hoop, row, grp));
 }
 
 // What the first half of an element update hands to the second: the strain
@@ -713,7 +829,6 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
   const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
-  constexpr int ROW = ElemShape<NPE>::ROW;
   using R4 = typename V4<R>::type;
   const double dt = C->dt_eff;
   const MatDev &mp = io.mat(e);
@@ -802,22 +917,8 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
         s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
       P[k][i] = -f.WxdJ * s;
     }
-  const R a = R(0.57735026918962576451);
-  const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
   const R hoop = AXI ? st.s[5] / f.radius * f.WxdJ : R(0);
-  ForcesToShared<R, NPE, 0>::run(xi0, xi1, xi2, P, hoop, row);
-  __syncwarp(amask);
-  R4 fs;
-  fs.x = fs.y = fs.z = fs.w = R(0);
-#pragma unroll
-  for (int l = 0; l < NPE; l++)
-  {
-    fs.x += grp[l * ROW + g * DIM];
-    fs.y += grp[l * ROW + g * DIM + 1];
-    if constexpr (DIM == 3)
-      fs.z += grp[l * ROW + g * DIM + 2];
-  }
-  io.slot(fs);
+  io.slot(element_forces<R, NPE>(amask, g, P, hoop, row, grp));
   return iters;
 }
 
@@ -878,7 +979,7 @@ __global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M)
 {
-  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   __shared__ R sh[TILE * ROW];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -953,7 +1054,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTiles, int *err)
 {
-  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
   constexpr uint32_t CONN_BYTES = TILE * sizeof(int);
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1037,21 +1138,38 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Element update I/O for a tile whose node coordinates and increments, force
 // slot positions and element materials were staged in shared memory.
+// A staged node vector: x and y in one 16-byte run, z in another array, so
+// that a tile of nodes takes 24 bytes a node (the device arrays are double4).
+struct StagedVec
+{
+  const double2 *xy;
+  const double *z;
+  __device__ __forceinline__ double4 get() const
+  {
+    const double2 a = *xy;
+    return make_double4(a.x, a.y, *z, 0.0);
+  }
+};
+
 template <typename R> struct StagedIo
 {
   using R4 = typename V4<R>::type;
   const DevModel &M;
   int q;
-  const double4 *nx, *nu; // this lane's node
+  StagedVec nx, nu; // this lane's node
   int spos;
   const MatDev *mp;
-  __device__ __forceinline__ double4 x(int) const { return *nx; }
-  __device__ __forceinline__ double4 u(int) const { return *nu; }
+  __device__ __forceinline__ double4 x(int) const { return nx.get(); }
+  __device__ __forceinline__ double4 u(int) const { return nu.get(); }
   __device__ __forceinline__ const MatDev &mat(int) const { return *mp; }
   __device__ __forceinline__ const MatDev *matp(int) const { return mp; }
   __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
@@ -1065,25 +1183,40 @@ template <typename R> struct StagedIo
 // coordinates and increments of the next tile's nodes are gathered by
 // asynchronous copies while the current tile computes, so the update reads
 // every input from shared memory.
+template <typename R, int NPE> struct StageLayout
+{
+  static constexpr int EPT = TILE / NPE; // elements per tile
+  static constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
+  // coordinates then increments, each as xy[TILE] (double2) and z[TILE]
+  static constexpr uint32_t NODE_BYTES = 2 * TILE * (sizeof(double2) + sizeof(double));
+  static constexpr uint32_t IDX_BYTES = TILE * sizeof(int);
+  static constexpr uint32_t EMAT_BYTES = EPT * sizeof(int);
+  static_assert(EMAT_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
+  // shared memory: state[2] | nodes[2] | (slot positions, materials)[2] | connectivity[3] | rows
+  static constexpr uint32_t OFF_NODES = 2 * STATE_BYTES;
+  static constexpr uint32_t OFF_IDX = OFF_NODES + 2 * NODE_BYTES;
+  static constexpr uint32_t IDX_STRIDE = IDX_BYTES + EMAT_BYTES;
+  static constexpr uint32_t OFF_CONN = OFF_IDX + 2 * IDX_STRIDE;
+  static constexpr uint32_t OFF_ROWS = OFF_CONN + 3 * IDX_BYTES;
+  static constexpr uint32_t BYTES = OFF_ROWS + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
+};
+
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nTiles, int *err)
 {
-  constexpr int ROW = ElemShape<NPE>::ROW;
-  constexpr int EPT = TILE / NPE; // elements per tile
-  constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
-  constexpr uint32_t NODE_BYTES = 2 * TILE * sizeof(double4); // coordinates then increments
-  constexpr uint32_t IDX_BYTES = TILE * sizeof(int);
-  constexpr uint32_t EMAT_BYTES = EPT * sizeof(int);
-  static_assert(EMAT_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
-  // shared memory: state[2] | nodes[2] | (slot positions, materials)[2] | connectivity[3] | rows
-  constexpr uint32_t OFF_NODES = 2 * STATE_BYTES;
-  constexpr uint32_t OFF_IDX = OFF_NODES + 2 * NODE_BYTES;
-  constexpr uint32_t IDX_STRIDE = IDX_BYTES + EMAT_BYTES;
-  constexpr uint32_t OFF_CONN = OFF_IDX + 2 * IDX_STRIDE;
-  constexpr uint32_t OFF_ROWS = OFF_CONN + 3 * IDX_BYTES;
+  using L = StageLayout<R, NPE>;
+  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int EPT = L::EPT;
+  constexpr uint32_t STATE_BYTES = L::STATE_BYTES, NODE_BYTES = L::NODE_BYTES, IDX_BYTES = L::IDX_BYTES,
+                     EMAT_BYTES = L::EMAT_BYTES, OFF_NODES = L::OFF_NODES, OFF_IDX = L::OFF_IDX,
+                     IDX_STRIDE = L::IDX_STRIDE, OFF_CONN = L::OFF_CONN, OFF_ROWS = L::OFF_ROWS;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   auto state = [&](int b) { return reinterpret_cast<R *>(smem_raw + b * STATE_BYTES); };
-  auto nodes = [&](int b) { return reinterpret_cast<double4 *>(smem_raw + OFF_NODES + b * NODE_BYTES); };
+  // node vector k (0 coordinates, 1 increments) of buffer b: xy then z arrays
+  auto nxy = [&](int b, int k) {
+    return reinterpret_cast<double2 *>(smem_raw + OFF_NODES + b * NODE_BYTES + k * TILE * (sizeof(double2) + sizeof(double)));
+  };
+  auto nz = [&](int b, int k) { return reinterpret_cast<double *>(nxy(b, k) + TILE); };
   auto spos = [&](int b) { return reinterpret_cast<int *>(smem_raw + OFF_IDX + b * IDX_STRIDE); };
   auto emat = [&](int b) { return reinterpret_cast<int *>(smem_raw + OFF_IDX + b * IDX_STRIDE + IDX_BYTES); };
   auto conn = [&](int c) { return reinterpret_cast<int *>(smem_raw + OFF_CONN + c * IDX_BYTES); };
@@ -1138,11 +1271,10 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     const int node = conn(c)[t];
     const char *src_x = reinterpret_cast<const char *>(M.x + node);
     const char *src_u = reinterpret_cast<const char *>(M.u[M.ctl[inst].f0] + node);
-    char *dst = reinterpret_cast<char *>(nodes(b) + t);
-    cp_async16(dst, src_x);
-    cp_async16(dst + 16, src_x + 16);
-    cp_async16(dst + TILE * sizeof(double4), src_u);
-    cp_async16(dst + TILE * sizeof(double4) + 16, src_u + 16);
+    cp_async16(nxy(b, 0) + t, src_x);
+    cp_async8(nz(b, 0) + t, src_x + 16);
+    cp_async16(nxy(b, 1) + t, src_u);
+    cp_async8(nz(b, 1) + t, src_u + 16);
     cp_async_commit();
   };
   uint32_t sph = 0, cph = 0; // parity bit of each barrier
@@ -1200,7 +1332,8 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     if (act)
     {
       SharedTile<R> old{state(b), t};
-      StagedIo<R> io{M, q, nodes(b) + t, nodes(b) + TILE + t, spos(b)[t], M.mat + emat(b)[t / NPE]};
+      StagedIo<R> io{M, q, {nxy(b, 0) + t, nz(b, 0) + t}, {nxy(b, 1) + t, nz(b, 1) + t}, spos(b)[t],
+                     M.mat + emat(b)[t / NPE]};
       element_update<R, NPE>(io, C, q, e, g, base, amask, 0, old, rows + t * ROW, rows + (t - g) * ROW);
     }
     __syncthreads(); // the buffers of this tile are refilled from the next iteration on
@@ -1227,7 +1360,7 @@ template <int NPE, int MODE>
 __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles, int *err)
 {
   using R = float;
-  constexpr int ROW = ElemShape<NPE>::ROW;
+  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   __shared__ R sh[TILE * ROW];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tslot;
@@ -1342,34 +1475,54 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
 // from the element slots in element order (the order of the scatter-add of
 // Model::computeInternalForces, Model.C:881-898), then the Chung-Hulbert
 // corrector and the boundary conditions, then disp += du, coords += du.
+//
+// One thread per node.  Every load that does not depend on another is issued
+// first (CSR offsets, mass, code, coordinates, displacement, the instance's
+// control block), then the fields of the current buffer and the node's slots
+// in one batch of predicated loads, so that a thread waits on about two memory
+// latencies instead of one per step of the chain.
+constexpr int NODAL_THREADS = 128;
+#ifndef DNL_NODAL_MINB
+#define DNL_NODAL_MINB 1
+#endif
 template <typename R, int DIM>
-__global__ void __launch_bounds__(128) k_nodal(DevModel M)
+__global__ void __launch_bounds__(NODAL_THREADS, DNL_NODAL_MINB) k_nodal(DevModel M)
 {
   using R4 = typename V4<R>::type;
+  constexpr int BATCH = sizeof(R) == 4 ? 8 : 4; // slots loaded together
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= M.nN)
     return;
+  const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
+  const double m = M.mass[i];
+  const unsigned code = M.bc[i];
+  double4 X = M.x[i], D = M.disp[i];
   const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
   const Ctl *C = M.ctl + inst;
   if (!C->active)
     return;
+  const int f0 = C->f0, f1 = 1 - f0;
+  double4 v0 = M.v[f0][i], a0 = M.a[f0][i];
+  const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
+  double4 f = make_double4(0, 0, 0, 0);
+  for (int k0 = kb; k0 < ke; k0 += BATCH)
+  {
+    R4 s[BATCH];
+#pragma unroll
+    for (int j = 0; j < BATCH; j++)
+      if (k0 + j < ke)
+        s[j] = slot[k0 + j];
+#pragma unroll
+    for (int j = 0; j < BATCH; j++)
+      if (k0 + j < ke)
+      {
+        f.x += (double)s[j].x;
+        f.y += (double)s[j].y;
+        f.z += (double)s[j].z;
+      }
+  }
   const double dt = C->dt_eff, t = C->t;
   const double beta = C->beta, gam = C->gammaN, alphaM = C->alphaM;
-  const int f0 = C->f0, f1 = 1 - f0;
-  double4 f = make_double4(0, 0, 0, 0);
-  const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
-  const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
-#pragma unroll 4
-  for (int k = kb; k < ke; k++)
-  {
-    const R4 s = slot[k];
-    f.x += (double)s.x;
-    f.y += (double)s.y;
-    f.z += (double)s.z;
-  }
-  const double m = M.mass[i];
-  double4 v0 = M.v[f0][i], a0 = M.a[f0][i];
-  const unsigned code = M.bc[i];
   double4 du, v1, a1;
   du.w = v1.w = a1.w = 0.0;
 #pragma unroll
@@ -1423,7 +1576,6 @@ __global__ void __launch_bounds__(128) k_nodal(DevModel M)
     M.v[f0][i] = v0;
     M.a[f0][i] = a0;
   }
-  double4 X = M.x[i], D = M.disp[i];
   X.x += du.x;
   X.y += du.y;
   X.z += du.z;
@@ -1954,6 +2106,19 @@ __global__ void __launch_bounds__(TILE) k_power_iteration(DevModel M, int force)
     C->pi_omega = sqrt(fmx);
     C->pi_iters += it;
   }
+}
+
+// ------------------------------------------------------- state read-back
+
+// Components [c0, c0 + nc) of the point state, tile-major in R, to a
+// component-major FP64 array (the layout of dnl_engine_get_ips).
+template <typename R> __global__ void k_ips_out(DevModel M, int c0, int nc, double *dst)
+{
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (long long)nc * M.nIP)
+    return;
+  const int c = c0 + (int)(k / M.nIP), q = (int)(k % M.nIP);
+  dst[k] = (double)ipv<R>(M, c, q);
 }
 
 // -------------------------------------------------------------- energies

@@ -195,7 +195,7 @@ template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
 
 template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
 {
-  const size_t smem = 2 * (DNL_IP_NCOMP * TILE * sizeof(R) + TILE * sizeof(int)) + TILE * ElemShape<NPE>::ROW * sizeof(R);
+  const size_t smem = 2 * (DNL_IP_NCOMP * TILE * sizeof(R) + TILE * sizeof(int)) + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
   static int perSM = -1; // per instantiation
   if (perSM < 0)
   {
@@ -211,10 +211,7 @@ template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
 
 template <typename R, int NPE, int MINB> int launch_stage(dnl_engine *h)
 {
-  constexpr int EPT = TILE / NPE;
-  const size_t smem = 2 * DNL_IP_NCOMP * TILE * sizeof(R) + 2 * 2 * TILE * sizeof(double4) +
-                      2 * (TILE + EPT) * sizeof(int) + 3 * TILE * sizeof(int) +
-                      TILE * ElemShape<NPE>::ROW * sizeof(R);
+  const size_t smem = StageLayout<R, NPE>::BYTES;
   static int perSM = -1; // per instantiation
   if (perSM < 0)
   {
@@ -269,7 +266,7 @@ template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
     case 2: return launch_tma<R, NPE, 4>(h);
     case 3: return launch_tma<R, NPE, 5>(h);
     case 4: return launch_tma<R, NPE, 3>(h);
-    case 5: return launch_tma<R, NPE, 2>(h);
+    case 5: return launch_stage<R, NPE, 4>(h);
     case 6: return launch_stage<R, NPE, 3>(h);
     default: return launch_stage<R, NPE, 2>(h);
     }
@@ -327,7 +324,7 @@ int launch_element_any(dnl_engine *h, int mode)
 
 int launch_nodal(dnl_engine *h)
 {
-  const int threads = 128, blocks = (h->nN + threads - 1) / threads;
+  const int threads = NODAL_THREADS, blocks = (h->nN + threads - 1) / threads;
   if (h->precision == DNL_PREC_MIXED)
   {
     if (h->dim == 3)
@@ -1152,27 +1149,30 @@ int dnl_engine_get_ips(dnl_engine *h, double *out)
 {
   if (!h || !out)
     return DNL_ERR_ARG;
-  const size_t n = (size_t)h->nIP, total = (size_t)DNL_IP_NCOMP * h->nIPpad;
-  int rc;
-  if (h->precision == DNL_PREC_MIXED)
+  // the device reorders and widens a few components at a time into a staging
+  // array, which is copied straight into the caller's array
+  const size_t n = (size_t)h->nIP;
+  const int group = 4;
+  double *stage = nullptr;
+  CK(cudaMalloc((void **)&stage, sizeof(double) * n * group));
+  int rc = DNL_OK;
+  for (int c0 = 0; c0 < DNL_IP_NCOMP && rc == DNL_OK; c0 += group)
   {
-    std::vector<float> tmp(total);
-    if ((rc = copy(h, tmp.data(), h->M.ip, total * sizeof(float), cudaMemcpyDeviceToHost)))
-      return rc;
-    for (int c = 0; c < DNL_IP_NCOMP; c++)
-      for (size_t q = 0; q < n; q++)
-        out[c * n + q] = tmp[ip_index(c, (int)q)];
+    const int nc = std::min(group, DNL_IP_NCOMP - c0);
+    const long long items = (long long)nc * (long long)n;
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((items + threads - 1) / threads);
+    if (h->precision == DNL_PREC_MIXED)
+      k_ips_out<float><<<blocks, threads, 0, h->stream>>>(h->M, c0, nc, stage);
+    else
+      k_ips_out<double><<<blocks, threads, 0, h->stream>>>(h->M, c0, nc, stage);
+    if (cudaGetLastError() != cudaSuccess)
+      rc = fail(h, DNL_ERR_CUDA, "state read-back kernel failed");
+    else
+      rc = copy(h, out + (size_t)c0 * n, stage, sizeof(double) * n * nc, cudaMemcpyDeviceToHost);
   }
-  else
-  {
-    std::vector<double> tmp(total);
-    if ((rc = copy(h, tmp.data(), h->M.ip, total * sizeof(double), cudaMemcpyDeviceToHost)))
-      return rc;
-    for (int c = 0; c < DNL_IP_NCOMP; c++)
-      for (size_t q = 0; q < n; q++)
-        out[c * n + q] = tmp[ip_index(c, (int)q)];
-  }
-  return DNL_OK;
+  cudaFree(stage);
+  return rc;
 }
 
 int dnl_engine_set_ips(dnl_engine *h, const double *in)

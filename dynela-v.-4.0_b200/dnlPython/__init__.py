@@ -19,7 +19,8 @@ engine library or a CUDA device `solve()` raises EngineUnavailable.
 
 Scope of the mirror: the elements ElQua4NAx, ElQua4N2D and ElHex8N3D, the Johnson-Cook
 law, BoundaryRestrain / BoundarySpeed (+ DiscreteFunction / RampFunction time
-functions), the Explicit solver with the Courant and power-iteration time
+functions) and the other boundary types with the reference's behaviour on the
+explicit path (no effect, or a stop for a constant displacement or force), the Explicit solver with the Courant and power-iteration time
 steps, and HistoryFile.  SvgInterface and the VTK result files are accepted
 and skipped (the reference writes them on the host at save times).
 """
@@ -32,6 +33,8 @@ import numpy as np
 from . import _abi
 
 __all__ = ["DynELA", "NodeSet", "ElementSet", "Material", "JohnsonCookLaw", "BoundaryRestrain", "BoundarySpeed",
+           "BoundaryDisplacement", "BoundaryForce", "BoundaryAcceleration", "BoundaryTemperature",
+           "BoundaryConvection", "BoundaryFlux",
            "DiscreteFunction", "RampFunction", "Explicit", "HistoryFile", "Field", "Element", "Vec3D",
            "SvgInterface", "Parallel"]
 
@@ -247,6 +250,51 @@ class BoundarySpeed(_Boundary):
     """Imposes the non-zero speed components, optionally scaled by a time
     function (BoundarySpeed.C:139-206); as an initial condition, sets the whole
     speed vector (BoundarySpeed.C:63-73)."""
+
+
+class BoundaryDisplacement(_Boundary):
+    """Imposed displacement.  As an initial condition it does nothing
+    (BoundaryDisplacement.C:62-65); as a constant condition the reference stops
+    at the first increment with "not yet implemented"
+    (BoundaryDisplacement.C:72-76), and so does solve() here."""
+    _constant_error = "BoundaryDisplacement::applyConstantOnNewFields: not yet implemented"
+
+
+class BoundaryForce(_Boundary):
+    """Imposed nodal force.  As an initial condition it does nothing
+    (BoundaryForce.C:61-65); as a constant condition the explicit solver reaches
+    Boundary::applyConstantOnNewFields, which stops (Boundary.h:62), and so does
+    solve() here."""
+    _constant_error = "BoundaryForce: applyConstantOnNewFields is not provided (Boundary.h:62)"
+
+
+class BoundaryAcceleration(_Boundary):
+    """Imposed acceleration: accepted, with no effect as an initial or a
+    constant condition (BoundaryAcceleration.C:54-70)."""
+
+
+class BoundaryTemperature(_Boundary):
+    """Imposed temperature: accepted, with no effect as an initial or a
+    constant condition (BoundaryTemperature.C:73-93)."""
+
+    def setValue(self, temperature):
+        self.value = float(temperature)
+
+
+class BoundaryConvection(_Boundary):
+    """Convection (exchange coefficient, fluid temperature): accepted, with no
+    effect as an initial or a constant condition (BoundaryConvection.C:85-103)."""
+
+    def setValue(self, hc, Tf):
+        self.value = (float(hc), float(Tf))
+
+
+class BoundaryFlux(_Boundary):
+    """Heat flux: accepted, with no effect as an initial or a constant
+    condition (BoundaryFlux.C:73-95)."""
+
+    def setValue(self, flux):
+        self.value = float(flux)
 
 
 class Explicit:
@@ -544,6 +592,10 @@ class DynELA:
             for n in ns.numbers:
                 per_node_init[index[n]].append(b)
         for b, ns in self._constant_bcs:
+            # the explicit solver applies every constant condition of a node at
+            # each increment (Explicit.C:478,526); the types that stop there stop here
+            if getattr(b, "_constant_error", None) and len(ns.numbers):
+                raise RuntimeError(b._constant_error)
             for n in ns.numbers:
                 per_node_const[index[n]].append(b)
         for i in range(nN):

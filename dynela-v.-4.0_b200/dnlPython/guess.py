@@ -40,7 +40,13 @@ def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf, scope=_abi.GUES
         e.run(t_pause=t_pause, max_incs=max_incs, check=False)
         n = e.harvest_count()
         stats = e.newton_stats()
-    return buf[:n].clone(), stats
+    # the kernels append pairs in whatever order their atomics resolve: sort
+    # the rows (lexicographically, by stable passes from the last word) so
+    # that training on them is reproducible
+    pairs = buf[:n].clone()
+    for c in range(_abi.MLP_PAIR_WORDS - 1, -1, -1):
+        pairs = pairs[torch.sort(pairs[:, c], stable=True).indices]
+    return pairs, stats
 
 
 def initial_network(x, r, seed=1):

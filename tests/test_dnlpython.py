@@ -145,6 +145,79 @@ def test_boundary_resolution_rules():
     assert list(desc.bc_code[4]) == [0, 0, 0]
 
 
+def _one_hex(speed=True):
+    model = dnl.DynELA("bc")
+    for n in range(1, 9):
+        model.createNode(n, (n - 1) & 1, ((n - 1) >> 1) & 1, (n - 1) >> 2)
+    model.setDefaultElement(dnl.Element.ElHex8N3D)
+    model.createElement(1, 1, 2, 4, 3, 5, 6, 8, 7)
+    es = dnl.ElementSet("E")
+    model.add(es, 1)
+    m = dnl.Material("m")
+    law = dnl.JohnsonCookLaw()
+    law.setParameters(1, 1, 0, 0.5, 1, 1, 1000, 0)
+    m.setHardeningLaw(law)
+    m.youngModulus, m.poissonRatio, m.density, m.heatCapacity, m.taylorQuinney = 1e5, 0.3, 1e-8, 1e8, 0.9
+    model.add(m, es)
+    ns = dnl.NodeSet("N")
+    model.add(ns, 1, 4)
+    if speed:
+        sp = dnl.BoundarySpeed("s")
+        sp.setValue(0, 5.0, 0)
+        model.attachConstantBC(sp, ns)
+    solver = dnl.Explicit("S")
+    solver.setTimes(0, 1e-6)
+    model.add(solver)
+    return model, ns
+
+
+def _same_desc(a, b):
+    for k in ("coords", "conn", "v_init", "bc_code", "bc_value", "bc_func"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_other_boundary_types():
+    """The boundary types other than restraint and speed behave on the explicit
+    path as in the reference: acceleration, temperature, convection and flux
+    change nothing, as initial or constant conditions; displacement and force
+    change nothing as initial conditions and stop the solve as constant ones
+    (BoundaryAcceleration.C:54-70, BoundaryTemperature.C:73-93,
+    BoundaryConvection.C:85-103, BoundaryFlux.C:73-95,
+    BoundaryDisplacement.C:62-76, BoundaryForce.C:61-65, Boundary.h:62)."""
+    plain, _ = _one_hex()
+    ref = plain._description()[0]
+    acc = dnl.BoundaryAcceleration("a")
+    acc.setValue(1.0, 2.0, 3.0)
+    temp = dnl.BoundaryTemperature("t")
+    temp.setValue(500.0)
+    conv = dnl.BoundaryConvection("c")
+    conv.setValue(10.0, 300.0)
+    flux = dnl.BoundaryFlux("f")
+    flux.setValue(1e3)
+    disp = dnl.BoundaryDisplacement("d")
+    disp.setValue(0.1, 0.0, 0.0)
+    force = dnl.BoundaryForce("F")
+    force.setValue(dnl.Vec3D(0.0, 0.0, 7.0))
+    for b in (acc, temp, conv, flux):
+        for attach in ("attachConstantBC", "attachInitialBC"):
+            model, ns = _one_hex()
+            getattr(model, attach)(b, ns)
+            _same_desc(model._description()[0], ref)
+    for b in (disp, force):
+        model, ns = _one_hex()
+        model.attachInitialBC(b, ns)
+        _same_desc(model._description()[0], ref)
+        model, ns = _one_hex()
+        model.attachConstantBC(b, ns)
+        with pytest.raises(RuntimeError):
+            model._description()
+        # a condition on an empty set is never applied
+        model, _ = _one_hex()
+        empty = dnl.NodeSet("empty")
+        model.attachConstantBC(b, empty)
+        _same_desc(model._description()[0], ref)
+
+
 @pytest.mark.skipif(not os.path.isdir(SAMPLES), reason="reference samples not in this checkout")
 @pytest.mark.parametrize("sample,etype,count", [
     ("Taylor/Taylor-Axi/Taylor.py", _abi.ELQUA4NAX, 250),
