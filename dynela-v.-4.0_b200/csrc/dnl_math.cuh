@@ -187,8 +187,35 @@ template <typename R> __device__ __noinline__ void spectral_jacobi(const R A[6],
 // term:  log(1+x) = sum (-1)^(k+1) x^k / k,  (1+x)^-1/2 - 1 = sum binom(-1/2, k) x^k.
 // The series stop when |A|_F^k falls below the rounding level; returns false
 // when |A|_F is too large for a short series (the caller then uses Jacobi).
+template <typename R> struct SeriesCoef
+{
+  R log1p[64];   // term k: (-1)^(k+1) / k              (index k, entry 0 unused)
+  R invsqrt[64]; // term k: binom(-1/2, k) = (-1)^k (2k-1)!! / (2k)!!
+};
+template <typename R> __host__ __device__ constexpr SeriesCoef<R> series_coef()
+{
+  SeriesCoef<R> c{};
+  double w = 1.0;
+  for (int k = 1; k < 64; k++)
+  {
+    c.log1p[k] = R(((k & 1) ? 1.0 : -1.0) / k);
+    w *= -(2.0 * k - 1.0) / (2.0 * k);
+    c.invsqrt[k] = R(w);
+  }
+  return c;
+}
+// read with the loop counter, the same on every active lane (one broadcast load)
+static __constant__ SeriesCoef<float> c_series_f = series_coef<float>();
+static __constant__ SeriesCoef<double> c_series_d = series_coef<double>();
+
 template <typename R> __device__ __forceinline__ bool spectral_series(const R A[6], R lnU[6], R Wm[6])
 {
+  const SeriesCoef<R> &co = [] () -> const SeriesCoef<R> & {
+    if constexpr (sizeof(R) == 4)
+      return c_series_f;
+    else
+      return c_series_d;
+  }();
   const bool fp64 = sizeof(R) == 8;
   const R r = Num<R>::sqrt_(A[0] * A[0] + A[3] * A[3] + A[5] * A[5] + R(2) * (A[1] * A[1] + A[2] * A[2] + A[4] * A[4]));
   const R rmax = fp64 ? R(0.25) : R(0.35);
@@ -201,9 +228,10 @@ template <typename R> __device__ __forceinline__ bool spectral_series(const R A[
   R al = R(0), be = R(1), ga = R(0);      // A^1
   R l0 = R(0), l1 = R(0), l2 = R(0);      // log(I + A)
   R w0 = R(0), w1 = R(0), w2 = R(0);      // (I + A)^-1/2 - I
-  R cl = R(1), cw = R(-0.5), rk = r;
+  R rk = r;
   for (int k = 1; k < 64; k++)
   {
+    const R cl = co.log1p[k], cw = co.invsqrt[k];
     l0 += cl * al;
     l1 += cl * be;
     l2 += cl * ga;
@@ -216,8 +244,6 @@ template <typename R> __device__ __forceinline__ bool spectral_series(const R A[
     al = nal;
     be = nbe;
     ga = nga;
-    cl = -cl * R(k) / R(k + 1);
-    cw = -cw * R(2 * k + 1) / R(2 * k + 2);
     rk *= r;
   }
   // A^2
