@@ -2121,6 +2121,53 @@ template <typename R> __global__ void k_ips_out(DevModel M, int c0, int nc, doub
   dst[k] = (double)ipv<R>(M, c, q);
 }
 
+// --------------------------------------------------------- history items
+
+// One thread per item (DNL_ITEM_*): the selected nodal vector, point state or
+// kinetic energy copied to its place in `out` (offsets precomputed).
+// kin holds the energies of every instance (3 per instance, kinetic first)
+// on the field0 speeds, then on the field1 speeds.
+template <typename R>
+__global__ void k_gather_items(DevModel M, const int4 *items, const long long *off, int n, const double *kin,
+                               double *out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n)
+    return;
+  const int4 it = items[k];
+  double *o = out + off[k];
+  if (it.x == DNL_ITEM_POINT)
+  {
+    for (int c = 0; c < DNL_IP_NCOMP; c++)
+      o[c] = (double)ipv<R>(M, c, it.z);
+    return;
+  }
+  if (it.x == DNL_ITEM_KINETIC)
+  {
+    o[0] = kin[3 * ((it.y == DNL_NODE_SPEED_PREV ? M.nInst : 0) + it.z)];
+    return;
+  }
+  const int i = it.z;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
+  const int f0 = M.ctl[inst].f0;
+  double4 v = make_double4(0, 0, 0, 0);
+  switch (it.y)
+  {
+  case DNL_NODE_COORDS: v = M.x[i]; break;
+  case DNL_NODE_DISP: v = M.disp[i]; break;
+  case DNL_NODE_U: v = M.u[f0][i]; break;
+  case DNL_NODE_SPEED: v = M.v[f0][i]; break;
+  case DNL_NODE_ACCEL: v = M.a[f0][i]; break;
+  case DNL_NODE_SPEED_PREV: v = M.v[1 - f0][i]; break;
+  case DNL_NODE_FORCE: v = M.fout[i]; break;
+  case DNL_NODE_MASS: v.x = v.y = v.z = M.mass[i]; break;
+  default: break;
+  }
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+}
+
 // -------------------------------------------------------------- energies
 
 // One block per instance, fixed-order tree sums (deterministic).

@@ -59,6 +59,14 @@ struct dnl_engine
   int mode = DNL_MODE_PLAIN;          // element-pass mode (DNL_MODE_*)
   void *mlpImage = nullptr;           // learned-guess network image
   unsigned long long *dstats = nullptr; // Newton statistics [4] + harvest count
+  // history items (dnl_engine_set_items): list, output offsets, values
+  int nItems = 0;
+  long long nValues = 0;
+  bool itemsKinetic = false;
+  int4 *ditems = nullptr;
+  long long *ditemOff = nullptr;
+  double *dvalues = nullptr, *dkin = nullptr;
+  double *hvalues = nullptr; // pinned
   std::string err;
 };
 
@@ -805,6 +813,11 @@ int dnl_engine_create(const dnl_model_desc *desc, dnl_engine **out)
   return dnl_engine_batch_create(d, 1, out);
 }
 
+namespace
+{
+void free_items(dnl_engine *h);
+}
+
 int dnl_engine_destroy(dnl_engine *h)
 {
   if (!h)
@@ -817,6 +830,7 @@ int dnl_engine_destroy(dnl_engine *h)
     cudaGraphDestroy(h->graph);
   for (void *p : h->allocs)
     cudaFree(p);
+  free_items(h);
   if (h->hctl)
     cudaFreeHost(h->hctl);
   if (h->stream)
@@ -1195,25 +1209,137 @@ int dnl_engine_set_ips(dnl_engine *h, const double *in)
   return copy(h, h->M.ip, tmp.data(), total * sizeof(double), cudaMemcpyHostToDevice);
 }
 
-int dnl_engine_energies(dnl_engine *h, int32_t i, double out[3])
+namespace
 {
-  if (!h || !out || i < 0 || i >= h->nInst)
-    return DNL_ERR_ARG;
+int launch_energies(dnl_engine *h, double *dst, int speed_field)
+{
   if (h->precision == DNL_PREC_MIXED)
   {
     if (h->npe == 8)
-      k_energies<float, 8><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+      k_energies<float, 8><<<h->nInst, 256, 0, h->stream>>>(h->M, dst, speed_field);
     else
-      k_energies<float, 4><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+      k_energies<float, 4><<<h->nInst, 256, 0, h->stream>>>(h->M, dst, speed_field);
   }
   else
   {
     if (h->npe == 8)
-      k_energies<double, 8><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+      k_energies<double, 8><<<h->nInst, 256, 0, h->stream>>>(h->M, dst, speed_field);
     else
-      k_energies<double, 4><<<h->nInst, 256, 0, h->stream>>>(h->M, h->denergy, 0);
+      k_energies<double, 4><<<h->nInst, 256, 0, h->stream>>>(h->M, dst, speed_field);
   }
   CK(cudaGetLastError());
+  return DNL_OK;
+}
+
+void free_items(dnl_engine *h)
+{
+  for (void *p : {(void *)h->ditems, (void *)h->ditemOff, (void *)h->dvalues, (void *)h->dkin})
+    if (p)
+      cudaFree(p);
+  if (h->hvalues)
+    cudaFreeHost(h->hvalues);
+  h->ditems = nullptr;
+  h->ditemOff = nullptr;
+  h->dvalues = h->dkin = h->hvalues = nullptr;
+  h->nItems = 0;
+  h->nValues = 0;
+  h->itemsKinetic = false;
+}
+} // namespace
+
+int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_t *n_values)
+{
+  if (!h || n < 0 || (n > 0 && !items))
+    return DNL_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  free_items(h);
+  std::vector<int4> it(n);
+  std::vector<long long> off(n);
+  long long total = 0;
+  bool kin = false;
+  for (int k = 0; k < n; k++)
+  {
+    const dnl_item &a = items[k];
+    int width = 0;
+    switch (a.kind)
+    {
+    case DNL_ITEM_NODE:
+      if (a.index < 0 || a.index >= h->nN || a.field < DNL_NODE_COORDS || a.field > DNL_NODE_SPEED_PREV)
+        return fail(h, DNL_ERR_ARG, "item %d: node %d / field %d out of range", k, a.index, a.field);
+      width = 3;
+      break;
+    case DNL_ITEM_POINT:
+      if (a.index < 0 || a.index >= h->nIP)
+        return fail(h, DNL_ERR_ARG, "item %d: integration point %d out of range", k, a.index);
+      width = DNL_IP_NCOMP;
+      break;
+    case DNL_ITEM_KINETIC:
+      if (a.index < 0 || a.index >= h->nInst || (a.field != DNL_NODE_SPEED && a.field != DNL_NODE_SPEED_PREV))
+        return fail(h, DNL_ERR_ARG, "item %d: instance %d / speed field %d invalid", k, a.index, a.field);
+      width = 1;
+      kin = true;
+      break;
+    default:
+      return fail(h, DNL_ERR_ARG, "item %d: unknown kind %d", k, a.kind);
+    }
+    it[k] = make_int4(a.kind, a.field, a.index, 0);
+    off[k] = total;
+    total += width;
+  }
+  if (n > 0)
+  {
+    CK(cudaMalloc((void **)&h->ditems, sizeof(int4) * n));
+    CK(cudaMalloc((void **)&h->ditemOff, sizeof(long long) * n));
+    CK(cudaMalloc((void **)&h->dvalues, sizeof(double) * total));
+    CK(cudaMalloc((void **)&h->dkin, sizeof(double) * 6 * h->nInst));
+    CK(cudaMallocHost((void **)&h->hvalues, sizeof(double) * total));
+    CK(cudaMemcpyAsync(h->ditems, it.data(), sizeof(int4) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->ditemOff, off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  h->nItems = n;
+  h->nValues = total;
+  h->itemsKinetic = kin;
+  if (n_values)
+    *n_values = total;
+  return DNL_OK;
+}
+
+int dnl_engine_gather_items(dnl_engine *h, double *out)
+{
+  if (!h || (h->nItems > 0 && !out))
+    return DNL_ERR_ARG;
+  if (h->nItems == 0)
+    return DNL_OK;
+  int rc;
+  if (h->itemsKinetic)
+  {
+    // energies of every instance on both speed fields: field0 then field1
+    for (int f = 0; f < 2; f++)
+      if ((rc = launch_energies(h, h->dkin + 3 * f * h->nInst, f)))
+        return rc;
+  }
+  const int threads = 128, blocks = (h->nItems + threads - 1) / threads;
+  if (h->precision == DNL_PREC_MIXED)
+    k_gather_items<float><<<blocks, threads, 0, h->stream>>>(h->M, h->ditems, h->ditemOff, h->nItems, h->dkin,
+                                                                h->dvalues);
+  else
+    k_gather_items<double><<<blocks, threads, 0, h->stream>>>(h->M, h->ditems, h->ditemOff, h->nItems, h->dkin,
+                                                                 h->dvalues);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->hvalues, h->dvalues, sizeof(double) * h->nValues, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  memcpy(out, h->hvalues, sizeof(double) * h->nValues);
+  return DNL_OK;
+}
+
+int dnl_engine_energies(dnl_engine *h, int32_t i, double out[3])
+{
+  if (!h || !out || i < 0 || i >= h->nInst)
+    return DNL_ERR_ARG;
+  int rc = launch_energies(h, h->denergy, 0);
+  if (rc)
+    return rc;
   CK(cudaMemcpyAsync(out, h->denergy + 3 * i, 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return DNL_OK;

@@ -639,6 +639,7 @@ class DynELA:
             h._f = open(h.fileName, "w")
             h._f.write("#DynELA FEM Code v. 4.0 history file\n#plotted :" + "".join(it[0] + " " for it in h.items)
                        + "\n")
+        self._plan_items()
         self._write_histories(initial=True)
         t_end = desc.t_end
         while True:
@@ -671,10 +672,56 @@ class DynELA:
             self._cache[field] = self._engine.nodes(field)
         return self._cache[field]
 
-    def _ips(self):
-        if "ips" not in self._cache:
-            self._cache["ips"] = self._engine.ips()
-        return self._cache["ips"]
+    # ---- history items: selected on the device, one gather per save time
+    _NODE_FIELDS = (("coords", _abi.NODE_COORDS), ("dispInc", _abi.NODE_U), ("disp", _abi.NODE_DISP),
+                    ("speedInc", _abi.NODE_ACCEL), ("speed", _abi.NODE_SPEED))
+
+    @classmethod
+    def _node_item(cls, field):
+        """(nodal field, component suffix) of a node history field."""
+        name = Field._names[field]
+        for base, f in cls._NODE_FIELDS:
+            if name.startswith(base) and name[len(base):] in ("X", "Y", "Z", ""):
+                return f, name[len(base):]
+        if name == "mass":
+            return _abi.NODE_MASS, "X"
+        raise NotImplementedError(f"node field {name}")
+
+    def _item_keys(self, kind, target, ip, field):
+        if kind == "global":
+            if field == Field.kineticEnergy:
+                return [(_abi.ITEM_KINETIC, _abi.NODE_SPEED, 0), (_abi.ITEM_KINETIC, _abi.NODE_SPEED_PREV, 0)]
+            return []
+        if kind == "node":
+            return [(_abi.ITEM_NODE, self._node_item(field)[0], self._node_index[target])]
+        e = self._elem_index[target]
+        qs = range(e * self._npe, (e + 1) * self._npe) if ip < 0 else [e * self._npe + ip]
+        return [(_abi.ITEM_POINT, 0, q) for q in qs]
+
+    def _plan_items(self):
+        """The engine items every history file needs (HistoryFile::save reads,
+        HistoryFile.C:289-317), registered once; a save time then copies only
+        their values from the device."""
+        keys = []
+        for h in self._histories:
+            for _, kind, target, ip, field in h.items:
+                for k in self._item_keys(kind, target, ip, field):
+                    if k not in keys:
+                        keys.append(k)
+        self._item_list = keys
+        self._item_off = {}
+        off = 0
+        for k in keys:
+            self._item_off[k] = off
+            off += _abi.ITEM_WIDTH[k[0]]
+        if keys:
+            self._engine.set_items(keys)
+
+    def _gathered(self, key):
+        if "items" not in self._cache:
+            self._cache["items"] = self._engine.gather_items()
+        o = self._item_off[key]
+        return self._cache["items"][o:o + _abi.ITEM_WIDTH[key[0]]]
 
     def _item_value(self, kind, target, ip, field):
         eng = self._engine
@@ -684,26 +731,15 @@ class DynELA:
                 return c["last_time_step"]
             if field == Field.kineticEnergy:
                 # Model::getTotalKineticEnergy on field0, written before the swap (Explicit.C:539-552)
-                v = self._node_field(_abi.NODE_SPEED_PREV if c["increment"] > 0 else _abi.NODE_SPEED)
-                m = self._node_field(_abi.NODE_MASS)[:, 0]
-                return float(np.sum(m * (v * v).sum(1) / 2.0))
+                f = _abi.NODE_SPEED_PREV if c["increment"] > 0 else _abi.NODE_SPEED
+                return float(self._gathered((_abi.ITEM_KINETIC, f, 0))[0])
             return 0.0
         if kind == "node":
-            i = self._node_index[target]
-            name = Field._names[field]
-            for base, f in (("coords", _abi.NODE_COORDS), ("dispInc", _abi.NODE_U), ("disp", _abi.NODE_DISP),
-                            ("speedInc", _abi.NODE_ACCEL), ("speed", _abi.NODE_SPEED)):
-                if name.startswith(base) and name[len(base):] in ("X", "Y", "Z", ""):
-                    row = self._node_field(f)[i]
-                    suf = name[len(base):]
-                    return float(np.linalg.norm(row)) if suf == "" else float(row["XYZ".index(suf)])
-            if name == "mass":
-                return float(self._node_field(_abi.NODE_MASS)[i, 0])
-            raise NotImplementedError(f"node field {name}")
-        e = self._elem_index[target]
-        ips = self._ips()
-        q = np.arange(e * self._npe, (e + 1) * self._npe) if ip < 0 else np.array([e * self._npe + ip])
-        return float(np.mean([self._ip_value(ips[:, k], field) for k in q]))
+            f, suf = self._node_item(field)
+            row = self._gathered((_abi.ITEM_NODE, f, self._node_index[target]))
+            return float(np.linalg.norm(row)) if suf == "" else float(row["XYZ".index(suf)])
+        return float(np.mean([self._ip_value(self._gathered(k), field)
+                              for k in self._item_keys(kind, target, ip, field)]))
 
     @staticmethod
     def _ip_value(s, field):

@@ -98,6 +98,16 @@ class ModelDescC(ctypes.Structure):
     ]
 
 
+ITEM_NODE, ITEM_POINT, ITEM_KINETIC = range(3)
+ITEM_WIDTH = {ITEM_NODE: 3, ITEM_POINT: IP_NCOMP, ITEM_KINETIC: 1}
+
+
+class Item(ctypes.Structure):
+    """dnl_item: one history item (kind DNL_ITEM_*, field, index)."""
+    _fields_ = [("kind", ctypes.c_int32), ("field", ctypes.c_int32), ("index", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 class Control(ctypes.Structure):
     _fields_ = [("time", ctypes.c_double), ("time_step", ctypes.c_double), ("t_end", ctypes.c_double),
                 ("increment", ctypes.c_int64), ("status", ctypes.c_int32), ("bad_index", ctypes.c_int32),
@@ -272,6 +282,8 @@ def load_library():
         "dnl_engine_get_ips": (ctypes.c_int, [vp, pd]),
         "dnl_engine_set_ips": (ctypes.c_int, [vp, pd]),
         "dnl_engine_energies": (ctypes.c_int, [vp, i32, pd]),
+        "dnl_engine_set_items": (ctypes.c_int, [vp, ctypes.POINTER(Item), i32, ctypes.POINTER(i64)]),
+        "dnl_engine_gather_items": (ctypes.c_int, [vp, pd]),
         "dnl_engine_set_timing": (ctypes.c_int, [vp, i32]),
         "dnl_engine_timings": (ctypes.c_int, [vp, pd]),
         "dnl_engine_launch_count": (ctypes.c_int64, [vp]),

@@ -98,6 +98,22 @@ class Engine:
         a = np.ascontiguousarray(values, dtype=np.float64).reshape(_abi.IP_NCOMP, self.n_ips)
         self._check(self._lib.dnl_engine_set_ips(self.h, _pd(a)))
 
+    def set_items(self, items):
+        """Select the history items gathered by gather_items(): a list of
+        (kind, field, index) with kind ITEM_NODE / ITEM_POINT / ITEM_KINETIC."""
+        arr = (_abi.Item * max(1, len(items)))(*[_abi.Item(int(k), int(f), int(i), 0) for k, f, i in items])
+        n = ctypes.c_int64()
+        self._check(self._lib.dnl_engine_set_items(self.h, arr, len(items), ctypes.byref(n)))
+        self._n_values = n.value
+        return n.value
+
+    def gather_items(self):
+        """The selected items' values, item after item (3 doubles for a node,
+        IP_NCOMP for a point, 1 for a kinetic energy)."""
+        out = np.zeros(max(1, getattr(self, "_n_values", 0)))
+        self._check(self._lib.dnl_engine_gather_items(self.h, _pd(out)))
+        return out[:getattr(self, "_n_values", 0)]
+
     def energies(self, instance=0):
         out = np.zeros(3)
         self._check(self._lib.dnl_engine_energies(self.h, int(instance), _pd(out)))

@@ -207,6 +207,32 @@ int dnl_engine_set_nodes(dnl_engine *h, int32_t field, const double *in);
 int dnl_engine_get_ips(dnl_engine *h, double *out);
 int dnl_engine_set_ips(dnl_engine *h, const double *in);
 
+/* History items (replaces the per-save reads of HistoryFile::save,
+ * HistoryFile.C:289-317, and of the Field extraction it calls,
+ * Element.C:1195-1240, Model.C:612-626): the values a history file needs at a
+ * save time are selected on the device and only they cross to the host.
+ * An item is one of
+ *   DNL_ITEM_NODE     3 doubles: nodal field `field` (DNL_NODE_*) of node `index`
+ *   DNL_ITEM_POINT    DNL_IP_NCOMP doubles: the state of integration point `index`
+ *   DNL_ITEM_KINETIC  1 double: kinetic energy of instance `index` on speed
+ *                     field `field` (DNL_NODE_SPEED or DNL_NODE_SPEED_PREV),
+ *                     fixed-order FP64 sum of m |v|^2 / 2.
+ * dnl_engine_set_items checks and uploads the list (replacing a previous one)
+ * and returns the number of doubles one gather writes; dnl_engine_gather_items
+ * writes them, item after item in list order, to `out`. */
+enum
+{
+  DNL_ITEM_NODE = 0,
+  DNL_ITEM_POINT = 1,
+  DNL_ITEM_KINETIC = 2
+};
+typedef struct
+{
+  int32_t kind, field, index, reserved;
+} dnl_item;
+int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_t *n_values);
+int dnl_engine_gather_items(dnl_engine *h, double *out);
+
 /* Energies of one instance, FP64 sums: [0] kinetic (Model.C:612-626, field0
  * speeds), [1] internal = sum rho0*detJ0*w*e_int (x 2 pi for axisymmetric),
  * [2] inelastic (plastic work), same weights. */

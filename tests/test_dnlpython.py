@@ -289,6 +289,22 @@ class OracleEngine:
     def ips(self):
         return self.o.ips()
 
+    def set_items(self, items):
+        self.items = list(items)
+
+    def gather_items(self):
+        """The engine's item gather restated from the full arrays."""
+        out = []
+        for kind, field, index in self.items:
+            if kind == _abi.ITEM_NODE:
+                out.extend(self.o.nodes(field)[index])
+            elif kind == _abi.ITEM_POINT:
+                out.extend(self.o.ips()[:, index])
+            else:
+                v, m = self.o.nodes(field), self.o.nodes(_abi.NODE_MASS)[:, 0]
+                out.append(float(np.sum(m * (v * v).sum(1) / 2.0)))
+        return np.array(out)
+
 
 def read_history(path):
     with open(path) as f:

@@ -174,6 +174,45 @@ def test_batched_instances_match_single_runs():
             assert cb["increment"] == c["increment"] and cb["time"] == c["time"]
 
 
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_history_items_equal_full_reads(precision):
+    """dnl_engine_gather_items returns, item after item, exactly what the full
+    reads of the nodal fields and the point state hold, and the kinetic
+    energy of both speed fields; a batch's instances are kept apart."""
+    descs = [helpers.case_hex_small(precision), helpers.case_hex_small(precision).copy(t_end=3e-6)]
+    with engine(descs) as e:
+        e.init()
+        e.run(max_incs=25)
+        n1, _, q1 = e.offsets(1)
+        fields = (_abi.NODE_COORDS, _abi.NODE_DISP, _abi.NODE_U, _abi.NODE_SPEED, _abi.NODE_ACCEL,
+                  _abi.NODE_MASS, _abi.NODE_SPEED_PREV)
+        items = [(_abi.ITEM_NODE, f, i) for f in fields for i in (0, 3, n1, e.n_nodes - 1)]
+        items += [(_abi.ITEM_POINT, 0, q) for q in (0, 7, q1 + 2, e.n_ips - 1)]
+        items += [(_abi.ITEM_KINETIC, f, k) for f in (_abi.NODE_SPEED, _abi.NODE_SPEED_PREV) for k in (0, 1)]
+        n = e.set_items(items)
+        assert n == sum(_abi.ITEM_WIDTH[k] for k, _, _ in items)
+        got = e.gather_items()
+        ips = e.ips()
+        want = []
+        for kind, f, i in items:
+            if kind == _abi.ITEM_NODE:
+                want.extend(e.nodes(f)[i])
+            elif kind == _abi.ITEM_POINT:
+                want.extend(ips[:, i])
+            else:
+                n0, _, _ = e.offsets(i)
+                n_end = e.offsets(i + 1)[0] if i + 1 < e.n_instances else e.n_nodes
+                v, m = e.nodes(f)[n0:n_end], e.nodes(_abi.NODE_MASS)[n0:n_end, 0]
+                want.append(np.sum(m * (v * v).sum(1) / 2.0))
+        want = np.array(want)
+        nk = 4
+        assert np.array_equal(got[:-nk], want[:-nk])
+        assert np.allclose(got[-nk:], want[-nk:], rtol=1e-13, atol=0)
+        assert got[-nk] > 0
+        with pytest.raises(_abi.EngineError):
+            e.set_items([(_abi.ITEM_POINT, 0, e.n_ips)])
+
+
 def test_runs_are_deterministic():
     d = helpers.case_hex_small(_abi.PREC_MIXED)
     out = []
