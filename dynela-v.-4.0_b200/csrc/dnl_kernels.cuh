@@ -92,6 +92,12 @@ struct DevModel
   int harvest_stride;
   int guess_scope;         // DNL_GUESS_ALL or DNL_GUESS_FIRST_YIELD
   unsigned *done_count;    // blocks of the fused Courant + end-of-increment kernel that have finished
+  unsigned *step_due;      // set by the nodal pass: the Courant pass of this increment has work
+  // batches: the instances that run this increment, in index order, and the
+  // prefix sums of their point tiles, nodes and elements (k_active_list)
+  int *act_count;          // [1]
+  int *act_list;           // [nInst]
+  int *act_tile_pre, *act_node_pre, *act_elem_pre; // [nInst + 1]
 };
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
@@ -975,28 +981,158 @@ __global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
   reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = s;
 }
 
+// ------------------------------------------------------ batch work lists
+
+// Tiles of TILE points that hold points of instance c's elements (the first
+// and last may be shared with the neighbouring instances).
+__device__ __forceinline__ int instance_tiles(const Ctl &c, int npe)
+{
+  return (c.elem_end * npe + TILE - 1) / TILE - (c.elem_begin * npe) / TILE;
+}
+
+// One block: the list of the instances that run this increment and the
+// prefix sums of their tiles, nodes and elements, so that the passes of a
+// batch spread only the running instances' work over the GPU (a batch ends
+// with a few long-running instances among hundreds that have stopped).
+__global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
+{
+  __shared__ int wsum[4][32];
+  __shared__ int carry[4];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  if (t < 4)
+    carry[t] = 0;
+  __syncthreads();
+  for (int base = 0; base < M.nInst; base += 1024)
+  {
+    const int i = base + t;
+    int v[4] = {0, 0, 0, 0}; // running, tiles, nodes, elements
+    if (i < M.nInst)
+    {
+      const Ctl &c = M.ctl[i];
+      if (c.active)
+      {
+        v[0] = 1;
+        v[1] = instance_tiles(c, npe);
+        v[2] = c.node_end - c.node_begin;
+        v[3] = c.elem_end - c.elem_begin;
+      }
+    }
+    int inc[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+    {
+      inc[k] = v[k];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const int y = __shfl_up_sync(0xffffffffu, inc[k], o);
+        if (lane >= o)
+          inc[k] += y;
+      }
+      if (lane == 31)
+        wsum[k][w] = inc[k];
+    }
+    __syncthreads();
+    if (w == 0)
+    {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+      {
+        int x = wsum[k][lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+          const int y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o)
+            x += y;
+        }
+        wsum[k][lane] = x; // inclusive over the warps
+      }
+    }
+    __syncthreads();
+    int ex[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      ex[k] = carry[k] + inc[k] - v[k] + (w > 0 ? wsum[k][w - 1] : 0);
+    if (v[0])
+    {
+      M.act_list[ex[0]] = i;
+      M.act_tile_pre[ex[0]] = ex[1];
+      M.act_node_pre[ex[0]] = ex[2];
+      M.act_elem_pre[ex[0]] = ex[3];
+    }
+    __syncthreads();
+    if (t < 4)
+      carry[t] += wsum[t][31];
+    __syncthreads();
+  }
+  if (t == 0)
+  {
+    *M.act_count = carry[0];
+    M.act_tile_pre[carry[0]] = carry[1];
+    M.act_node_pre[carry[0]] = carry[2];
+    M.act_elem_pre[carry[0]] = carry[3];
+  }
+}
+
+// Work slots of the element pass.  A single model: one slot per tile while it
+// runs.  A batch: the tiles of the running instances (k_active_list); a tile
+// shared by two running instances is a slot of each, and each pass updates
+// only its own instance's elements (their points and slots are disjoint).
+template <int NPE> struct TileMap
+{
+  const DevModel &M;
+  int nTiles;
+  __device__ __forceinline__ int count() const
+  {
+    if (M.nInst == 1)
+      return M.ctl[0].active ? nTiles : 0;
+    return M.act_tile_pre[*M.act_count];
+  }
+  __device__ __forceinline__ void get(int slot, int &tile, int &inst) const
+  {
+    if (M.nInst == 1)
+    {
+      tile = slot;
+      inst = 0;
+      return;
+    }
+    const int a = find_segment(M.act_tile_pre, *M.act_count, slot);
+    inst = M.act_list[a];
+    tile = (M.ctl[inst].elem_begin * NPE) / TILE + (slot - M.act_tile_pre[a]);
+  }
+};
+
 // Element pass, one thread per Gauss point, state read straight from global memory.
+// A block takes the work slots (TileMap) blockIdx.x, + gridDim.x, ...
 template <typename R, int NPE, int MINB>
-__global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M)
+__global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M, int nTiles)
 {
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   __shared__ R sh[TILE * ROW];
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int g = lane & (NPE - 1);
   const int base = lane & ~(NPE - 1);
-  const int e = q / NPE;
-  const bool valid = e < M.nE;
-  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
-  Ctl *C = M.ctl + inst;
-  const bool act = valid && C->active;
-  const unsigned amask = __ballot_sync(0xffffffffu, act);
-  if (!act)
-    return;
-  GlobalState<R> old{M, q};
-  EngineIo<R> io{M, q, C->f0};
-  element_update<R, NPE>(io, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
-                         sh + (threadIdx.x - g) * ROW);
+  const TileMap<NPE> map{M, nTiles};
+  const int nSlots = map.count();
+  for (int slot = blockIdx.x; slot < nSlots; slot += gridDim.x)
+  {
+    int tile, inst;
+    map.get(slot, tile, inst);
+    const int q = tile * TILE + threadIdx.x;
+    const int e = q / NPE;
+    Ctl *C = M.ctl + inst;
+    const bool act = e >= C->elem_begin && e < C->elem_end && C->active;
+    const unsigned amask = __ballot_sync(0xffffffffu, act);
+    if (act)
+    {
+      GlobalState<R> old{M, q};
+      EngineIo<R> io{M, q, C->f0};
+      element_update<R, NPE>(io, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
+                             sh + (threadIdx.x - g) * ROW);
+    }
+    __syncwarp();
+  }
 }
 
 // ----------------------------------------------- bulk-copy (TMA) primitives
@@ -1080,33 +1216,24 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
     bulk_g2s(state[b], reinterpret_cast<const R *>(M.ip) + (size_t)tile * DNL_IP_NCOMP * TILE, STATE_BYTES, &bar[b]);
     bulk_g2s(conn[b], M.conn + (size_t)tile * TILE, CONN_BYTES, &bar[b]);
   };
-  // Tiles whose instances have all stopped are neither copied nor computed.
-  // The active flags do not change during the pass, so every thread of the
-  // block walks the same sequence of tiles.
-  auto live = [&](int tl) {
-    if (M.nInst == 1)
-      return M.ctl[0].active != 0;
-    const int e0 = tl * (TILE / NPE), e1 = min(M.nE - 1, e0 + TILE / NPE - 1);
-    const int i1 = find_segment(M.inst_elem_begin, M.nInst, e1);
-    for (int i = find_segment(M.inst_elem_begin, M.nInst, e0); i <= i1; i++)
-      if (M.ctl[i].active)
-        return true;
-    return false;
-  };
-  auto next_live = [&](int tl) {
-    while (tl < nTiles && !live(tl))
-      tl += gridDim.x;
-    return tl;
-  };
-  int tile = next_live(blockIdx.x);
-  if (t == 0 && tile < nTiles)
+  // Work slots (TileMap): the tiles of the running instances only.  The
+  // running set does not change during the pass, so every thread of the
+  // block walks the same sequence.
+  const TileMap<NPE> map{M, nTiles};
+  const int nSlots = map.count();
+  int slot = blockIdx.x, tile = 0, inst = 0, ntile = 0, ninst = 0;
+  if (slot < nSlots)
+    map.get(slot, tile, inst);
+  if (t == 0 && slot < nSlots)
     issue(tile, 0);
   uint32_t phase[2] = {0, 0};
-  for (int b = 0, next; tile < nTiles; tile = next, b ^= 1)
+  for (int b = 0; slot < nSlots; slot += gridDim.x, tile = ntile, inst = ninst, b ^= 1)
   {
-    next = next_live(tile + gridDim.x);
-    if (t == 0 && next < nTiles)
-      issue(next, b ^ 1);
+    const bool more = slot + (int)gridDim.x < nSlots;
+    if (more)
+      map.get(slot + gridDim.x, ntile, ninst);
+    if (t == 0 && more)
+      issue(ntile, b ^ 1);
     if (!mbar_wait(&bar[b], phase[b]))
     {
       atomicExch(err, 1);
@@ -1116,10 +1243,8 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
     phase[b] ^= 1;
     const int q = tile * TILE + t;
     const int e = q / NPE;
-    const bool valid = e < M.nE;
-    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
     Ctl *C = M.ctl + inst;
-    const bool act = valid && C->active;
+    const bool act = e >= C->elem_begin && e < C->elem_end && C->active;
     const unsigned amask = __ballot_sync(0xffffffffu, act);
     if (act)
     {
@@ -1236,21 +1361,6 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  auto live = [&](int tl) {
-    if (M.nInst == 1)
-      return M.ctl[0].active != 0;
-    const int e0 = tl * EPT, e1 = min(M.nE - 1, e0 + EPT - 1);
-    const int i1 = find_segment(M.inst_elem_begin, M.nInst, e1);
-    for (int i = find_segment(M.inst_elem_begin, M.nInst, e0); i <= i1; i++)
-      if (M.ctl[i].active)
-        return true;
-    return false;
-  };
-  auto next_live = [&](int tl) {
-    while (tl < nTiles && !live(tl))
-      tl += gridDim.x;
-    return tl;
-  };
   auto issue_state = [&](int tl, int b) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&sbar[b], STATE_BYTES + IDX_BYTES + EMAT_BYTES);
@@ -1263,11 +1373,9 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     mbar_expect_tx(&cbar[c], IDX_BYTES);
     bulk_g2s(conn(c), M.conn + (size_t)tl * TILE, IDX_BYTES, &cbar[c]);
   };
-  // this lane's node of a tile: coordinates and increment of field0 of its instance
-  auto gather = [&](int tl, int c, int b) {
-    const int q = tl * TILE + t;
-    const int e = min(q / NPE, M.nE - 1);
-    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, e) : 0;
+  // this lane's node of a tile: coordinates and increment of field0 of the
+  // slot's instance
+  auto gather = [&](int inst, int c, int b) {
     const int node = conn(c)[t];
     const char *src_x = reinterpret_cast<const char *>(M.x + node);
     const char *src_u = reinterpret_cast<const char *>(M.u[M.ctl[inst].f0] + node);
@@ -1288,46 +1396,58 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     bits ^= 1u << k;
   };
 
-  int tile = next_live(blockIdx.x);
-  int next = tile < nTiles ? next_live(tile + gridDim.x) : nTiles;
-  if (t == 0 && tile < nTiles)
+  // work slots (TileMap): this block's slots blockIdx.x, + gridDim.x, ...,
+  // each a (tile, instance); cur, next and after are three consecutive ones
+  const TileMap<NPE> map{M, nTiles};
+  const int nSlots = map.count();
+  struct Work
   {
-    issue_conn(tile, 0);
-    issue_state(tile, 0);
-    if (next < nTiles)
-      issue_conn(next, 1);
+    int slot, tile, inst;
+  };
+  auto work = [&](int slot) {
+    Work w{slot, 0, 0};
+    if (slot < nSlots)
+      map.get(slot, w.tile, w.inst);
+    return w;
+  };
+  Work cur = work(blockIdx.x);
+  Work next = work(cur.slot + gridDim.x);
+  if (t == 0 && cur.slot < nSlots)
+  {
+    issue_conn(cur.tile, 0);
+    issue_state(cur.tile, 0);
+    if (next.slot < nSlots)
+      issue_conn(next.tile, 1);
   }
-  if (tile < nTiles)
+  if (cur.slot < nSlots)
   {
     wait_bar(&cbar[0], cph, 0);
-    gather(tile, 0, 0);
+    gather(cur.inst, 0, 0);
   }
-  for (int b = 0, c = 0; tile < nTiles; b ^= 1, c = (c == 2 ? 0 : c + 1))
+  for (int b = 0, c = 0; cur.slot < nSlots; b ^= 1, c = (c == 2 ? 0 : c + 1))
   {
-    const int after = next < nTiles ? next_live(next + gridDim.x) : nTiles;
+    const Work after = work(next.slot + gridDim.x);
     const int c1 = (c == 2 ? 0 : c + 1), c2 = (c1 == 2 ? 0 : c1 + 1);
     if (t == 0)
     {
-      if (next < nTiles)
-        issue_state(next, b ^ 1);
-      if (after < nTiles)
-        issue_conn(after, c2);
+      if (next.slot < nSlots)
+        issue_state(next.tile, b ^ 1);
+      if (after.slot < nSlots)
+        issue_conn(after.tile, c2);
     }
-    if (next < nTiles)
+    if (next.slot < nSlots)
     {
       wait_bar(&cbar[c1], cph, c1);
-      gather(next, c1, b ^ 1);
+      gather(next.inst, c1, b ^ 1);
       cp_async_wait<1>(); // this tile's nodes (all but the group just issued)
     }
     else
       cp_async_wait<0>();
     wait_bar(&sbar[b], sph, b);
-    const int q = tile * TILE + t;
+    const int q = cur.tile * TILE + t;
     const int e = q / NPE;
-    const bool valid = e < M.nE;
-    const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, valid ? e : M.nE - 1) : 0;
-    Ctl *C = M.ctl + inst;
-    const bool act = valid && C->active && !failed;
+    Ctl *C = M.ctl + cur.inst;
+    const bool act = e >= C->elem_begin && e < C->elem_end && C->active && !failed;
     const unsigned amask = __ballot_sync(0xffffffffu, act);
     if (act)
     {
@@ -1337,7 +1457,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
       element_update<R, NPE>(io, C, q, e, g, base, amask, 0, old, rows + t * ROW, rows + (t - g) * ROW);
     }
     __syncthreads(); // the buffers of this tile are refilled from the next iteration on
-    tile = next;
+    cur = next;
     next = after;
   }
   cp_async_wait<0>();
@@ -1476,117 +1596,122 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
 // Model::computeInternalForces, Model.C:881-898), then the Chung-Hulbert
 // corrector and the boundary conditions, then disp += du, coords += du.
 //
-// One thread per node.  Every load that does not depend on another is issued
-// first (CSR offsets, mass, code, coordinates, displacement, the instance's
-// control block), then the fields of the current buffer and the node's slots
-// in one batch of predicated loads, so that a thread waits on about two memory
-// latencies instead of one per step of the chain.
+// One thread per (node, component): the three components of the update are
+// independent (the corrector, the boundary conditions and the nodal vectors
+// all act component-wise), so a thread needs few registers and the pass runs
+// at full occupancy, which is what hides the latency of its gather.  The
+// component's force is still summed over the node's slots in element order.
 constexpr int NODAL_THREADS = 128;
-#ifndef DNL_NODAL_MINB
-#define DNL_NODAL_MINB 1
-#endif
 template <typename R, int DIM>
-__global__ void __launch_bounds__(NODAL_THREADS, DNL_NODAL_MINB) k_nodal(DevModel M)
+__device__ __forceinline__ void nodal_update(const DevModel &M, int i, int c, const Ctl *C)
 {
-  using R4 = typename V4<R>::type;
-  constexpr int BATCH = sizeof(R) == 4 ? 8 : 4; // slots loaded together
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= M.nN)
-    return;
+  constexpr int BATCH = 8; // slots loaded together
   const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
   const double m = M.mass[i];
-  const unsigned code = M.bc[i];
-  double4 X = M.x[i], D = M.disp[i];
-  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
-  const Ctl *C = M.ctl + inst;
+  const unsigned code = (M.bc[i] >> (2 * c)) & 3u;
+  const double X = reinterpret_cast<const double *>(M.x + i)[c];
+  const double D = reinterpret_cast<const double *>(M.disp + i)[c];
   if (!C->active)
     return;
   const int f0 = C->f0, f1 = 1 - f0;
-  double4 v0 = M.v[f0][i], a0 = M.a[f0][i];
-  const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
-  double4 f = make_double4(0, 0, 0, 0);
+  double v0 = reinterpret_cast<const double *>(M.v[f0] + i)[c];
+  double a0 = reinterpret_cast<const double *>(M.a[f0] + i)[c];
+  // this component of the node's slots (4 values per slot)
+  const R *sc = reinterpret_cast<const R *>(M.slot) + c;
+  double f = 0.0;
   for (int k0 = kb; k0 < ke; k0 += BATCH)
   {
-    R4 s[BATCH];
+    R s[BATCH];
 #pragma unroll
     for (int j = 0; j < BATCH; j++)
       if (k0 + j < ke)
-        s[j] = slot[k0 + j];
+        s[j] = sc[4 * (k0 + j)];
 #pragma unroll
     for (int j = 0; j < BATCH; j++)
       if (k0 + j < ke)
-      {
-        f.x += (double)s[j].x;
-        f.y += (double)s[j].y;
-        f.z += (double)s[j].z;
-      }
+        f += (double)s[j];
   }
   const double dt = C->dt_eff, t = C->t;
   const double beta = C->beta, gam = C->gammaN, alphaM = C->alphaM;
-  double4 du, v1, a1;
-  du.w = v1.w = a1.w = 0.0;
-#pragma unroll
-  for (int c = 0; c < 3; c++)
+  double du = dt * (v0 + (0.5 - beta) * dt * a0);
+  double v1 = v0 + (1.0 - gam) * dt * a0;
+  double a1 = (c < DIM) ? f / m : 0.0;
+  a1 = (a1 - alphaM * a0) / (1.0 - alphaM);
+  v1 += gam * dt * a1;
+  du += beta * (dt * dt) * a1;
+  // the z thread also writes the (zero) fourth word, so that every 32-byte
+  // sector of the node vectors is written whole (a partly written sector
+  // costs a read of it from DRAM when it leaves the L2)
+  auto put = [&](double4 *v, double val) {
+    if (c == 2)
+      reinterpret_cast<double2 *>(v)[1] = make_double2(val, 0.0);
+    else
+      reinterpret_cast<double *>(v)[c] = val;
+  };
+  if (code == DNL_BC_RESTRAIN)
   {
-    const double vc = comp(v0, c), ac = comp(a0, c);
-    double u_ = dt * (vc + (0.5 - beta) * dt * ac);
-    double v_ = vc + (1.0 - gam) * dt * ac;
-    double a_ = (c < DIM) ? comp(f, c) / m : 0.0;
-    a_ = (a_ - alphaM * ac) / (1.0 - alphaM);
-    v_ += gam * dt * a_;
-    u_ += beta * (dt * dt) * a_;
-    comp(du, c) = u_;
-    comp(v1, c) = v_;
-    comp(a1, c) = a_;
+    // BoundaryRestrain.C:98-128 (both fields)
+    du = v1 = a1 = 0.0;
+    put(M.u[f0] + i, 0.0);
+    put(M.v[f0] + i, 0.0);
+    put(M.a[f0] + i, 0.0);
   }
-  if (code)
+  else if (code == DNL_BC_SPEED)
   {
-    // BoundaryRestrain.C:98-128, BoundarySpeed.C:139-206 (both fields)
-    double4 u0 = M.u[f0][i];
-    for (int c = 0; c < 3; c++)
+    // BoundarySpeed.C:139-206 (both fields)
+    const double sv = reinterpret_cast<const double *>(M.bcval + i)[c];
+    const int fn = reinterpret_cast<const int *>(M.bcfun + i)[c];
+    double va = sv, vb = sv, acc = 0.0;
+    if (fn >= 0)
     {
-      const unsigned cc = (code >> (2 * c)) & 3u;
-      if (cc == DNL_BC_RESTRAIN)
-      {
-        comp(du, c) = comp(v1, c) = comp(a1, c) = 0.0;
-        comp(u0, c) = comp(v0, c) = comp(a0, c) = 0.0;
-      }
-      else if (cc == DNL_BC_SPEED)
-      {
-        double4 sv = M.bcval[i];
-        int4 sf = M.bcfun[i];
-        const double s = comp(sv, c);
-        const int fn = c == 0 ? sf.x : (c == 1 ? sf.y : sf.z);
-        double va = s, vb = s, acc = 0.0;
-        if (fn >= 0)
-        {
-          const double fa = func_value(M, fn, t), fb = func_value(M, fn, t + dt);
-          acc = (fb - fa) * s / dt;
-          va = fa * s;
-          vb = fb * s;
-        }
-        comp(a0, c) = comp(a1, c) = acc;
-        comp(v0, c) = va;
-        comp(v1, c) = vb;
-        comp(u0, c) = va * dt;
-        comp(du, c) = vb * dt;
-      }
+      const double fa = func_value(M, fn, t), fb = func_value(M, fn, t + dt);
+      acc = (fb - fa) * sv / dt;
+      va = fa * sv;
+      vb = fb * sv;
     }
-    M.u[f0][i] = u0;
-    M.v[f0][i] = v0;
-    M.a[f0][i] = a0;
+    a1 = acc;
+    v1 = vb;
+    du = vb * dt;
+    put(M.u[f0] + i, va * dt);
+    put(M.v[f0] + i, va);
+    put(M.a[f0] + i, acc);
   }
-  X.x += du.x;
-  X.y += du.y;
-  X.z += du.z;
-  D.x += du.x;
-  D.y += du.y;
-  D.z += du.z;
-  M.x[i] = X;
-  M.disp[i] = D;
-  M.u[f1][i] = du;
-  M.v[f1][i] = v1;
-  M.a[f1][i] = a1;
+  put(M.x + i, X + du);
+  put(M.disp + i, D + du);
+  put(M.u[f1] + i, du);
+  put(M.v[f1] + i, v1);
+  put(M.a[f1] + i, a1);
+}
+
+// A single model: one thread per (node, component).
+template <typename R, int DIM>
+__global__ void __launch_bounds__(NODAL_THREADS) k_nodal(DevModel M)
+{
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0) // for the Courant pass that follows (k_courant_finish)
+    *M.step_due = M.ctl[0].active && M.ctl[0].due;
+  const int i = (int)(k / 3), c = (int)(k - 3LL * i);
+  if (i < M.nN)
+    nodal_update<R, DIM>(M, i, c, M.ctl);
+}
+
+// A batch: a grid-stride loop over the (node, component) pairs of the running
+// instances only (k_active_list), so that stopped instances cost nothing.
+template <typename R, int DIM>
+__global__ void __launch_bounds__(NODAL_THREADS) k_nodal_batch(DevModel M)
+{
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0)
+    *M.step_due = 1u;
+  const int na = *M.act_count;
+  const long long n3 = 3LL * M.act_node_pre[na];
+  for (long long kk = k; kk < n3; kk += (long long)gridDim.x * blockDim.x)
+  {
+    const int j = (int)(kk / 3), c = (int)(kk - 3LL * j);
+    const int a = find_segment(M.act_node_pre, na, j);
+    const Ctl *C = M.ctl + M.act_list[a];
+    nodal_update<R, DIM>(M, C->node_begin + (j - M.act_node_pre[a]), c, C);
+  }
 }
 
 // Predictor boundary conditions on field0 of the imposed-speed nodes before the
@@ -1862,18 +1987,43 @@ __global__ void __launch_bounds__(256) k_courant_finish(DevModel M)
   const int lane = threadIdx.x & 31;
   const int stride = gridDim.x * blockDim.x;
   const int nE32 = (M.nE + 31) & ~31; // whole warps, so every lane takes the same trips
-  const bool any = (M.nInst > 1) || (M.ctl[0].active && M.ctl[0].due);
-  if (any)
+  // read from the flag the nodal pass wrote, not from the control block, which
+  // the block that finishes the increment rewrites while others may still read
+  if (*M.step_due == 0u)
+  {
+    // a single model whose time step is not due: no minimum to wait for, the
+    // first block finishes the increment and the others leave at once
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      finish_increment(M.ctl[0]);
+    return;
+  }
+  if (M.nInst == 1)
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nE32; e += stride)
     {
       const bool valid = e < M.nE;
-      const int ec = valid ? e : M.nE - 1;
-      const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, ec) : 0;
+      Ctl *C = M.ctl;
+      const bool act = valid && C->active && C->due;
+      if (__ballot_sync(0xffffffffu, act) != 0)
+        courant_warp<R, NPE>(M, valid ? e : M.nE - 1, lane, 0, act, C);
+    }
+  else
+  {
+    // the elements of the running instances only (k_active_list)
+    const int na = *M.act_count;
+    const int nAct = M.act_elem_pre[na], nAct32 = (nAct + 31) & ~31;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nAct32; k += stride)
+    {
+      const bool valid = k < nAct;
+      const int kc = valid ? k : nAct - 1;
+      const int a = find_segment(M.act_elem_pre, na, kc);
+      const int inst = M.act_list[a];
       Ctl *C = M.ctl + inst;
+      const int e = C->elem_begin + (kc - M.act_elem_pre[a]);
       const bool act = valid && C->active && C->due;
       if (__ballot_sync(0xffffffffu, act) != 0)
         courant_warp<R, NPE>(M, e, lane, inst, act, C);
     }
+  }
   // last block done: every block's minima are in memory before it counts itself
   __shared__ bool last;
   __threadfence();

@@ -196,8 +196,11 @@ const Variant &variant_of(const dnl_engine *h, int v)
 
 template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
 {
-  const int blocks = (int)(((long)h->nE * NPE + TILE - 1) / TILE);
-  k_element<R, NPE, MINB><<<blocks, TILE, 0, h->stream>>>(h->M);
+  // one block per tile; a batch loops over its running instances' tiles
+  int blocks = h->nTiles;
+  if (h->nInst > 1)
+    blocks = std::min(blocks, MINB * h->numSMs);
+  k_element<R, NPE, MINB><<<blocks, TILE, 0, h->stream>>>(h->M, h->nTiles);
   return DNL_OK;
 }
 
@@ -313,39 +316,72 @@ int launch_element_any(dnl_engine *h, int mode)
         k_element_start<double, 4><<<blocks, TILE, 0, h->stream>>>(h->M);
     }
   }
-  else if (h->mode != DNL_MODE_PLAIN)
-    rc = h->npe == 8 ? launch_mode_any<8>(h) : launch_mode_any<4>(h);
-  else if (h->npe == 4)
-  {
-    // the axisymmetric models are small: one plain variant
-    if (h->precision == DNL_PREC_MIXED)
-      rc = launch_plain<float, 4, 6>(h);
-    else
-      rc = launch_plain<double, 4, 4>(h);
-  }
   else
-    rc = h->precision == DNL_PREC_MIXED ? launch_variant<float, 8>(h, h->variant)
-                                        : launch_variant<double, 8>(h, h->variant);
+  {
+    if (h->nInst > 1)
+    {
+      // the running instances of this increment, for the element, nodal and Courant passes
+      k_active_list<<<1, 1024, 0, h->stream>>>(h->M, h->npe);
+      h->launches++;
+    }
+    if (h->mode != DNL_MODE_PLAIN)
+      rc = h->npe == 8 ? launch_mode_any<8>(h) : launch_mode_any<4>(h);
+    else if (h->npe == 4)
+    {
+      // the axisymmetric models are small: one plain variant
+      if (h->precision == DNL_PREC_MIXED)
+        rc = launch_plain<float, 4, 6>(h);
+      else
+        rc = launch_plain<double, 4, 4>(h);
+    }
+    else
+      rc = h->precision == DNL_PREC_MIXED ? launch_variant<float, 8>(h, h->variant)
+                                          : launch_variant<double, 8>(h, h->variant);
+  }
   h->launches++;
   return rc;
 }
 
 int launch_nodal(dnl_engine *h)
 {
-  const int threads = NODAL_THREADS, blocks = (h->nN + threads - 1) / threads;
-  if (h->precision == DNL_PREC_MIXED)
+  const int threads = NODAL_THREADS;
+  if (h->nInst > 1)
   {
-    if (h->dim == 3)
-      k_nodal<float, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+    // a batch loops over its running instances' (node, component) pairs
+    const int blocks = (int)std::min<long long>((3LL * h->nN + threads - 1) / threads, 16LL * h->numSMs);
+    if (h->precision == DNL_PREC_MIXED)
+    {
+      if (h->dim == 3)
+        k_nodal_batch<float, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+      else
+        k_nodal_batch<float, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+    }
     else
-      k_nodal<float, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+    {
+      if (h->dim == 3)
+        k_nodal_batch<double, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+      else
+        k_nodal_batch<double, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+    }
   }
   else
   {
-    if (h->dim == 3)
-      k_nodal<double, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+    // a thread per (node, component)
+    const int blocks = (int)((3LL * h->nN + threads - 1) / threads);
+    if (h->precision == DNL_PREC_MIXED)
+    {
+      if (h->dim == 3)
+        k_nodal<float, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+      else
+        k_nodal<float, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+    }
     else
-      k_nodal<double, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+    {
+      if (h->dim == 3)
+        k_nodal<double, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+      else
+        k_nodal<double, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+    }
   }
   h->launches++;
   return DNL_OK;
@@ -749,14 +785,28 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     return rc;
   }
   cudaMemsetAsync(h->dstats, 0, 5 * sizeof(unsigned long long), h->stream);
-  if ((rc = dalloc(h, &M.done_count, 1)))
+  if ((rc = dalloc(h, &M.done_count, 2)))
   {
     std::string e = h->err;
     dnl_engine_destroy(h);
     snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
     return rc;
   }
-  cudaMemsetAsync(M.done_count, 0, sizeof(unsigned), h->stream);
+  cudaMemsetAsync(M.done_count, 0, 2 * sizeof(unsigned), h->stream);
+  M.step_due = M.done_count + 1;
+  if ((rc = dalloc(h, &M.act_count, 1)) || (rc = dalloc(h, &M.act_list, h->nInst)) ||
+      (rc = dalloc(h, &M.act_tile_pre, h->nInst + 1)) || (rc = dalloc(h, &M.act_node_pre, h->nInst + 1)) ||
+      (rc = dalloc(h, &M.act_elem_pre, h->nInst + 1)))
+  {
+    std::string e = h->err;
+    dnl_engine_destroy(h);
+    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+    return rc;
+  }
+  cudaMemsetAsync(M.act_count, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(M.act_tile_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
+  cudaMemsetAsync(M.act_node_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
+  cudaMemsetAsync(M.act_elem_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
   M.stats = h->dstats;
   M.harvest_count = h->dstats + 4;
   M.harvest_stride = 1;
