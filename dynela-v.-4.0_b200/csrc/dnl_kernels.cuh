@@ -1104,7 +1104,11 @@ template <int NPE> struct TileMap
 };
 
 // Element pass, one thread per Gauss point, state read straight from global memory.
-// A block takes the work slots (TileMap) blockIdx.x, + gridDim.x, ...
+// One block per work slot (TileMap): a tile of a single model, or a tile of a
+// running instance of a batch (blocks past the slots leave at once).  The
+// same binary serves both, so that a model gives the same bits alone and in a
+// batch; the persistent variants below are the ones that suit the tail of a
+// batch, where few instances still run.
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M, int nTiles)
 {
@@ -1114,25 +1118,21 @@ __global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M, int nTiles)
   const int g = lane & (NPE - 1);
   const int base = lane & ~(NPE - 1);
   const TileMap<NPE> map{M, nTiles};
-  const int nSlots = map.count();
-  for (int slot = blockIdx.x; slot < nSlots; slot += gridDim.x)
-  {
-    int tile, inst;
-    map.get(slot, tile, inst);
-    const int q = tile * TILE + threadIdx.x;
-    const int e = q / NPE;
-    Ctl *C = M.ctl + inst;
-    const bool act = e >= C->elem_begin && e < C->elem_end && C->active;
-    const unsigned amask = __ballot_sync(0xffffffffu, act);
-    if (act)
-    {
-      GlobalState<R> old{M, q};
-      EngineIo<R> io{M, q, C->f0};
-      element_update<R, NPE>(io, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
-                             sh + (threadIdx.x - g) * ROW);
-    }
-    __syncwarp();
-  }
+  if ((int)blockIdx.x >= map.count())
+    return;
+  int tile, inst;
+  map.get(blockIdx.x, tile, inst);
+  const int q = tile * TILE + threadIdx.x;
+  const int e = q / NPE;
+  Ctl *C = M.ctl + inst;
+  const bool act = e >= C->elem_begin && e < C->elem_end && C->active;
+  const unsigned amask = __ballot_sync(0xffffffffu, act);
+  if (!act)
+    return;
+  GlobalState<R> old{M, q};
+  EngineIo<R> io{M, q, C->f0};
+  element_update<R, NPE>(io, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
+                         sh + (threadIdx.x - g) * ROW);
 }
 
 // ----------------------------------------------- bulk-copy (TMA) primitives

@@ -184,7 +184,7 @@ struct Variant
 // blocks per SM (fewest registers, most spilled) to the fewest (no spills)
 // then the fully staged kernel (node gathers one tile ahead as well)
 const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4}, {"tma/5", 1, 5},
-                                {"tma/3", 1, 3},   {"tma/2", 1, 2},   {"stage/3", 2, 3}, {"stage/2", 2, 2}};
+                                {"tma/3", 1, 3},   {"stage/4", 2, 4}, {"stage/3", 2, 3}, {"stage/2", 2, 2}};
 const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2},  {"tma/3", 1, 3},
                                 {"plain/2", 0, 2}, {"tma/1", 1, 1},   {"stage/2", 2, 2}, {"stage/1", 2, 1}};
 constexpr int kNumVariants = DNL_NUM_VARIANTS;
@@ -196,11 +196,9 @@ const Variant &variant_of(const dnl_engine *h, int v)
 
 template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
 {
-  // one block per tile; a batch loops over its running instances' tiles
-  int blocks = h->nTiles;
-  if (h->nInst > 1)
-    blocks = std::min(blocks, MINB * h->numSMs);
-  k_element<R, NPE, MINB><<<blocks, TILE, 0, h->stream>>>(h->M, h->nTiles);
+  // one block per work slot: a batch has up to nInst - 1 more slots than tiles
+  // (a tile shared by two running instances is a slot of each)
+  k_element<R, NPE, MINB><<<h->nTiles + h->nInst - 1, TILE, 0, h->stream>>>(h->M, h->nTiles);
   return DNL_OK;
 }
 
@@ -811,7 +809,10 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.harvest_count = h->dstats + 4;
   M.harvest_stride = 1;
   M.guess_scope = DNL_GUESS_ALL;
-  h->variant = 0;
+  // batches start on a persistent variant: the plain one launches a block per
+  // tile of the whole batch, which the tail of a batch (few instances still
+  // running) cannot afford
+  h->variant = (h->nInst > 1) ? 6 : 0;
   h->powerIteration = (descs[0]->ts_method == DNL_TS_POWER_ITERATION);
   if (h->powerIteration)
   {
@@ -1434,10 +1435,15 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps)
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  int best = 0;
+  int best = h->variant;
   double bestMs = 1e30;
   for (int v = 0; v < kNumVariants; v++)
   {
+    if (h->nInst > 1 && variant_of(h, v).tma == 0)
+    {
+      h->variantMs[v] = -1.0; // plain variants are not offered to batches (see create)
+      continue;
+    }
     for (auto &p : parts)
       CK(cudaMemcpyAsync(const_cast<void *>(p.src), p.dst, p.bytes, cudaMemcpyDeviceToDevice, h->stream));
     h->variant = v;

@@ -250,8 +250,11 @@ int64_t dnl_engine_launch_count(const dnl_engine *h);
 /* Element-pass autotuner (hex8 models): times each kernel variant (register
  * budget, plain or bulk-copy-staged persistent tiles) over `steps` increments
  * run from a saved copy of the state, keeps the fastest for the following runs
- * and restores the state.  No counterpart in the reference (its element loop
- * has one implementation). */
+ * and restores the state.  A batch (several instances) is offered the
+ * persistent variants only (its ms entries for the plain ones are -1): the
+ * plain variants launch a block per tile of the whole batch at every
+ * increment, even when few instances still run.  No counterpart in the
+ * reference (its element loop has one implementation). */
 int dnl_engine_autotune(dnl_engine *h, int32_t steps);
 #define DNL_NUM_VARIANTS 8
 /* Variant in use and the element-pass time (ms) the autotuner measured for each. */
