@@ -178,10 +178,27 @@ __host__ __device__ constexpr int node_sign(int n, int k)
 // Point state in tiles of TILE consecutive integration points: within a tile,
 // component-major (one TILE-long run per component), so that a tile is one
 // contiguous block for a bulk copy and every component access is coalesced.
+// Inside a tile the components that the element pass reads come first: the
+// pressure and the density (which it only writes) are moved to the last two
+// runs, so that the staged passes copy DNL_IP_NREAD of the DNL_IP_NCOMP runs.
+// ip_slot maps a component (DNL_IP_*) to its run; the public layout of
+// dnl_engine_get_ips / set_ips is unchanged.
 constexpr int TILE = 128;
+constexpr int DNL_IP_NREAD = DNL_IP_NCOMP - 2;
+__host__ __device__ constexpr int ip_slot(int c)
+{
+  return c < DNL_IP_PRESSURE ? c
+         : c == DNL_IP_PRESSURE ? DNL_IP_NCOMP - 2
+         : c == DNL_IP_DENSITY  ? DNL_IP_NCOMP - 1
+         : c < DNL_IP_DENSITY   ? c - 1
+                                : c - 2; // DNL_IP_EINT, DNL_IP_EINEL -> 24, 25; DNL_IP_DETJ0 -> 26
+}
+static_assert(ip_slot(DNL_IP_EINT) == 24 && ip_slot(DNL_IP_EINEL) == 25 && ip_slot(DNL_IP_DETJ0) == 26 &&
+                  ip_slot(DNL_IP_PRESSURE) == 27 && ip_slot(DNL_IP_DENSITY) == 28 && DNL_IP_NCOMP == 29,
+              "run order of the point state");
 __host__ __device__ __forceinline__ size_t ip_index(int c, int q)
 {
-  return (size_t)(q / TILE) * (DNL_IP_NCOMP * TILE) + (size_t)c * TILE + (q % TILE);
+  return (size_t)(q / TILE) * (DNL_IP_NCOMP * TILE) + (size_t)ip_slot(c) * TILE + (q % TILE);
 }
 
 template <typename R> __device__ __forceinline__ R ipv(const DevModel &M, int c, int q)
@@ -508,7 +525,8 @@ template <typename R> struct SharedTile
 {
   const R *buf;
   int t;
-  __device__ __forceinline__ R operator()(int c) const { return buf[c * TILE + t]; }
+  // a staged tile holds the first DNL_IP_NREAD runs (the pass never reads the others)
+  __device__ __forceinline__ R operator()(int c) const { return buf[ip_slot(c) * TILE + t]; }
 };
 
 // Jacobian J = sum x_n dN_n/dxi and G = sum du_n dN_n/dxi at this lane's Gauss
@@ -1191,7 +1209,7 @@ template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTiles, int *err)
 {
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
-  constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
+  constexpr uint32_t STATE_BYTES = DNL_IP_NREAD * TILE * sizeof(R); // the runs the pass reads
   constexpr uint32_t CONN_BYTES = TILE * sizeof(int);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   R *state[2] = {reinterpret_cast<R *>(smem_raw), reinterpret_cast<R *>(smem_raw + STATE_BYTES)};
@@ -1311,7 +1329,7 @@ template <typename R> struct StagedIo
 template <typename R, int NPE> struct StageLayout
 {
   static constexpr int EPT = TILE / NPE; // elements per tile
-  static constexpr uint32_t STATE_BYTES = DNL_IP_NCOMP * TILE * sizeof(R);
+  static constexpr uint32_t STATE_BYTES = DNL_IP_NREAD * TILE * sizeof(R); // the runs the pass reads
   // coordinates then increments, each as xy[TILE] (double2) and z[TILE]
   static constexpr uint32_t NODE_BYTES = 2 * TILE * (sizeof(double2) + sizeof(double));
   static constexpr uint32_t IDX_BYTES = TILE * sizeof(int);

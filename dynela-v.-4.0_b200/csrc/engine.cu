@@ -204,7 +204,7 @@ template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
 
 template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
 {
-  const size_t smem = 2 * (DNL_IP_NCOMP * TILE * sizeof(R) + TILE * sizeof(int)) + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
+  const size_t smem = 2 * (DNL_IP_NREAD * TILE * sizeof(R) + TILE * sizeof(int)) + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
   static int perSM = -1; // per instantiation
   if (perSM < 0)
   {
