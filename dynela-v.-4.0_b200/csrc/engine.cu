@@ -601,6 +601,31 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   std::vector<int> foff(1, 0);
   h->elemBegin.assign(1, 0);
   h->nodeBegin.assign(1, 0);
+  {
+    long long nn = 0, ne = 0;
+    bool anySpeed = false;
+    for (int i = 0; i < n; i++)
+    {
+      nn += descs[i]->n_nodes;
+      ne += descs[i]->n_elems;
+      if (descs[i]->bc_code)
+        for (long long k = 0; k < 3LL * descs[i]->n_nodes && !anySpeed; k++)
+          anySpeed = descs[i]->bc_code[k] == DNL_BC_SPEED;
+    }
+    x.reserve(nn);
+    v.reserve(nn);
+    bc.reserve(nn);
+    conn.reserve(((size_t)ne * h->npe + TILE - 1) / TILE * TILE);
+    emat.reserve(ne + TILE);
+    // per-node imposed speeds only when some node has one (the nodal pass
+    // reads them only where a component's code is DNL_BC_SPEED)
+    if (anySpeed)
+    {
+      bcval.reserve(nn);
+      bcfun.reserve(nn);
+    }
+    h->hasSpeed = anySpeed;
+  }
   for (int i = 0; i < n; i++)
   {
     const dnl_model_desc *d = descs[i];
@@ -634,13 +659,20 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
             code |= (uint8_t)(cc << (2 * c));
         }
       bc.push_back(code);
-      bcval.push_back(sv);
-      bcfun.push_back(sf);
+      if (h->hasSpeed)
+      {
+        bcval.push_back(sv);
+        bcfun.push_back(sf);
+      }
       if (speed)
         speedNodes.push_back(nb + k);
     }
-    for (long k = 0; k < (long)d->n_elems * h->npe; k++)
-      conn.push_back(d->conn[k] + nb);
+    {
+      const size_t c0 = conn.size(), cn = (size_t)d->n_elems * h->npe;
+      conn.resize(c0 + cn);
+      for (size_t k = 0; k < cn; k++)
+        conn[c0 + k] = d->conn[k] + nb;
+    }
     for (int e = 0; e < d->n_elems; e++)
       emat.push_back(mb + (d->elem_mat ? d->elem_mat[e] : 0));
     for (int m = 0; m < d->n_materials; m++)
@@ -689,6 +721,11 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   conn.resize((size_t)h->nIPpad, 0); // whole tiles for the bulk copies (padding lanes are inactive)
   h->nSpeed = (int)speedNodes.size();
   h->hasSpeed = h->nSpeed > 0;
+  if (!h->hasSpeed)
+  {
+    bcval.assign(1, make_double4(0, 0, 0, 0)); // never read without imposed speeds
+    bcfun.assign(1, make_int4(-1, -1, -1, -1));
+  }
   h->nFunc = (int)foff.size() - 1;
   if (fx.empty())
   {
@@ -730,15 +767,14 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   double4 *d_bcval = nullptr;
   int4 *d_bcfun = nullptr;
   double *d_fx = nullptr, *d_fy = nullptr;
-  std::vector<double4> zeros4(h->nN, make_double4(0, 0, 0, 0));
   if ((rc = upload(h, &d_eb, h->elemBegin)) || (rc = upload(h, &d_nb, h->nodeBegin)) ||
       (rc = upload(h, &d_conn, conn)) || (rc = upload(h, &d_emat, emat)) || (rc = upload(h, &d_mat, mats)) ||
       (rc = upload(h, &d_off, off)) || (rc = upload(h, &d_pos, pos)) || (rc = upload(h, &d_bc, bc)) ||
       (rc = upload(h, &d_bcval, bcval)) || (rc = upload(h, &d_bcfun, bcfun)) ||
       (rc = upload(h, &d_speed, speedNodes)) || (rc = upload(h, &d_fx, fx)) || (rc = upload(h, &d_fy, fy)) ||
-      (rc = upload(h, &d_foff, foff)) || (rc = upload(h, &M.x, x)) || (rc = upload(h, &M.disp, zeros4)) ||
-      (rc = upload(h, &M.u[0], zeros4)) || (rc = upload(h, &M.u[1], zeros4)) || (rc = upload(h, &M.v[0], v)) ||
-      (rc = upload(h, &M.v[1], v)) || (rc = upload(h, &M.a[0], zeros4)) || (rc = upload(h, &M.a[1], zeros4)) ||
+      (rc = upload(h, &d_foff, foff)) || (rc = upload(h, &M.x, x)) || (rc = dalloc(h, &M.disp, h->nN)) ||
+      (rc = dalloc(h, &M.u[0], h->nN)) || (rc = dalloc(h, &M.u[1], h->nN)) || (rc = upload(h, &M.v[0], v)) ||
+      (rc = dalloc(h, &M.v[1], h->nN)) || (rc = dalloc(h, &M.a[0], h->nN)) || (rc = dalloc(h, &M.a[1], h->nN)) ||
       (rc = dalloc(h, &M.mass, h->nN)) || (rc = dalloc(h, &M.fout, h->nN)) ||
       (rc = upload(h, &M.ctl, h->ctlInit)) || (rc = dalloc(h, &h->denergy, 3 * h->nInst)) ||
       (rc = dalloc(h, &h->derr, 1)))
@@ -747,6 +783,21 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     dnl_engine_destroy(h);
     snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
     return rc;
+  }
+  // the zero node fields are cleared on the device, the second speed buffer copied there
+  {
+    const size_t nb4 = sizeof(double4) * h->nN;
+    cudaError_t e = cudaSuccess;
+    for (double4 *p : {M.disp, M.u[0], M.u[1], M.a[0], M.a[1]})
+      if (e == cudaSuccess)
+        e = cudaMemsetAsync(p, 0, nb4, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(M.v[1], M.v[0], nb4, cudaMemcpyDeviceToDevice, h->stream);
+    if (e != cudaSuccess)
+    {
+      dnl_engine_destroy(h);
+      return fail(nullptr, DNL_ERR_CUDA, "clearing the node fields failed: %s", cudaGetErrorString(e));
+    }
   }
   void *ip = nullptr, *slot = nullptr;
   if ((rc = dalloc(h, (char **)&ip, (size_t)DNL_IP_NCOMP * h->nIPpad * rsz)) ||
