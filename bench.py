@@ -473,27 +473,34 @@ def run_engine_arm(args, rank, world, dist):
         import torch
         ips_host = torch.empty((_abi.IP_NCOMP, desc.n_ips), dtype=torch.float64, pin_memory=True).numpy()
         coords_host = torch.empty((desc.n_nodes, 3), dtype=torch.float64, pin_memory=True).numpy()
-        barrier()
-        t0 = time.perf_counter()
-        e = Engine(desc)
-        ta = time.perf_counter()
-        e.init()
-        e.set_variant(variant)
-        tb = time.perf_counter()
-        e.run(max_incs=args.steps)
-        tc = time.perf_counter()
-        coords = e.nodes(_abi.NODE_COORDS, out=coords_host)
-        ips = e.ips(out=ips_host)
-        t1 = time.perf_counter()
-        e.close()
-        wall = max_over_ranks(t1 - t0)
+        # three repetitions, the median reported (host-side times vary from
+        # one run to the next with the state of the host's memory)
+        reps = []
+        for _ in range(3):
+            barrier()
+            t0 = time.perf_counter()
+            e = Engine(desc)
+            ta = time.perf_counter()
+            e.init()
+            e.set_variant(variant)
+            tb = time.perf_counter()
+            e.run(max_incs=args.steps)
+            tc = time.perf_counter()
+            coords = e.nodes(_abi.NODE_COORDS, out=coords_host)
+            ips = e.ips(out=ips_host)
+            t1 = time.perf_counter()
+            e.close()
+            reps.append((max_over_ranks(t1 - t0),
+                         {"create_upload": ta - t0, "start": tb - ta, "increments": tc - tb, "read_back": t1 - tc}))
+        reps.sort(key=lambda r: r[0])
+        wall, secs = reps[len(reps) // 2]
         h2d = desc.coords.nbytes + desc.conn.nbytes + desc.v_init.nbytes + desc.bc_code.nbytes
         d2h = coords.nbytes + ips.nbytes
         e2e = {"value": world * desc.n_elems * args.steps / wall, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "what": "model upload + start of the solve + K increments + coordinates and point state read back "
-                       "into page-locked host arrays allocated before the timing",
-               "seconds": {"create_upload": ta - t0, "start": tb - ta, "increments": tc - tb, "read_back": t1 - tc}}
+                       "into page-locked host arrays allocated before the timing; median of 3 runs",
+               "seconds": secs, "walls_s": [r[0] for r in reps]}
 
     batched = None
     if not args.no_batch:

@@ -51,6 +51,17 @@ struct __align__(128) Ctl
 
 static constexpr unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
+// Programmatic dependent launch: the kernels of an increment are launched so
+// that the next one is scheduled as the blocks of the one before leave; each
+// waits here, before its first memory access, until the previous grid has
+// completed and its writes are visible (a no-op after a normal launch).  No
+// kernel triggers its dependents early: blocks of the next kernel holding
+// registers while the previous one still runs slowed the increment.
+__device__ __forceinline__ void pdl_wait()
+{
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <typename R> struct V4;
 template <> struct V4<double> { using type = double4; };
 template <> struct V4<float> { using type = float4; };
@@ -1130,6 +1141,7 @@ template <int NPE> struct TileMap
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M, int nTiles)
 {
+  pdl_wait();
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   __shared__ R sh[TILE * ROW];
   const int lane = threadIdx.x & 31;
@@ -1208,6 +1220,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTiles, int *err)
 {
+  pdl_wait();
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   constexpr uint32_t STATE_BYTES = DNL_IP_NREAD * TILE * sizeof(R); // the runs the pass reads
   constexpr uint32_t CONN_BYTES = TILE * sizeof(int);
@@ -1347,6 +1360,7 @@ template <typename R, int NPE> struct StageLayout
 template <typename R, int NPE, int MINB>
 __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nTiles, int *err)
 {
+  pdl_wait();
   using L = StageLayout<R, NPE>;
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
   constexpr int EPT = L::EPT;
@@ -1705,6 +1719,7 @@ __device__ __forceinline__ void nodal_update(const DevModel &M, int i, int c, co
 template <typename R, int DIM>
 __global__ void __launch_bounds__(NODAL_THREADS) k_nodal(DevModel M)
 {
+  pdl_wait();
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k == 0) // for the Courant pass that follows (k_courant_finish)
     *M.step_due = M.ctl[0].active && M.ctl[0].due;
@@ -2002,6 +2017,7 @@ __global__ void __launch_bounds__(256) k_courant(DevModel M, int force)
 template <typename R, int NPE>
 __global__ void __launch_bounds__(256) k_courant_finish(DevModel M)
 {
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   const int stride = gridDim.x * blockDim.x;
   const int nE32 = (M.nE + 31) & ~31; // whole warps, so every lane takes the same trips

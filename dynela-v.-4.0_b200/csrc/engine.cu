@@ -194,11 +194,30 @@ const Variant &variant_of(const dnl_engine *h, int v)
   return h->precision == DNL_PREC_MIXED ? kVariantsF32[v] : kVariantsF64[v];
 }
 
+// A kernel of the increment (element, nodal and Courant passes) launched with
+// programmatic stream serialization (see pdl_wait); in the captured graph
+// this is a programmatic edge.
+template <typename... P, typename... A>
+void launch_pdl(dnl_engine *h, void (*k)(P...), int grid, int block, size_t smem, A... args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
 {
   // one block per work slot: a batch has up to nInst - 1 more slots than tiles
   // (a tile shared by two running instances is a slot of each)
-  k_element<R, NPE, MINB><<<h->nTiles + h->nInst - 1, TILE, 0, h->stream>>>(h->M, h->nTiles);
+  launch_pdl(h, k_element<R, NPE, MINB>, h->nTiles + h->nInst - 1, TILE, 0, h->M, h->nTiles);
   return DNL_OK;
 }
 
@@ -214,7 +233,7 @@ template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
       perSM = 1;
   }
   const int grid = std::min(h->nTiles, perSM * h->numSMs);
-  k_element_tma<R, NPE, MINB><<<grid, TILE, smem, h->stream>>>(h->M, h->nTiles, h->derr);
+  launch_pdl(h, k_element_tma<R, NPE, MINB>, grid, TILE, smem, h->M, h->nTiles, h->derr);
   return DNL_OK;
 }
 
@@ -230,7 +249,7 @@ template <typename R, int NPE, int MINB> int launch_stage(dnl_engine *h)
       perSM = 1;
   }
   const int grid = std::min(h->nTiles, perSM * h->numSMs);
-  k_element_stage<R, NPE, MINB><<<grid, TILE, smem, h->stream>>>(h->M, h->nTiles, h->derr);
+  launch_pdl(h, k_element_stage<R, NPE, MINB>, grid, TILE, smem, h->M, h->nTiles, h->derr);
   return DNL_OK;
 }
 
@@ -369,16 +388,16 @@ int launch_nodal(dnl_engine *h)
     if (h->precision == DNL_PREC_MIXED)
     {
       if (h->dim == 3)
-        k_nodal<float, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+        launch_pdl(h, k_nodal<float, 3>, blocks, threads, 0, h->M);
       else
-        k_nodal<float, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+        launch_pdl(h, k_nodal<float, 2>, blocks, threads, 0, h->M);
     }
     else
     {
       if (h->dim == 3)
-        k_nodal<double, 3><<<blocks, threads, 0, h->stream>>>(h->M);
+        launch_pdl(h, k_nodal<double, 3>, blocks, threads, 0, h->M);
       else
-        k_nodal<double, 2><<<blocks, threads, 0, h->stream>>>(h->M);
+        launch_pdl(h, k_nodal<double, 2>, blocks, threads, 0, h->M);
     }
   }
   h->launches++;
@@ -475,16 +494,16 @@ int launch_step_end(dnl_engine *h)
   if (h->precision == DNL_PREC_MIXED)
   {
     if (h->npe == 8)
-      k_courant_finish<float, 8><<<blocks, threads, 0, h->stream>>>(h->M);
+      launch_pdl(h, k_courant_finish<float, 8>, blocks, threads, 0, h->M);
     else
-      k_courant_finish<float, 4><<<blocks, threads, 0, h->stream>>>(h->M);
+      launch_pdl(h, k_courant_finish<float, 4>, blocks, threads, 0, h->M);
   }
   else
   {
     if (h->npe == 8)
-      k_courant_finish<double, 8><<<blocks, threads, 0, h->stream>>>(h->M);
+      launch_pdl(h, k_courant_finish<double, 8>, blocks, threads, 0, h->M);
     else
-      k_courant_finish<double, 4><<<blocks, threads, 0, h->stream>>>(h->M);
+      launch_pdl(h, k_courant_finish<double, 4>, blocks, threads, 0, h->M);
   }
   h->launches++;
   return DNL_OK;
