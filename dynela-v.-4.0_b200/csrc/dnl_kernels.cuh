@@ -109,6 +109,7 @@ struct DevModel
   int *act_count;          // [1]
   int *act_list;           // [nInst]
   int *act_tile_pre, *act_node_pre, *act_elem_pre; // [nInst + 1]
+  int *due_count, *due_list, *due_elem_pre;         // the same for the running instances whose time step is due
 };
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
@@ -1025,16 +1026,17 @@ __device__ __forceinline__ int instance_tiles(const Ctl &c, int npe)
 // with a few long-running instances among hundreds that have stopped).
 __global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
 {
-  __shared__ int wsum[4][32];
-  __shared__ int carry[4];
+  __shared__ int wsum[6][32];
+  __shared__ int carry[6];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  if (t < 4)
+  if (t < 6)
     carry[t] = 0;
   __syncthreads();
   for (int base = 0; base < M.nInst; base += 1024)
   {
     const int i = base + t;
-    int v[4] = {0, 0, 0, 0}; // running, tiles, nodes, elements
+    // running, tiles, nodes, elements; running with the time step due, its elements
+    int v[6] = {0, 0, 0, 0, 0, 0};
     if (i < M.nInst)
     {
       const Ctl &c = M.ctl[i];
@@ -1044,11 +1046,16 @@ __global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
         v[1] = instance_tiles(c, npe);
         v[2] = c.node_end - c.node_begin;
         v[3] = c.elem_end - c.elem_begin;
+        if (c.due)
+        {
+          v[4] = 1;
+          v[5] = v[3];
+        }
       }
     }
-    int inc[4];
+    int inc[6];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
+    for (int k = 0; k < 6; k++)
     {
       inc[k] = v[k];
 #pragma unroll
@@ -1065,7 +1072,7 @@ __global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
     if (w == 0)
     {
 #pragma unroll
-      for (int k = 0; k < 4; k++)
+      for (int k = 0; k < 6; k++)
       {
         int x = wsum[k][lane];
 #pragma unroll
@@ -1079,9 +1086,9 @@ __global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
       }
     }
     __syncthreads();
-    int ex[4];
+    int ex[6];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
+    for (int k = 0; k < 6; k++)
       ex[k] = carry[k] + inc[k] - v[k] + (w > 0 ? wsum[k][w - 1] : 0);
     if (v[0])
     {
@@ -1090,8 +1097,13 @@ __global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
       M.act_node_pre[ex[0]] = ex[2];
       M.act_elem_pre[ex[0]] = ex[3];
     }
+    if (v[4])
+    {
+      M.due_list[ex[4]] = i;
+      M.due_elem_pre[ex[4]] = ex[5];
+    }
     __syncthreads();
-    if (t < 4)
+    if (t < 6)
       carry[t] += wsum[t][31];
     __syncthreads();
   }
@@ -1101,6 +1113,8 @@ __global__ void __launch_bounds__(1024) k_active_list(DevModel M, int npe)
     M.act_tile_pre[carry[0]] = carry[1];
     M.act_node_pre[carry[0]] = carry[2];
     M.act_elem_pre[carry[0]] = carry[3];
+    *M.due_count = carry[4];
+    M.due_elem_pre[carry[4]] = carry[5];
   }
 }
 
@@ -2042,17 +2056,17 @@ __global__ void __launch_bounds__(256) k_courant_finish(DevModel M)
     }
   else
   {
-    // the elements of the running instances only (k_active_list)
-    const int na = *M.act_count;
-    const int nAct = M.act_elem_pre[na], nAct32 = (nAct + 31) & ~31;
+    // the elements of the running instances whose time step is due (k_active_list)
+    const int na = *M.due_count;
+    const int nAct = M.due_elem_pre[na], nAct32 = (nAct + 31) & ~31;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nAct32; k += stride)
     {
       const bool valid = k < nAct;
       const int kc = valid ? k : nAct - 1;
-      const int a = find_segment(M.act_elem_pre, na, kc);
-      const int inst = M.act_list[a];
+      const int a = find_segment(M.due_elem_pre, na, kc);
+      const int inst = M.due_list[a];
       Ctl *C = M.ctl + inst;
-      const int e = C->elem_begin + (kc - M.act_elem_pre[a]);
+      const int e = C->elem_begin + (kc - M.due_elem_pre[a]);
       const bool act = valid && C->active && C->due;
       if (__ballot_sync(0xffffffffu, act) != 0)
         courant_warp<R, NPE>(M, e, lane, inst, act, C);

@@ -864,7 +864,8 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.step_due = M.done_count + 1;
   if ((rc = dalloc(h, &M.act_count, 1)) || (rc = dalloc(h, &M.act_list, h->nInst)) ||
       (rc = dalloc(h, &M.act_tile_pre, h->nInst + 1)) || (rc = dalloc(h, &M.act_node_pre, h->nInst + 1)) ||
-      (rc = dalloc(h, &M.act_elem_pre, h->nInst + 1)))
+      (rc = dalloc(h, &M.act_elem_pre, h->nInst + 1)) || (rc = dalloc(h, &M.due_count, 1)) ||
+      (rc = dalloc(h, &M.due_list, h->nInst)) || (rc = dalloc(h, &M.due_elem_pre, h->nInst + 1)))
   {
     std::string e = h->err;
     dnl_engine_destroy(h);
@@ -875,6 +876,8 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   cudaMemsetAsync(M.act_tile_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
   cudaMemsetAsync(M.act_node_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
   cudaMemsetAsync(M.act_elem_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
+  cudaMemsetAsync(M.due_count, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(M.due_elem_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
   M.stats = h->dstats;
   M.harvest_count = h->dstats + 4;
   M.harvest_stride = 1;
