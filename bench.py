@@ -354,12 +354,21 @@ def guess_run():
     increments 6,000-8,000)."""
     from dnlPython import _abi, guess, meshes
     t0 = time.perf_counter()
-    pairs, st = guess.harvest(meshes.taylor_batch(), capacity=10_000_000, stride=1, max_incs=1500,
-                              scope=_abi.GUESS_FIRST_YIELD)
+    cap, info = 10_000_000, {}
+    pairs, st = guess.harvest(meshes.taylor_batch(), capacity=cap, stride=1, max_incs=1500,
+                              scope=_abi.GUESS_FIRST_YIELD, info=info)
+    stride = 1
+    if info["candidates"] > cap:
+        # more candidates than room: harvest again one in `stride`, a set that
+        # fits and so does not depend on the order of the appends
+        stride = -(-info["candidates"] // cap)
+        del pairs
+        pairs, st = guess.harvest(meshes.taylor_batch(), capacity=cap, stride=stride, max_incs=1500,
+                                  scope=_abi.GUESS_FIRST_YIELD, info=info)
     t1 = time.perf_counter()
     net, hist = guess.train(pairs, epochs=20, batch_tiles=128, learning_rate=1e-3, log_target=True)
     t2 = time.perf_counter()
-    out = {"pairs": int(pairs.shape[0]), "harvest_s": t1 - t0, "train_s": t2 - t1,
+    out = {"pairs": int(pairs.shape[0]), "harvest_stride": stride, "harvest_s": t1 - t0, "train_s": t2 - t1,
            "loss_first_last": [hist[0], hist[-1]], "scope": "first yield (eps_p = 0)",
            "harvest_plain_evals_per_first_yield_point": st[3] / max(st[2], 1)}
     del pairs

@@ -30,7 +30,7 @@ constexpr uint32_t OFF_B1 = OFF_W3 + H * H * 2;   // fp32 biases
 constexpr uint32_t OFF_B2 = OFF_B1 + H * 4;
 constexpr uint32_t OFF_B3 = OFF_B2 + H * 4;
 constexpr uint32_t OFF_W4 = OFF_B3 + H * 4;       // fp32 output weights
-constexpr uint32_t OFF_MISC = OFF_W4 + H * 4;     // b4, in_mean[5], in_scale[5], out_exp, pad
+constexpr uint32_t OFF_MISC = OFF_W4 + H * 4;     // b4, in_mean[5], in_scale[5], out_exp, in_clip, pad
 constexpr uint32_t IMAGE_BYTES = OFF_MISC + 16 * 4;
 // training adds the transposed hidden weights (for dh = dz W), after the image
 constexpr uint32_t OFF_W2T = 0, OFF_W3T = H * H * 2, TRANS_BYTES = 2 * H * H * 2;
@@ -205,9 +205,15 @@ struct Tile
   __device__ __forceinline__ void put_input(int t, const float (&x)[NIN], float (&xin)[KIN])
   {
     const float *misc = reinterpret_cast<const float *>(smem + OFF_MISC);
+    const float clip = misc[12];
 #pragma unroll
     for (int i = 0; i < KIN; i++)
-      xin[i] = (i < NIN) ? (x[i] - misc[1 + i]) * misc[6 + i] : 0.0f;
+    {
+      float v = (i < NIN) ? (x[i] - misc[1 + i]) * misc[6 + i] : 0.0f;
+      if (clip > 0.0f)
+        v = fminf(fmaxf(v, -clip), clip);
+      xin[i] = v;
+    }
     uint4 v[2];
     uint32_t *w = reinterpret_cast<uint32_t *>(v);
 #pragma unroll
@@ -364,6 +370,7 @@ inline void build_image(const dnl_mlp &n, unsigned char *img)
     misc[6 + i] = n.in_scale[i];
   }
   misc[11] = n.out_exp;
+  misc[12] = n.in_clip;
   memcpy(img + OFF_MISC, misc, sizeof(misc));
 }
 

@@ -1678,7 +1678,7 @@ int dnl_engine_harvest_count(dnl_engine *h, int64_t *count)
   unsigned long long n = 0;
   CK(cudaMemcpyAsync(&n, h->dstats + 4, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  *count = (int64_t)std::min<unsigned long long>(n, (unsigned long long)h->M.harvest_cap);
+  *count = (int64_t)n;
   return DNL_OK;
 }
 

@@ -219,11 +219,12 @@ class Mlp(ctypes.Structure):
                 ("w3", (ctypes.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b3", ctypes.c_float * MLP_HIDDEN),
                 ("w4", ctypes.c_float * MLP_HIDDEN), ("b4", ctypes.c_float),
                 ("in_mean", ctypes.c_float * MLP_IN), ("in_scale", ctypes.c_float * MLP_IN),
-                ("out_exp", ctypes.c_float)]
+                ("out_exp", ctypes.c_float), ("in_clip", ctypes.c_float)]
 
     NPARAM = 64 * 16 + 64 + 64 * 64 + 64 + 64 * 64 + 64 + 64 + 1
     _LAYOUT = (("w1", (64, 16)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)), ("w3", (64, 64)),
-               ("b3", (64,)), ("w4", (64,)), ("b4", ()), ("in_mean", (5,)), ("in_scale", (5,)), ("out_exp", ()))
+               ("b3", (64,)), ("w4", (64,)), ("b4", ()), ("in_mean", (5,)), ("in_scale", (5,)), ("out_exp", ()),
+               ("in_clip", ()))
 
     def to_dict(self):
         import numpy as np

@@ -25,11 +25,15 @@ def _torch():
     return torch
 
 
-def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf, scope=_abi.GUESS_ALL):
+def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf, scope=_abi.GUESS_ALL, info=None):
     """Run `descs` (one model or a batch) with the plain return and keep one
     yielding point of `scope` in `stride` as a (5 inputs, r = gamma /
     gamma_max, gamma, gamma_max) pair.  Returns a device tensor [n, 8] and the Newton statistics
-    of the run (Engine.newton_stats)."""
+    of the run (Engine.newton_stats).  The points are chosen by a hash of
+    (point, increment), so the set is reproducible as long as it fits in
+    `capacity`; past it, which points are kept depends on the order of the
+    appends.  info (a dict), if given, receives "candidates": the points that
+    passed the stride, kept or not."""
     torch = _torch()
     buf = torch.zeros((int(capacity), _abi.MLP_PAIR_WORDS), dtype=torch.float32, device="cuda")
     with Engine(descs) as e:
@@ -40,6 +44,9 @@ def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf, scope=_abi.GUES
         e.run(t_pause=t_pause, max_incs=max_incs, check=False)
         n = e.harvest_count()
         stats = e.newton_stats()
+    if info is not None:
+        info["candidates"] = int(n)
+    n = min(int(n), int(capacity))
     # the kernels append pairs in whatever order their atomics resolve: sort
     # the rows (lexicographically, by stable passes from the last word) so
     # that training on them is reproducible
@@ -50,18 +57,21 @@ def harvest(descs, capacity, stride, max_incs=0, t_pause=np.inf, scope=_abi.GUES
 
 
 def initial_network(x, r, seed=1):
-    """He-initialised network whose input normalisation is the mean and
-    standard deviation of the harvested inputs x [n, 5] and whose output bias
-    is the mean target."""
+    """He-initialised network whose input normalisation maps the 0.1-99.9 %
+    range of the harvested inputs x [n, 5] to [-1, 1] and holds inputs outside
+    it at the edge (in_clip = 1: a model whose inputs leave the training
+    range, a finer mesh's time step for instance, is not extrapolated), and
+    whose output bias is the mean target."""
     rng = np.random.default_rng(seed)
     H, K, NIN = _abi.MLP_HIDDEN, 16, _abi.MLP_IN
+    lo, hi = np.percentile(x, [0.1, 99.9], axis=0)
     w1 = np.zeros((H, K), np.float32)
     w1[:, :NIN] = rng.normal(0, np.sqrt(2.0 / NIN), (H, NIN))
     d = dict(w1=w1, b1=np.zeros(H, np.float32), w2=rng.normal(0, np.sqrt(2.0 / H), (H, H)).astype(np.float32),
              b2=np.zeros(H, np.float32), w3=rng.normal(0, np.sqrt(2.0 / H), (H, H)).astype(np.float32),
              b3=np.zeros(H, np.float32), w4=(0.1 * rng.normal(0, np.sqrt(1.0 / H), H)).astype(np.float32),
-             b4=np.float32(np.mean(r)), in_mean=np.mean(x, axis=0).astype(np.float32),
-             in_scale=(1.0 / (np.std(x, axis=0) + 1e-6)).astype(np.float32))
+             b4=np.float32(np.mean(r)), in_mean=((lo + hi) / 2).astype(np.float32),
+             in_scale=(2.0 / np.maximum(hi - lo, 1e-6)).astype(np.float32), in_clip=np.float32(1.0))
     return _abi.Mlp.from_dict(d)
 
 

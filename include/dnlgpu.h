@@ -300,7 +300,9 @@ int dnl_element_pass_static(int32_t elem_type, int32_t n_nodes, int32_t n_elems,
  * Inputs, computed in FP32 from the point state before the return:
  *   x0 = sigma_trial / A, x1 = eps_p, x2 = ln(1 + depsp / depsp0),
  *   x3 = T / Tm, x4 = ln(3 G dt depsp0 / A)
- * and normalised as (x - in_mean) * in_scale.  The hidden layers run as BF16
+ * and normalised as (x - in_mean) * in_scale, then, when in_clip > 0, held to
+ * [-in_clip, in_clip] (inputs past the range the network was trained on are
+ * taken at its edge instead of extrapolated).  The hidden layers run as BF16
  * tensor-core products with FP32 accumulation; the output layer in FP32.
  * Weights are FP32 here and rounded to BF16 on the device. */
 #define DNL_MLP_IN 5
@@ -317,6 +319,7 @@ typedef struct dnl_mlp {
   float in_mean[DNL_MLP_IN];
   float in_scale[DNL_MLP_IN];
   float out_exp; /* 0: r = output; 1: r = exp(output) (a network trained on ln r) */
+  float in_clip; /* > 0: normalised inputs held to [-in_clip, in_clip]; 0: not held */
 } dnl_mlp;
 
 /* One training pair as harvested from the radial return: the 5 raw inputs,
@@ -336,6 +339,8 @@ int dnl_engine_set_guess_network(dnl_engine *h, const dnl_mlp *net);
  * (chosen by a hash of point and increment) is kept until the buffer is full.
  * Resets the pair count. */
 int dnl_engine_set_harvest(dnl_engine *h, float *d_pairs, int64_t capacity, int32_t stride);
+/* Points that passed the stride since the last dnl_engine_set_harvest: the
+ * pairs stored are the first min(count, capacity) rows of the buffer. */
 int dnl_engine_harvest_count(dnl_engine *h, int64_t *count);
 /* Which yielding points start from the network in DNL_MODE_GUESS:
  * DNL_GUESS_ALL every one, DNL_GUESS_FIRST_YIELD only those without a

@@ -37,6 +37,9 @@ def silu_grad(z):
 def normalise(net, x, dt=np.float32):
     xin = np.zeros((x.shape[0], KIN), dtype=dt)
     xin[:, :NIN] = (x.astype(dt) - np.asarray(net["in_mean"], dt)) * np.asarray(net["in_scale"], dt)
+    clip = float(net.get("in_clip", 0.0))
+    if clip > 0.0:  # inputs past the training range held at its edge (dnl_mlp.in_clip)
+        xin[:, :NIN] = np.clip(xin[:, :NIN], -clip, clip)
     return xin
 
 
