@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
     p.add_argument("--no-guess", action="store_true", help="skip the learned Newton initial guess block")
     p.add_argument("--no-necking", action="store_true", help="skip the necking workloads block")
+    p.add_argument("--no-config0", action="store_true", help="skip the axisymmetric Taylor bar block")
     p.add_argument("--batch-fp64-sample", type=int, default=32,
                    help="instances of the batch timed one by one on the FP64 path")
     p.add_argument("--axial", type=int, default=160,
@@ -344,6 +345,37 @@ def necking_run(incs=300):
     return out
 
 
+def config0_run():
+    """The reference's own CPU-scale case: the axisymmetric copper Taylor bar
+    (10 x 80 ElQua4NAx, 227 m/s, 80 us), run whole on the GPU with the Courant
+    time step (every 10 increments) and with the power iteration of the
+    Taylor-Axi sample (every increment), mixed and FP64; beside it the
+    reference on the host cores for a bounded sample of its increments."""
+    from dnlPython import _abi, meshes
+    from dnlPython.engine import Engine
+    out = {}
+    for ts, tname, freq in ((_abi.TS_COURANT, "courant_every_10", 10), (_abi.TS_POWER_ITERATION, "power_iteration_every_1", 1)):
+        res = {}
+        for prec, pname in ((_abi.PREC_MIXED, "mixed"), (_abi.PREC_FP64, "fp64")):
+            d = meshes.taylor_axi(ts_method=ts, ts_freq=freq, precision=prec)
+            with Engine(d) as e:
+                e.init()
+                n = e.run()
+                ms = e.timings()["run_ms"]
+                c = e.nodes(_abi.NODE_COORDS)
+                res[pname] = {"increments": int(n), "run_s": ms / 1e3, "elem_steps_per_s": d.n_elems * n / (ms / 1e3),
+                              "height_mm": float(c[d.n_nodes - 1 - 10, 1]), "foot_radius_mm": float(c[10, 0])}
+        d = meshes.taylor_axi(ts_method=ts, ts_freq=freq, precision=_abi.PREC_FP64)
+        got = reference_rate(d, steps=1000, warmup=0, threads=os.cpu_count() or 1)
+        if got is not None:
+            v, kind, cores, sample = got
+            res["reference"] = {"elem_steps_per_s": v, "cores": cores, "sample": sample,
+                                "est_run_s": d.n_elems * res["fp64"]["increments"] / v}
+        out[tname] = res
+    out["elements"] = 800
+    return out
+
+
 def guess_run():
     """The learned Newton initial guess: pairs harvested from the first-yield
     returns of the 256-bar batch (its first 1,500 increments), the network
@@ -550,6 +582,8 @@ def run_engine_arm(args, rank, world, dist):
         out["batched"] = batched
     if world == 1 and not args.no_necking:
         out["necking"] = necking_run()
+    if world == 1 and not args.no_config0:
+        out["taylor_axi_800"] = config0_run()
     if world == 1 and AXIAL == 160 and not args.no_guess:
         out["learned_guess"] = guess_run()
     print(json.dumps(out))
