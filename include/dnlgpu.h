@@ -250,7 +250,9 @@ int64_t dnl_engine_launch_count(const dnl_engine *h);
 /* Element-pass autotuner (hex8 models): times each kernel variant (register
  * budget, plain or bulk-copy-staged persistent tiles) over `steps` increments
  * run from a saved copy of the state, keeps the fastest for the following runs
- * and restores the state.  A batch (several instances) is offered the
+ * (on the mixed path the staged 4-blocks-per-SM variant, 5, when it is within
+ * 1 % of the fastest: it holds up best later in an impact) and restores the
+ * state.  A batch (several instances) is offered the
  * persistent variants only (its ms entries for the plain ones are -1): the
  * plain variants launch a block per tile of the whole batch at every
  * increment, even when few instances still run.  No counterpart in the
