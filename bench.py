@@ -473,9 +473,16 @@ def run_engine_arm(args, rank, world, dist):
     value = world * desc.n_elems * args.steps / (ms / 1e3)
     ctl = eng.control()
 
-    # ---- roofline of the element kernel (per-kernel CUDA events on the engine stream)
+    # ---- roofline of the element kernel (per-kernel CUDA events on the engine
+    # stream) over the same increments as the timed region: a second engine on
+    # the same model replays them (the solve is deterministic) kernel by kernel
+    eng.close()
+    eng = Engine(desc).init()
+    eng.set_variant(variant)
+    if args.warmup:
+        eng.run(max_incs=args.warmup)
     eng.set_timing(True)
-    kt = min(args.steps, 200)
+    kt = args.steps
     eng.run(max_incs=kt)
     tim = eng.timings()
     eng.set_timing(False)
