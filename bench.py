@@ -286,17 +286,20 @@ def batch_run(sample, dist=None, world=1, rank=0):
         launches = b.launch_count()
         ctl = [b.control(i) for i in range(len(descs))]
     incs = np.array([c["increment"] for c in ctl], dtype=np.float64)
-    failed = [mine[i] for i, c in enumerate(ctl) if c["status"] != 0]
     steps_rank = float((elems * incs).sum())
     ms = parallel.reduce_max(ms_rank, dist)
     steps = parallel.reduce_sum(steps_rank, dist)
+    # one gather of the per-instance records at the end (every rank ran its own bars)
+    rec = parallel.gather_records({mine[i]: {"increments": int(c["increment"]), "status": int(c["status"]),
+                                             "time": float(c["time"])} for i, c in enumerate(ctl)}, dist)
+    all_incs = np.array([rec[i]["increments"] for i in sorted(rec)], dtype=np.float64)
     n_all = len(all_descs)
     out = {"instances": n_all, "elements": int(sum(d.n_elems for d in all_descs)), "seed": 20261203,
            "precision": "mixed", "ranks": world, "replays_rank0": int(replays), "run_ms": ms,
            "sims_per_s": n_all / (ms / 1e3), "elem_steps_per_s": steps / (ms / 1e3),
-           "increments_min_max_rank0": [int(incs.min()), int(incs.max())],
-           "stopped_on_error_rank0": {str(i): _abi.ERRORS.get(ctl[mine.index(i)]["status"], "error")
-                                      + f" at t={ctl[mine.index(i)]['time']:.3e}" for i in failed},
+           "increments_min_median_max": [int(all_incs.min()), int(np.median(all_incs)), int(all_incs.max())],
+           "stopped_on_error": {str(i): _abi.ERRORS.get(r["status"], "error") + f" at t={r['time']:.3e}"
+                                for i, r in sorted(rec.items()) if r["status"] != 0},
            "element_variant_rank0": int(variant), "gpu_launches_rank0": launches, "setup_s_rank0": setup}
     if sample > 0:
         order = np.argsort(elems, kind="stable")

@@ -1,7 +1,8 @@
 """Several GPUs, one process per GPU: independent models (a batch of
 simulations) are partitioned across the ranks with no exchange during the
 run; a single mesh runs as one replica per rank.  The only collectives are
-the timing barrier and the max-over-ranks of the measured times
+the timing barrier, the max-over-ranks of the measured times and, at the
+end, one gather of the per-instance result records (a few bytes each)
 (torch.distributed: NCCL on GPUs, gloo on the host).
 """
 import numpy as np
@@ -51,3 +52,21 @@ def reduce_sum(value, dist, device=None):
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def gather_records(records, dist):
+    """Per-instance result records of every rank, merged on every rank:
+    `records` maps this rank's instance indices to small dicts; returns one
+    dict of all instances (records of the same index from two ranks are an
+    error: the partition gives each instance to one rank)."""
+    if dist is None:
+        return dict(records)
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, dict(records))
+    out = {}
+    for p in parts:
+        for k, v in p.items():
+            if k in out:
+                raise ValueError(f"instance {k} reported by two ranks")
+            out[k] = v
+    return out

@@ -45,7 +45,8 @@ def _rank_main(rank, world, port, out):
         work = sum(descs[i].n_elems for i in mine)
         total = parallel.reduce_sum(work, dist)
         slowest = parallel.reduce_max(1.0 + rank, dist)
-        out.put((rank, mine, total, slowest))
+        records = parallel.gather_records({i: {"elements": descs[i].n_elems, "rank": rank} for i in mine}, dist)
+        out.put((rank, mine, total, slowest, records))
     finally:
         dist.destroy_process_group()
 
@@ -67,3 +68,8 @@ def test_two_gloo_ranks_split_a_batch():
     assert sorted(res[0][1] + res[1][1]) == list(range(16)) and not set(res[0][1]) & set(res[1][1])
     assert res[0][2] == res[1][2] == sum(d.n_elems for d in descs)
     assert res[0][3] == res[1][3] == 2.0
+    # every rank ends with every instance's record, each from the rank that ran it
+    for r in res:
+        assert sorted(r[4]) == list(range(16))
+        assert all(r[4][i]["elements"] == descs[i].n_elems for i in range(16))
+        assert all(r[4][i]["rank"] == (0 if i in res[0][1] else 1) for i in range(16))
