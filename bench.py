@@ -94,16 +94,17 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """dram read+write bytes per element-kernel launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "element_kernel_taylor3d.md")
+    """DRAM bytes (read + write) of one element-kernel launch on this
+    workload, from a committed ncu capture (profiles/element_kernel_traffic.json):
+    a counter bench.py cannot read while it times.  Returns (bytes, source)."""
+    p = os.path.join(ROOT, "profiles", "element_kernel_traffic.json")
     try:
         with open(p) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_launch_mixed:"):
-                    return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+            d = json.load(f)
+        return float(d["traffic_bytes_per_launch_mixed"]), \
+            f"committed ncu capture of {d['kernel']} ({d['workload']}), profiles/element_kernel_traffic.json"
+    except (OSError, KeyError, ValueError):
+        return None, None
 
 
 # ------------------------------------------------------------------- clocks
@@ -213,7 +214,7 @@ def port_rate(desc, steps):
 
 def cpu_baseline(desc):
     threads = os.cpu_count() or 1
-    got = reference_rate(desc, steps=3, warmup=0, threads=threads)
+    got = reference_rate(desc, steps=10, warmup=0, threads=threads)
     if got is None:
         got = port_rate(desc, steps=1)
     v, kind, cores, sample = got
@@ -416,12 +417,29 @@ def guess_run():
 
 # ------------------------------------------------------------------ arms
 
-def run_reference_arm(args, rank):
+# The reference runs an increment of the measured mesh in about 0.75 s on 16
+# host threads: its arm runs the GPU arm's steps and warm-up as long as they
+# stay within this many increments (a few minutes), and fewer beyond.
+REF_MAX_INCREMENTS = 200
+
+
+def bench_config(desc, args, world):
+    """The `config` of the JSON line, the same on both arms."""
+    return {"workload": WORKLOAD, "elements": desc.n_elems, "nodes": desc.n_nodes, "gauss_points": desc.n_ips,
+            "time_step": "courant every 10", "increments_from_t0": [args.warmup, args.warmup + args.steps],
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "inputs larger than L2 (point state 143 MB mixed / 285 MB FP64 > 126 MB)"}
+
+
+def run_reference_arm(args, rank, world):
     if rank != 0:
         return
     desc = workload("fp64")
     threads = os.cpu_count() or 1
-    steps, warmup = max(1, min(args.steps, 10)), min(args.warmup, 2)
+    steps, warmup = args.steps, args.warmup
+    if steps + warmup > REF_MAX_INCREMENTS:
+        steps = max(1, min(steps, REF_MAX_INCREMENTS // 2))
+        warmup = min(warmup, REF_MAX_INCREMENTS - steps)
     got = reference_rate(desc, steps=steps, warmup=warmup, threads=threads)
     if got is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libdnlref.so is not built"}))
@@ -430,9 +448,8 @@ def run_reference_arm(args, rank):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": warmup, "ms_per_step": desc.n_elems / v * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": desc.n_elems, "nodes": desc.n_nodes, "precision": "fp64",
-                   "parallelism": f"openmp{cores}"},
+        "vs_baseline": None, "dtype": "f64", "precision": "fp64", "data": "synthetic",
+        "config": bench_config(desc, args, world),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -493,9 +510,10 @@ def run_engine_arm(args, rank, world, dist):
     eb, sb = alg_bytes(desc, word)
     peak, peak_kind = measured_peak()
     achieved = eb / (elem_ms / 1e3) / 1e9
-    traffic = profiled_traffic() if args.precision == "mixed" else None
+    traffic, traffic_source = profiled_traffic() if args.precision == "mixed" else (None, None)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_element", "peak_source": peak_kind,
+                "traffic": traffic, "traffic_source": traffic_source, "kernel": "k_element",
+                "peak_source": peak_kind,
                 "alg_bytes_per_launch": eb, "ms_per_launch": elem_ms}
     step_roofline = {"achieved": sb / (ms / args.steps / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": sb / (ms / args.steps / 1e3) / 1e9 / peak, "alg_bytes_per_step": sb,
@@ -564,12 +582,9 @@ def run_engine_arm(args, rank, world, dist):
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "elements": desc.n_elems, "nodes": desc.n_nodes,
-                   "gauss_points": desc.n_ips, "precision": args.precision, "time_step": "courant every 10",
-                   "increments_from_t0": [args.warmup, args.warmup + args.steps],
-                   "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": f"inputs larger than L2 (point state {desc.n_ips * 29 * word / 1e6:.0f} MB > 126 MB)"},
+        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "precision": args.precision, "data": "synthetic",
+        "config": bench_config(desc, args, world),
         "roofline": roofline,
         "step_roofline": step_roofline,
         "gpu_launches": launches,
@@ -578,6 +593,8 @@ def run_engine_arm(args, rank, world, dist):
     }
     if fp64:
         out["fp64_path"] = fp64
+        # the like-for-like figure beside the reference (both FP64), at the top level
+        out["fp64_value"] = fp64["value"]
         out["mixed_over_fp64"] = (desc.n_elems * args.steps / (run_ms / 1e3)) / fp64["value"]
     if clocks:
         out["clocks"] = clocks
@@ -585,6 +602,8 @@ def run_engine_arm(args, rank, world, dist):
         out["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(desc)
+        if fp64:
+            out["fp64_over_cpu_baseline"] = fp64["value"] / out["cpu_baseline"]["value"]
     # whole runs and the batch hold one GPU for a few minutes: single-GPU runs only
     if world == 1 and AXIAL == 160 and not args.no_accuracy:
         out["accuracy_whole_run"] = accuracy_run()
@@ -599,22 +618,51 @@ def run_engine_arm(args, rank, world, dist):
     print(json.dumps(out))
 
 
+def spawn_ranks(n):
+    """Run this command again as n ranks under torch.distributed.run (local
+    rendezvous on 127.0.0.1, a free port, a hard time limit well above the
+    process group's own timeout) and exit with its status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    sys.exit(subprocess.run(cmd).returncode)
+
+
 def main():
     global AXIAL, WORKLOAD
     args = parse()
     AXIAL = args.axial
     if AXIAL != 160:
         WORKLOAD = f"taylor3d-copper-ogrid-{960 * AXIAL}-hex8"
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # --gpus N without a launcher: start the N ranks here (one process per GPU)
+        spawn_ranks(args.gpus)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but the launcher started {world} ranks")
     if args.impl == "reference":
-        run_reference_arm(args, rank)
+        run_reference_arm(args, rank, world)
         return
     dist = None
     if world > 1:
-        # one process per GPU: this rank sees only its own device
-        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+        # one process per GPU: this rank sees only its own device, the
+        # local_rank-th of the devices the launcher gave the job (the engine
+        # creates its handles on the current device, device 0 of what it sees)
+        visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if visible:
+            ids = [x for x in visible.split(",") if x.strip()]
+            if local >= len(ids):
+                sys.exit(f"bench.py: local rank {local} but CUDA_VISIBLE_DEVICES lists {len(ids)} devices")
+            os.environ["CUDA_VISIBLE_DEVICES"] = ids[local].strip()
+        else:
+            os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
         import datetime
         import torch
         import torch.distributed as tdist

@@ -115,18 +115,38 @@ __global__ void k_sp_clear(Args a)
     s.count[i] = 0;
 }
 
+// Node slot counts.  The connectivity is the caller's device array: an entry
+// outside [0, n_nodes) is not counted, and the call reports DNL_ERR_ARG with
+// the element in the control block; the kernels after this one then leave at
+// once, so no index taken from the connectivity reaches memory unchecked.
 __global__ void k_sp_count(Args a)
 {
   Scratch s = carve(a.scratch);
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < a.nE * a.npe)
-    atomicAdd(&s.count[a.conn[k] + 1], 1);
+  if (k >= a.nE * a.npe)
+    return;
+  const int n = a.conn[k];
+  if ((unsigned)n < (unsigned)a.nN)
+    atomicAdd(&s.count[n + 1], 1);
+  else
+    raise_status(s.ctl, DNL_ERR_ARG, k / a.npe);
+}
+
+// true once k_sp_count has found a connectivity entry out of range.  Only
+// k_sp_count sets DNL_ERR_ARG, and it completes before the kernels that test
+// it start, so every thread of a launch reads the same answer (the element
+// kernel may raise other codes while it runs; those do not stop the pass).
+__device__ __forceinline__ bool bad_input(const Scratch &s)
+{
+  return *(volatile int *)&s.ctl->status == DNL_ERR_ARG;
 }
 
 // exclusive offsets of the node slot lists (one block)
 __global__ void k_sp_scan(Args a)
 {
   Scratch s = carve(a.scratch);
+  if (bad_input(s))
+    return;
   __shared__ int part[1024];
   const int n = a.nN + 1, t = threadIdx.x, per = (n + blockDim.x - 1) / blockDim.x;
   const int b = t * per, e = min(n, b + per);
@@ -161,7 +181,7 @@ __global__ void k_sp_fill(Args a)
 {
   Scratch s = carve(a.scratch);
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < a.nE * a.npe)
+  if (k < a.nE * a.npe && !bad_input(s))
     s.list[atomicAdd(&s.cursor[a.conn[k]], 1)] = k;
 }
 
@@ -170,7 +190,7 @@ __global__ void k_sp_sort(Args a)
 {
   Scratch s = carve(a.scratch);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nN)
+  if (i >= a.nN || bad_input(s))
     return;
   int *L = s.list + s.count[i];
   const int n = s.count[i + 1] - s.count[i];
@@ -197,7 +217,7 @@ template <int NPE> __global__ void __launch_bounds__(TILE) k_sp_element(Args a)
   const int g = lane & (NPE - 1);
   const int base = lane & ~(NPE - 1);
   const int e = q / NPE;
-  const bool act = e < a.nE;
+  const bool act = e < a.nE && !bad_input(s);
   const unsigned amask = __ballot_sync(0xffffffffu, act);
   if (!act)
     return;
@@ -212,7 +232,7 @@ __global__ void k_sp_gather(Args a)
 {
   Scratch s = carve(a.scratch);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nN)
+  if (i >= a.nN || bad_input(s))
     return;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   for (int k = s.count[i]; k < s.count[i + 1]; k++)
@@ -327,8 +347,9 @@ extern "C" int dnl_element_pass_static(int32_t elem_type, int32_t n_nodes, int32
   }
   if (status != 0)
   {
-    dnl_internal_set_error(status == DNL_ERR_NEG_JACOBIAN ? "dnl_element_pass_static: negative Jacobian"
-                                                          : "dnl_element_pass_static: radial return failed");
+    dnl_internal_set_error(status == DNL_ERR_ARG ? "dnl_element_pass_static: connectivity entry outside [0, n_nodes)"
+                           : status == DNL_ERR_NEG_JACOBIAN ? "dnl_element_pass_static: negative Jacobian"
+                                                            : "dnl_element_pass_static: radial return failed");
     return status;
   }
   return DNL_OK;

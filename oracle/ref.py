@@ -24,6 +24,21 @@ def available():
     return os.path.exists(LIB)
 
 
+def reference_dir():
+    """The reference checkout (its Samples/ and Sources/): the environment
+    variable DNL_REFERENCE, else the default of oracle/Makefile.  None when
+    the directory does not exist (the prebuilt oracle/_ref still works)."""
+    import subprocess
+    d = os.environ.get("DNL_REFERENCE")
+    if not d:
+        try:
+            d = subprocess.run(["make", "-s", "-C", HERE, "ref-dir"], capture_output=True, text=True,
+                               check=True).stdout.strip()
+        except (OSError, subprocess.CalledProcessError):
+            d = None
+    return d if d and os.path.isdir(d) else None
+
+
 def lib():
     global _lib
     if _lib is None:

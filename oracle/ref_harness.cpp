@@ -159,7 +159,11 @@ void *ref_create(const dnl_model_desc *d, const char *workdir)
       return nullptr;
     }
   }
-  unsetenv("DYNELA_BIN"); // solver defaults from Solver.h, overridden below
+  // An empty DYNELA_BIN makes Settings::Settings (Settings.C:30-43) skip its
+  // configuration file: the solver keeps the defaults of Solver.h, which the
+  // harness overrides below.  (Unset, System::env returns a placeholder path
+  // and the settings loader prints an error on every model.)
+  setenv("DYNELA_BIN", "", 1);
   dynelaData = nullptr;
   m->dyn = new DynELA((char *)"ref");
   if (workdir != nullptr && cwd[0] && chdir(cwd) != 0)

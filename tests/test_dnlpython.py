@@ -13,8 +13,11 @@ import pytest
 import helpers
 from helpers import _abi, meshes
 import dnlPython as dnl
+import ref
 
-SAMPLES = "/root/reference/Samples"
+# the reference's sample scripts (DNL_REFERENCE, else the oracle Makefile's default)
+_REF_DIR = ref.reference_dir()
+SAMPLES = os.path.join(_REF_DIR, "Samples") if _REF_DIR else ""
 
 
 def taylor_axi_script(nr=5, nz=50, speed=287000.0, method=None, save_dir=None, precision=None):
@@ -218,7 +221,8 @@ def test_other_boundary_types():
         _same_desc(model._description()[0], ref)
 
 
-@pytest.mark.skipif(not os.path.isdir(SAMPLES), reason="reference samples not in this checkout")
+@pytest.mark.skipif(not SAMPLES or not os.path.isdir(SAMPLES),
+                    reason="the reference's Samples/ is not here (set DNL_REFERENCE to its checkout)")
 @pytest.mark.parametrize("sample,etype,count", [
     ("Taylor/Taylor-Axi/Taylor.py", _abi.ELQUA4NAX, 250),
     ("Taylor/Taylor-3D/Taylor.py", _abi.ELHEX8N3D, 4455),

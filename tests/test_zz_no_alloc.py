@@ -60,11 +60,16 @@ def test_static_pass_matches_engine_pass_twice(case):
         desc = meshes.taylor_3d(n_core=6, n_ring=4, n_axial=50, precision=_abi.PREC_FP64)
     assert desc.n_elems <= 16384
     from oracle import OracleModel
+    u = helpers.random_increment(desc, seed=32, strain=3e-3)
+    dt = 9e-9
     with OracleModel(desc) as o:
         o.init()
         ips = helpers.random_point_state(desc, o.ips(), seed=31, stress_scale=250.0)
-    u = helpers.random_increment(desc, seed=32, strain=3e-3)
-    dt = 9e-9
+        # the C oracle's element pass on the same state, increment and time step
+        o.set_ips(ips)
+        o.set_nodes(_abi.NODE_U, u)
+        o.element_pass(dt)
+        ip_orc, f_orc = o.ips(), o.nodes(_abi.NODE_FORCE)
     x, ip_ref, f_ref = _reference_pass(desc, ips, u, dt)
     # two calls in a row on the same inputs: the scratch keeps the first call's
     # contents, the second must not see them
@@ -72,6 +77,31 @@ def test_static_pass_matches_engine_pass_twice(case):
         ip_s, f_s = _static_pass(desc, x, u, ips, dt)
         assert helpers.field_errors(ip_s, ip_ref).max() < 1e-9
         assert helpers.rel_err(f_s, f_ref) < 1e-9
+        # and against the oracle, with the bounds of the engine's own parity tests
+        assert helpers.field_errors(ip_s, ip_orc).max() < 1e-9
+        assert helpers.rel_err(f_s, f_orc) < 1e-9
+
+
+def test_static_pass_rejects_connectivity_out_of_range():
+    """A connectivity entry outside [0, n_nodes) (here n_nodes itself, and -1)
+    is caught on the device before any node is read through it: the call
+    returns DNL_ERR_ARG and a following call on valid input works."""
+    desc = helpers.case_hex_small()
+    from oracle import OracleModel
+    with OracleModel(desc) as o:
+        o.init()
+        ips = helpers.random_point_state(desc, o.ips(), seed=41)
+    u = helpers.random_increment(desc, seed=42)
+    x = desc.coords
+    lib = _abi.load_library()
+    for bad in (desc.n_nodes, -1):
+        conn = desc.conn.copy()
+        conn[desc.n_elems // 2, 3] = bad
+        with pytest.raises(AssertionError, match="connectivity entry outside"):
+            _static_pass(desc.copy(conn=conn), x, u, ips, 5e-9)
+        assert "connectivity entry outside" in lib.dnl_engine_last_error(None).decode()
+    ip_s, f_s = _static_pass(desc, x, u, ips, 5e-9)
+    assert np.isfinite(ip_s).all() and np.abs(f_s).max() > 0
 
 
 def test_static_pass_rejects_sizes_beyond_its_scratch():
