@@ -2308,6 +2308,120 @@ __global__ void __launch_bounds__(TILE) k_power_iteration(DevModel M, int force)
 
 // ------------------------------------------------------- state read-back
 
+// Nodal vector `field` (DNL_NODE_*) of node i, on the parity of the two-buffer
+// fields of the node's instance (field0 = the current values; the _PREV
+// fields the other buffer, the values before the last increment).
+__device__ __forceinline__ double4 node_vec(const DevModel &M, int field, int i)
+{
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
+  const int f0 = M.ctl[inst].f0;
+  double4 v = make_double4(0, 0, 0, 0);
+  switch (field)
+  {
+  case DNL_NODE_COORDS: v = M.x[i]; break;
+  case DNL_NODE_DISP: v = M.disp[i]; break;
+  case DNL_NODE_U: v = M.u[f0][i]; break;
+  case DNL_NODE_SPEED: v = M.v[f0][i]; break;
+  case DNL_NODE_ACCEL: v = M.a[f0][i]; break;
+  case DNL_NODE_SPEED_PREV: v = M.v[1 - f0][i]; break;
+  case DNL_NODE_U_PREV: v = M.u[1 - f0][i]; break;
+  case DNL_NODE_ACCEL_PREV: v = M.a[1 - f0][i]; break;
+  case DNL_NODE_FORCE: v = M.fout[i]; break;
+  case DNL_NODE_MASS: v.x = v.y = v.z = M.mass[i]; break;
+  default: break;
+  }
+  return v;
+}
+
+// Nodal vector `field` of nodes [n0, n0 + n) as [n][3] FP64 (the layout of
+// dnl_engine_get_nodes), packed on the device so that one copy brings it out.
+__global__ void k_nodes_out(DevModel M, int field, int n0, int n, double *dst)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n)
+    return;
+  const double4 v = node_vec(M, field, n0 + k);
+  dst[3 * k] = v.x;
+  dst[3 * k + 1] = v.y;
+  dst[3 * k + 2] = v.z;
+}
+
+// Incidence (e * npe + local node) of each force slot: the inverse of slot_pos.
+__global__ void k_slot_incidence(DevModel M, int *slot_inc)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < M.nIP)
+    slot_inc[M.slot_pos[k]] = k;
+}
+
+// Weight of Gauss point g's value at local node n (ElementData
+// integrationPointsToNode, ElHex8N3D.C:40-90, ElQua4NAx.C:37-58): the
+// shape function of g's corner of the sub-element whose corners are the
+// Gauss points (local coordinates +-1/sqrt3), evaluated at node n, i.e.
+// prod_k (1 + sqrt3 s_k(n) s_k(g)) / 2 over the element's axes.  It depends
+// only on the number m of axes on which n and g lie on the same side.
+template <int NPE> __device__ __forceinline__ double extrapolation_weight(int n, int g)
+{
+  constexpr int DIM = NPE == 8 ? 3 : 2;
+  const double r3 = 1.7320508075688772935; // sqrt(3)
+  int m = 0;
+#pragma unroll
+  for (int k = 0; k < DIM; k++)
+    m += node_sign(n, k) == node_sign(g, k);
+  if constexpr (NPE == 8)
+    return m == 3 ? (5.0 + 3.0 * r3) / 4 : m == 2 ? (-1.0 - r3) / 4 : m == 1 ? (-1.0 + r3) / 4 : (5.0 - 3.0 * r3) / 4;
+  else
+    return m == 2 ? 1.0 + r3 / 2 : m == 1 ? -0.5 : 1.0 - r3 / 2;
+}
+
+// Nodal values of point-state quantities as the reference extracts them for
+// its node fields and result files (Node::fieldScalar / fieldSymTensor2,
+// Node.C:244-365): at node i, the sum over its elements (in element order)
+// and their Gauss points of extrapolation_weight * value, divided by the
+// number of elements.  comps.c[j]: a point-state component DNL_IP_*, or
+// DNL_NODE_AVG_VON_MISES (the von Mises stress of each point, dnlVonMises,
+// Macros.h:71).  One thread per (component, node); dst [comps.n][nN].
+struct AvgComps
+{
+  static constexpr int MAX = 32;
+  int n;
+  int c[MAX];
+};
+template <typename R, int NPE>
+__global__ void k_node_average(DevModel M, const int *slot_inc, AvgComps comps, double *dst)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)comps.n * M.nN)
+    return;
+  const int j = (int)(t / M.nN), i = (int)(t % M.nN);
+  const int comp = comps.c[j];
+  const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
+  double acc = 0.0;
+  for (int k = kb; k < ke; k++)
+  {
+    const int inc = slot_inc[k];
+    const int e = inc / NPE, loc = inc % NPE;
+#pragma unroll
+    for (int g = 0; g < NPE; g++)
+    {
+      const int q = e * NPE + g;
+      double v;
+      if (comp == DNL_NODE_AVG_VON_MISES)
+      {
+        const double s1 = ipv<R>(M, DNL_IP_STRESS + 0, q), s2 = ipv<R>(M, DNL_IP_STRESS + 3, q),
+                     s3 = ipv<R>(M, DNL_IP_STRESS + 5, q), s4 = ipv<R>(M, DNL_IP_STRESS + 1, q),
+                     s5 = ipv<R>(M, DNL_IP_STRESS + 2, q), s6 = ipv<R>(M, DNL_IP_STRESS + 4, q);
+        v = sqrt(((s1 - s2) * (s1 - s2) + (s1 - s3) * (s1 - s3) + (s2 - s3) * (s2 - s3) +
+                  6.0 * (s4 * s4 + s5 * s5 + s6 * s6)) / 2);
+      }
+      else
+        v = (double)ipv<R>(M, comp, q);
+      acc = __dadd_rn(acc, __dmul_rn(extrapolation_weight<NPE>(loc, g), v));
+    }
+  }
+  dst[t] = acc / (double)(ke - kb);
+}
+
 // Components [c0, c0 + nc) of the point state, tile-major in R, to a
 // component-major FP64 array (the layout of dnl_engine_get_ips).
 template <typename R> __global__ void k_ips_out(DevModel M, int c0, int nc, double *dst)
@@ -2345,22 +2459,7 @@ __global__ void k_gather_items(DevModel M, const int4 *items, const long long *o
     o[0] = kin[3 * ((it.y == DNL_NODE_SPEED_PREV ? M.nInst : 0) + it.z)];
     return;
   }
-  const int i = it.z;
-  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
-  const int f0 = M.ctl[inst].f0;
-  double4 v = make_double4(0, 0, 0, 0);
-  switch (it.y)
-  {
-  case DNL_NODE_COORDS: v = M.x[i]; break;
-  case DNL_NODE_DISP: v = M.disp[i]; break;
-  case DNL_NODE_U: v = M.u[f0][i]; break;
-  case DNL_NODE_SPEED: v = M.v[f0][i]; break;
-  case DNL_NODE_ACCEL: v = M.a[f0][i]; break;
-  case DNL_NODE_SPEED_PREV: v = M.v[1 - f0][i]; break;
-  case DNL_NODE_FORCE: v = M.fout[i]; break;
-  case DNL_NODE_MASS: v.x = v.y = v.z = M.mass[i]; break;
-  default: break;
-  }
+  const double4 v = node_vec(M, it.y, it.z);
   o[0] = v.x;
   o[1] = v.y;
   o[2] = v.z;

@@ -67,6 +67,10 @@ struct dnl_engine
   long long *ditemOff = nullptr;
   double *dvalues = nullptr, *dkin = nullptr;
   double *hvalues = nullptr; // pinned
+  // read-back staging on the device, kept from call to call (grown on demand)
+  void *dstage = nullptr;
+  size_t stageBytes = 0;
+  int *dslotInc = nullptr; // incidence of each force slot (node averages)
   std::string err;
 };
 
@@ -123,6 +127,27 @@ int copy(dnl_engine *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind
 {
   CK(cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return DNL_OK;
+}
+
+// Device staging of the read-back entry points: allocated by the first call
+// that needs it and kept (grown when a later call needs more), so that a
+// read-back costs its kernel and its copy, not an allocation.
+int staging(dnl_engine *h, size_t bytes, void **out)
+{
+  if (bytes > h->stageBytes)
+  {
+    if (h->dstage)
+    {
+      CK(cudaStreamSynchronize(h->stream));
+      cudaFree(h->dstage);
+      h->dstage = nullptr;
+      h->stageBytes = 0;
+    }
+    CK(cudaMalloc(&h->dstage, bytes));
+    h->stageBytes = bytes;
+  }
+  *out = h->dstage;
   return DNL_OK;
 }
 
@@ -954,6 +979,8 @@ int dnl_engine_destroy(dnl_engine *h)
     cudaGraphDestroy(h->graph);
   for (void *p : h->allocs)
     cudaFree(p);
+  if (h->dstage)
+    cudaFree(h->dstage);
   free_items(h);
   if (h->hctl)
     cudaFreeHost(h->hctl);
@@ -1190,59 +1217,24 @@ int dnl_engine_get_nodes(dnl_engine *h, int32_t field, double *out)
 {
   if (!h || !out)
     return DNL_ERR_ARG;
-  int rc = sync_ctl(h);
-  if (rc)
+  if (field < DNL_NODE_COORDS || field > DNL_NODE_ACCEL_PREV)
+    return fail(h, DNL_ERR_ARG, "unknown nodal field %d", field);
+  int rc;
+  // the element slots hold the forces of the last element pass (of a run's
+  // last increment, or of dnl_engine_element_pass): assemble them now, as
+  // Model::computeInternalForces leaves them in Model::internalForces
+  if (field == DNL_NODE_FORCE && (rc = launch_gather(h, 1)))
     return rc;
-  const int f0 = h->hctl[0].f0; // node fields of all instances share the parity only for one instance
-  std::vector<double4> tmp(h->nN);
-  std::vector<double> m;
-  auto fetch = [&](const double4 *src) -> int {
-    CK(cudaMemcpyAsync(tmp.data(), src, sizeof(double4) * h->nN, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    return DNL_OK;
-  };
-  if (field == DNL_NODE_MASS)
-  {
-    m.resize(h->nN);
-    CK(cudaMemcpyAsync(m.data(), h->M.mass, sizeof(double) * h->nN, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    for (int i = 0; i < h->nN; i++)
-      out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = m[i];
-    return DNL_OK;
-  }
-  // per-instance parity of the ping-pong nodal buffers
-  std::vector<double4> alt;
-  const double4 *src = nullptr, *srcAlt = nullptr;
-  switch (field)
-  {
-  case DNL_NODE_COORDS: src = h->M.x; break;
-  case DNL_NODE_DISP: src = h->M.disp; break;
-  case DNL_NODE_U: src = h->M.u[f0]; srcAlt = h->M.u[1 - f0]; break;
-  case DNL_NODE_SPEED: src = h->M.v[f0]; srcAlt = h->M.v[1 - f0]; break;
-  case DNL_NODE_ACCEL: src = h->M.a[f0]; srcAlt = h->M.a[1 - f0]; break;
-  case DNL_NODE_SPEED_PREV: src = h->M.v[1 - f0]; srcAlt = h->M.v[f0]; break;
-  case DNL_NODE_FORCE: src = h->M.fout; break;
-  default: return fail(h, DNL_ERR_ARG, "unknown nodal field %d", field);
-  }
-  if ((rc = fetch(src)))
+  // packed to [n][3] on the device (each instance on its own buffer parity),
+  // then one copy into the caller's array
+  const size_t bytes = sizeof(double) * 3 * (size_t)h->nN;
+  void *st = nullptr;
+  if ((rc = staging(h, bytes, &st)))
     return rc;
-  if (srcAlt && h->nInst > 1)
-  {
-    alt.resize(h->nN);
-    CK(cudaMemcpyAsync(alt.data(), srcAlt, sizeof(double4) * h->nN, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    for (int i = 1; i < h->nInst; i++)
-      if (h->hctl[i].f0 != f0)
-        for (int k = h->nodeBegin[i]; k < h->nodeBegin[i + 1]; k++)
-          tmp[k] = alt[k];
-  }
-  for (int i = 0; i < h->nN; i++)
-  {
-    out[3 * i] = tmp[i].x;
-    out[3 * i + 1] = tmp[i].y;
-    out[3 * i + 2] = tmp[i].z;
-  }
-  return DNL_OK;
+  k_nodes_out<<<(h->nN + 255) / 256, 256, 0, h->stream>>>(h->M, field, 0, h->nN, (double *)st);
+  CK(cudaGetLastError());
+  h->launches++;
+  return copy(h, out, st, bytes, cudaMemcpyDeviceToHost);
 }
 
 int dnl_engine_set_nodes(dnl_engine *h, int32_t field, const double *in)
@@ -1292,8 +1284,9 @@ int dnl_engine_get_ips(dnl_engine *h, double *out)
   const size_t n = (size_t)h->nIP;
   const int group = 4;
   double *stage = nullptr;
-  CK(cudaMalloc((void **)&stage, sizeof(double) * n * group));
-  int rc = DNL_OK;
+  int rc = staging(h, sizeof(double) * n * group, (void **)&stage);
+  if (rc)
+    return rc;
   for (int c0 = 0; c0 < DNL_IP_NCOMP && rc == DNL_OK; c0 += group)
   {
     const int nc = std::min(group, DNL_IP_NCOMP - c0);
@@ -1309,8 +1302,264 @@ int dnl_engine_get_ips(dnl_engine *h, double *out)
     else
       rc = copy(h, out + (size_t)c0 * n, stage, sizeof(double) * n * nc, cudaMemcpyDeviceToHost);
   }
-  cudaFree(stage);
   return rc;
+}
+
+namespace
+{
+// Device side of dnl_engine_node_averages: n components into dst [n][nN].
+int node_averages_dev(dnl_engine *h, const int32_t *comps, int n, double *dst)
+{
+  for (int k = 0; k < n; k++)
+    if (!((comps[k] >= 0 && comps[k] < DNL_IP_NCOMP) || comps[k] == DNL_NODE_AVG_VON_MISES))
+      return fail(h, DNL_ERR_ARG, "node average of unknown component %d", comps[k]);
+  int rc;
+  if (!h->dslotInc)
+  {
+    if ((rc = dalloc(h, &h->dslotInc, h->nIP)))
+      return rc;
+    k_slot_incidence<<<(h->nIP + 255) / 256, 256, 0, h->stream>>>(h->M, h->dslotInc);
+    h->launches++;
+  }
+  for (int b = 0; b < n; b += AvgComps::MAX)
+  {
+    AvgComps ac;
+    ac.n = std::min(AvgComps::MAX, n - b);
+    for (int k = 0; k < ac.n; k++)
+      ac.c[k] = comps[b + k];
+    const long long items = (long long)ac.n * h->nN;
+    const unsigned blocks = (unsigned)((items + 255) / 256);
+    double *o = dst + (size_t)b * h->nN;
+    const bool f32 = h->precision == DNL_PREC_MIXED;
+    if (h->npe == 8)
+      f32 ? k_node_average<float, 8><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o)
+          : k_node_average<double, 8><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o);
+    else
+      f32 ? k_node_average<float, 4><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o)
+          : k_node_average<double, 4><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o);
+    CK(cudaGetLastError());
+    h->launches++;
+  }
+  return DNL_OK;
+}
+
+// The reference's VTK labels (Field.C:17-48) of the DNL_VTK_* fields, their kind
+// (0 scalar, 1 vector, 2 tensor) and source: a nodal field DNL_NODE_* for
+// the vectors (and the mass), a point-state component for the others.
+struct VtkField
+{
+  const char *label;
+  int kind;
+  int node;  // DNL_NODE_* (current), or -1
+  int prev;  // DNL_NODE_* read when prev = 1
+  int comp;  // DNL_IP_* (first of 6 for a tensor) or DNL_NODE_AVG_VON_MISES, or -1
+};
+const VtkField kVtkFields[DNL_VTK_NFIELDS] = {
+    {"coords", 1, DNL_NODE_COORDS, DNL_NODE_COORDS, -1},
+    {"disp", 1, DNL_NODE_DISP, DNL_NODE_DISP, -1},
+    {"dispInc", 1, DNL_NODE_U, DNL_NODE_U_PREV, -1},
+    {"speed", 1, DNL_NODE_SPEED, DNL_NODE_SPEED_PREV, -1},
+    {"speedInc", 1, DNL_NODE_ACCEL, DNL_NODE_ACCEL_PREV, -1},
+    {"density", 0, -1, -1, DNL_IP_DENSITY},
+    {"gamma", 0, -1, -1, DNL_IP_GAMMA},
+    {"gammaCumulate", 0, -1, -1, DNL_IP_GAMMA_CUM},
+    {"internalEnergy", 0, -1, -1, DNL_IP_EINT},
+    {"plasticStrain", 0, -1, -1, DNL_IP_EPSP},
+    {"plasticStrainRate", 0, -1, -1, DNL_IP_DEPSP},
+    {"pressure", 0, -1, -1, DNL_IP_PRESSURE},
+    {"T", 0, -1, -1, DNL_IP_T},
+    {"vonMises", 0, -1, -1, DNL_NODE_AVG_VON_MISES},
+    {"yield", 0, -1, -1, DNL_IP_YIELD},
+    {"mass", 0, DNL_NODE_MASS, DNL_NODE_MASS, -1},
+    {"PlasticStrain", 2, -1, -1, DNL_IP_PLASTIC_STRAIN},
+    {"Strain", 2, -1, -1, DNL_IP_STRAIN},
+    {"Stress", 2, -1, -1, DNL_IP_STRESS},
+};
+
+// Text output buffer: numbers printed as std::ostream prints a double by
+// default (%g, 6 significant digits).
+struct Text
+{
+  std::string s;
+  char tmp[64];
+  void num(double v)
+  {
+    const int k = snprintf(tmp, sizeof(tmp), "%g", v);
+    s.append(tmp, (size_t)k);
+  }
+  void num(long v) { s += std::to_string(v); }
+  void str(const char *t) { s += t; }
+};
+} // namespace
+
+int dnl_engine_node_averages(dnl_engine *h, const int32_t *comps, int32_t n, double *out)
+{
+  if (!h || !comps || !out || n <= 0)
+    return DNL_ERR_ARG;
+  void *st = nullptr;
+  int rc;
+  if ((rc = staging(h, sizeof(double) * (size_t)n * h->nN, &st)) ||
+      (rc = node_averages_dev(h, comps, n, (double *)st)))
+    return rc;
+  return copy(h, out, st, sizeof(double) * (size_t)n * h->nN, cudaMemcpyDeviceToHost);
+}
+
+int dnl_engine_write_vtk(dnl_engine *h, int32_t inst, const char *path, const char *title, const int32_t *fields,
+                         int32_t n_fields, int32_t prev)
+{
+  if (!h || !path || (n_fields > 0 && !fields) || n_fields < 0)
+    return DNL_ERR_ARG;
+  if (inst < 0 || inst >= h->nInst)
+    return fail(h, DNL_ERR_ARG, "instance %d out of range", inst);
+  for (int k = 0; k < n_fields; k++)
+    if (fields[k] < 0 || fields[k] >= DNL_VTK_NFIELDS)
+      return fail(h, DNL_ERR_ARG, "unknown result field %d", fields[k]);
+  int rc = sync_ctl(h);
+  if (rc)
+    return rc;
+  const int n0 = h->nodeBegin[inst], nn = h->nodeBegin[inst + 1] - n0;
+  const int e0 = h->elemBegin[inst], ne = h->elemBegin[inst + 1] - e0;
+  // device columns: coordinates, then the nodal vectors, then the averages
+  std::vector<int> nodeFields{DNL_NODE_COORDS};
+  std::vector<int32_t> comps;
+  std::vector<int> col(n_fields, -1); // first column (vector index or component index) of each field
+  for (int k = 0; k < n_fields; k++)
+  {
+    const VtkField &f = kVtkFields[fields[k]];
+    if (f.node >= 0)
+    {
+      col[k] = (int)nodeFields.size();
+      nodeFields.push_back(prev ? f.prev : f.node);
+    }
+    else
+    {
+      col[k] = (int)comps.size();
+      for (int c = 0; c < (f.kind == 2 ? 6 : 1); c++)
+        comps.push_back(f.comp + c);
+    }
+  }
+  const size_t vecBytes = sizeof(double) * 3 * (size_t)nn * nodeFields.size();
+  const size_t avgBytes = sizeof(double) * (size_t)h->nN * comps.size();
+  const size_t connBytes = sizeof(int) * (size_t)ne * h->npe;
+  void *st = nullptr;
+  if ((rc = staging(h, vecBytes + avgBytes + connBytes, &st)))
+    return rc;
+  double *dvec = (double *)st, *davg = (double *)((char *)st + vecBytes);
+  for (size_t v = 0; v < nodeFields.size(); v++)
+  {
+    k_nodes_out<<<(nn + 255) / 256, 256, 0, h->stream>>>(h->M, nodeFields[v], n0, nn, dvec + v * 3 * (size_t)nn);
+    CK(cudaGetLastError());
+    h->launches++;
+  }
+  if (!comps.empty() && (rc = node_averages_dev(h, comps.data(), (int)comps.size(), davg)))
+    return rc;
+  std::vector<double> vec(3 * (size_t)nn * nodeFields.size()), avg((size_t)h->nN * comps.size());
+  std::vector<int> conn((size_t)ne * h->npe);
+  CK(cudaMemcpyAsync(vec.data(), dvec, vecBytes, cudaMemcpyDeviceToHost, h->stream));
+  if (!comps.empty())
+    CK(cudaMemcpyAsync(avg.data(), davg, avgBytes, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(conn.data(), h->M.conn + (size_t)e0 * h->npe, connBytes, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+
+  // VtkInterface::headerWrite / nodesWrite / elementsWrite / dataWrite
+  Text o;
+  o.s.reserve(64 * (size_t)nn * (1 + n_fields) + 32 * (size_t)ne);
+  o.str("# vtk DataFile Version 4.0\n");
+  o.str(title ? title : "");
+  o.str("\nASCII\nDATASET UNSTRUCTURED_GRID\nFIELD FieldData 1\nTIME 1 1 double\n");
+  o.num(h->hctl[inst].t);
+  o.str("\nPOINTS ");
+  o.num((long)nn);
+  o.str(" float\n");
+  for (int i = 0; i < nn; i++)
+  {
+    o.num(vec[3 * (size_t)i]);
+    o.str(" ");
+    o.num(vec[3 * (size_t)i + 1]);
+    o.str(" ");
+    o.num(vec[3 * (size_t)i + 2]);
+    o.str("\n");
+  }
+  o.str("\nCELLS ");
+  o.num((long)ne);
+  o.str(" ");
+  o.num((long)ne * (h->npe + 1));
+  o.str("\n");
+  for (int e = 0; e < ne; e++)
+  {
+    o.num((long)h->npe);
+    o.str(" ");
+    for (int j = 0; j < h->npe; j++)
+    {
+      o.num((long)(conn[(size_t)e * h->npe + j] - n0));
+      o.str(" ");
+    }
+    o.str("\n");
+  }
+  o.str("\nCELL_TYPES ");
+  o.num((long)ne);
+  o.str("\n");
+  const char *vtkType = h->npe == 8 ? "12\n" : "9\n"; // VTK_HEXAHEDRON, VTK_QUAD (ElementData vtkType)
+  for (int e = 0; e < ne; e++)
+    o.str(vtkType);
+  o.str("\nPOINT_DATA ");
+  o.num((long)nn);
+  o.str("\n");
+  for (int k = 0; k < n_fields; k++)
+  {
+    const VtkField &f = kVtkFields[fields[k]];
+    if (f.kind == 1)
+    {
+      const double *v = vec.data() + (size_t)col[k] * 3 * nn;
+      o.str("VECTORS ");
+      o.str(f.label);
+      o.str(" float\n");
+      for (int i = 0; i < nn; i++)
+      {
+        o.num(v[3 * (size_t)i]);
+        o.str(" ");
+        o.num(v[3 * (size_t)i + 1]);
+        o.str(" ");
+        o.num(v[3 * (size_t)i + 2]);
+        o.str("\n");
+      }
+    }
+    else if (f.kind == 0)
+    {
+      o.str("SCALARS ");
+      o.str(f.label);
+      o.str(" float\nLOOKUP_TABLE default\n");
+      for (int i = 0; i < nn; i++)
+      {
+        // the mass is a nodal vector (repeated on its components), the others node averages
+        o.num(f.node >= 0 ? vec[(size_t)col[k] * 3 * nn + 3 * (size_t)i]
+                          : avg[(size_t)col[k] * h->nN + n0 + i]);
+        o.str("\n");
+      }
+    }
+    else
+    {
+      o.str("TENSORS ");
+      o.str(f.label);
+      o.str(" float\n");
+      static const int full[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5}; // (i, j) -> xx, xy, xz, yy, yz, zz
+      for (int i = 0; i < nn; i++)
+        for (int c = 0; c < 9; c++)
+        {
+          o.num(avg[(size_t)(col[k] + full[c]) * h->nN + n0 + i]);
+          o.str(c == 8 ? "\n" : " ");
+        }
+    }
+  }
+  o.str("\n");
+  FILE *fp = fopen(path, "wb");
+  if (!fp)
+    return fail(h, DNL_ERR_ARG, "cannot open %s for writing", path);
+  const size_t w = fwrite(o.s.data(), 1, o.s.size(), fp);
+  const int cl = fclose(fp);
+  if (w != o.s.size() || cl != 0)
+    return fail(h, DNL_ERR_ARG, "writing %s failed", path);
+  return DNL_OK;
 }
 
 int dnl_engine_set_ips(dnl_engine *h, const double *in)

@@ -21,8 +21,9 @@ Scope of the mirror: the elements ElQua4NAx, ElQua4N2D and ElHex8N3D, the Johnso
 law, BoundaryRestrain / BoundarySpeed (+ DiscreteFunction / RampFunction time
 functions) and the other boundary types with the reference's behaviour on the
 explicit path (no effect, or a stop for a constant displacement or force), the Explicit solver with the Courant and power-iteration time
-steps, and HistoryFile.  SvgInterface and the VTK result files are accepted
-and skipped (the reference writes them on the host at save times).
+steps, HistoryFile, and the VTK result files of DynELA::setSaveTimes (written
+by the engine library: the fields are extracted at the nodes on the device).
+SvgInterface is accepted and skipped.
 """
 import math
 import os
@@ -36,7 +37,7 @@ __all__ = ["DynELA", "NodeSet", "ElementSet", "Material", "JohnsonCookLaw", "Bou
            "BoundaryDisplacement", "BoundaryForce", "BoundaryAcceleration", "BoundaryTemperature",
            "BoundaryConvection", "BoundaryFlux",
            "DiscreteFunction", "RampFunction", "Explicit", "HistoryFile", "Field", "Element", "Vec3D",
-           "SvgInterface", "Parallel"]
+           "SvgInterface", "Parallel", "VtkInterface"]
 
 
 class Vec3D:
@@ -435,6 +436,47 @@ class Node:
         return float(self._row(_abi.NODE_MASS)[0])
 
 
+class VtkInterface:
+    """The fields of the result files (VtkInterface, VtkInterface.C:224-278):
+    initially those of the reference's settings file (VtkFields) that it
+    recognises; addField / removeField take dnl.Field codes."""
+
+    # Sources/dnlSettings/configuration.dnl VtkFields, as Field::getField reads them
+    DEFAULT = ["Stress", "Strain", "PlasticStrain", "vonMises", "yield", "pressure", "plasticStrain",
+               "plasticStrainRate", "gamma", "gammaCumulate", "speed"]
+
+    def __init__(self, name=None):
+        self.name = name or "VtkInterface::_noname_"
+        self.fields = list(self.DEFAULT)
+
+    def initFields(self):
+        self.fields = list(self.DEFAULT)
+
+    @staticmethod
+    def _label(field):
+        label = Field.label(field) if isinstance(field, int) else str(field)
+        if label not in _abi.VTK_FIELDS:
+            raise ValueError(f"field {label} cannot be written to a result file")
+        return label
+
+    def existField(self, field):
+        label = self._label(field)
+        return self.fields.index(label) if label in self.fields else -1
+
+    def addField(self, field):
+        label = self._label(field)
+        if label not in self.fields:
+            self.fields.append(label)
+
+    def removeField(self, field):
+        label = self._label(field)
+        if label in self.fields:
+            self.fields.remove(label)
+
+    def getNumberOfFields(self):
+        return len(self.fields)
+
+
 class DynELA:
     """The model (DynELA.h:40-100)."""
 
@@ -451,7 +493,11 @@ class DynELA:
         self._histories = []
         self.solver = None
         self.parallel = Parallel()
+        # DynELA::setSaveTimes: start, end, increment (defaults of DynELA.h:36-39)
         self.saveTimes = (0.0, 0.0, 0.0)
+        self.dataFile = VtkInterface()
+        self._vtk_index = 0
+        self._next_save = 0.0
         self.precision = _abi.PREC_MIXED if os.environ.get("DNL_PRECISION", "fp64") == "mixed" else _abi.PREC_FP64
         self.stress_method = _abi.STRESS_NEWTON
         self._engine = None
@@ -530,7 +576,10 @@ class DynELA:
         self._initial_bcs.append((bc, nodeSet))
 
     def setSaveTimes(self, start, end, inc):
+        """DynELA::setSaveTimes (DynELA.C:479-487): result files from `start`
+        to `end` every `inc` (the next save time starts at `start`)."""
         self.saveTimes = (float(start), float(end), float(inc))
+        self._next_save = float(start)
 
     def setStressComputation(self, method):
         """DynELA::setStressComputation (DynELA.C:1407-1431): "NewtonRaphson"
@@ -641,26 +690,56 @@ class DynELA:
                        + "\n")
         self._plan_items()
         self._write_histories(initial=True)
+        self._vtk_index = 0
+        # the initial result file (DynELA::solve -> writeResultFile after initSolve, DynELA.C:745)
+        self._write_result_file(prev=False)
         t_end = desc.t_end
         while True:
             c = eng.control()
             if c["done"] or c["time"] >= t_end:
                 break
-            if any(h.saveTime > 0 and h.nextTime <= c["time"] for h in self._histories):
+            t = c["time"]
+            if any(h.saveTime > 0 and h.nextTime <= t for h in self._histories) or self._result_due(t):
                 # an increment passed more than one save time: the reference writes
                 # again after the next increment (its next time lags behind)
                 eng.run(t_pause=t_end, max_incs=1)
             else:
                 pauses = [h.nextTime for h in self._histories if h.saveTime > 0]
+                if self._next_save <= self.saveTimes[1]:
+                    pauses.append(self._next_save)
                 eng.run(t_pause=min(pauses) if pauses else t_end)
             self._cache = {}
             self._write_histories()
+            self._write_result_file(prev=True)
         c = eng.control()
         print(f"{self.name} inc={c['increment']} time={c['time']:8.4E} timeStep={c['time_step']:8.4E}")
         for h in self._histories:
             h._f.close()
             h._f = None
+        # the final result file (DynELA::solve -> writeVTKFile, DynELA.C:770)
+        self._write_vtk(prev=False)
         return True
+
+    # ---- result files (DynELA::writeResultFile / writeVTKFile, DynELA.C:489-504, 688-711)
+    def _result_due(self, t):
+        return t >= self._next_save and t <= self.saveTimes[1]
+
+    def _write_result_file(self, prev):
+        """At the end of an increment (Explicit::endStep, before the field
+        swap, hence the nodal increments, speeds and accelerations of before
+        it: prev) or at the start: a file when the time has reached the next
+        save time and not passed the last one; the next save time then moves
+        on by one increment of save time."""
+        if self._result_due(self._engine.control()["time"]):
+            self._write_vtk(prev)
+            self._next_save += self.saveTimes[2]
+
+    def _write_vtk(self, prev):
+        path = f"{self.name}{self._vtk_index:03d}.vtk"
+        t = self._engine.control()["time"]
+        self._engine.write_vtk(path, self.dataFile.fields, prev=prev)
+        print(f"Write VTK result file: {path} at time {t:g} s")
+        self._vtk_index += 1
 
     @staticmethod
     def _make_engine(desc):
@@ -693,7 +772,11 @@ class DynELA:
                 return [(_abi.ITEM_KINETIC, _abi.NODE_SPEED, 0), (_abi.ITEM_KINETIC, _abi.NODE_SPEED_PREV, 0)]
             return []
         if kind == "node":
-            return [(_abi.ITEM_NODE, self._node_item(field)[0], self._node_index[target])]
+            f = self._node_item(field)[0]
+            keys = [(_abi.ITEM_NODE, f, self._node_index[target])]
+            if f in _abi.NODE_PREV:
+                keys.append((_abi.ITEM_NODE, _abi.NODE_PREV[f], self._node_index[target]))
+            return keys
         e = self._elem_index[target]
         qs = range(e * self._npe, (e + 1) * self._npe) if ip < 0 else [e * self._npe + ip]
         return [(_abi.ITEM_POINT, 0, q) for q in qs]
@@ -736,6 +819,10 @@ class DynELA:
             return 0.0
         if kind == "node":
             f, suf = self._node_item(field)
+            # inside the loop the reference writes before its field swap
+            # (Explicit.C:539-552): field0 is then the start of the increment
+            if f in _abi.NODE_PREV and eng.control()["increment"] > 0:
+                f = _abi.NODE_PREV[f]
             row = self._gathered((_abi.ITEM_NODE, f, self._node_index[target]))
             return float(np.linalg.norm(row)) if suf == "" else float(row["XYZ".index(suf)])
         return float(np.mean([self._ip_value(self._gathered(k), field)

@@ -47,6 +47,19 @@ IP_PRESSURE, IP_EINT, IP_EINEL, IP_DENSITY, IP_DETJ0 = 24, 25, 26, 27, 28
 IP_NCOMP = 29
 
 NODE_COORDS, NODE_DISP, NODE_U, NODE_SPEED, NODE_ACCEL, NODE_MASS, NODE_FORCE, NODE_SPEED_PREV = range(8)
+NODE_U_PREV, NODE_ACCEL_PREV = 8, 9
+# nodal fields as the reference's writers read them inside an increment
+# (before its field swap): the buffer of before the last increment
+NODE_PREV = {NODE_U: NODE_U_PREV, NODE_SPEED: NODE_SPEED_PREV, NODE_ACCEL: NODE_ACCEL_PREV}
+
+# node averages of the point state (dnl_engine_node_averages)
+NODE_AVG_VON_MISES = 64
+
+# result-file fields (DNL_VTK_*), by the reference's VTK label (Field.C:17-48)
+VTK_FIELDS = {"coords": 0, "disp": 1, "dispInc": 2, "speed": 3, "speedInc": 4, "density": 5, "gamma": 6,
+              "gammaCumulate": 7, "internalEnergy": 8, "plasticStrain": 9, "plasticStrainRate": 10,
+              "pressure": 11, "T": 12, "vonMises": 13, "yield": 14, "mass": 15, "PlasticStrain": 16,
+              "Strain": 17, "Stress": 18}
 
 
 class EngineUnavailable(RuntimeError):
@@ -285,6 +298,9 @@ def load_library():
         "dnl_engine_energies": (ctypes.c_int, [vp, i32, pd]),
         "dnl_engine_set_items": (ctypes.c_int, [vp, ctypes.POINTER(Item), i32, ctypes.POINTER(i64)]),
         "dnl_engine_gather_items": (ctypes.c_int, [vp, pd]),
+        "dnl_engine_node_averages": (ctypes.c_int, [vp, ctypes.POINTER(i32), i32, pd]),
+        "dnl_engine_write_vtk": (ctypes.c_int, [vp, i32, ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(i32),
+                                                i32, i32]),
         "dnl_engine_set_timing": (ctypes.c_int, [vp, i32]),
         "dnl_engine_timings": (ctypes.c_int, [vp, pd]),
         "dnl_engine_launch_count": (ctypes.c_int64, [vp]),

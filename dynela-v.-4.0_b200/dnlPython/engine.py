@@ -6,6 +6,7 @@ advanced together.  There is no CPU path: construction raises
 missing.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -113,6 +114,24 @@ class Engine:
         out = np.zeros(max(1, getattr(self, "_n_values", 0)))
         self._check(self._lib.dnl_engine_gather_items(self.h, _pd(out)))
         return out[:getattr(self, "_n_values", 0)]
+
+    def node_averages(self, comps):
+        """Nodal values of point-state components (IP_* or NODE_AVG_VON_MISES)
+        as the reference extracts them for its node fields: [len(comps), n_nodes]."""
+        c = (ctypes.c_int32 * len(comps))(*[int(x) for x in comps])
+        out = np.zeros((len(comps), self.n_nodes))
+        self._check(self._lib.dnl_engine_node_averages(self.h, c, len(comps), _pd(out)))
+        return out
+
+    def write_vtk(self, path, fields, prev=False, instance=0, title="DynELA FEM Code v.4.0"):
+        """Result file of one instance in the reference's VTK format; `fields`
+        are labels of _abi.VTK_FIELDS; prev: the nodal increments, speeds and
+        accelerations of before the last increment (the reference's files
+        written inside an increment)."""
+        codes = [_abi.VTK_FIELDS[f] for f in fields]
+        c = (ctypes.c_int32 * max(1, len(codes)))(*codes)
+        self._check(self._lib.dnl_engine_write_vtk(self.h, int(instance), os.fsencode(path), title.encode(), c,
+                                                   len(codes), int(bool(prev))))
 
     def energies(self, instance=0):
         out = np.zeros(3)

@@ -85,8 +85,14 @@ enum {
   DNL_NODE_ACCEL = 4,  /* field0->acceleration */
   DNL_NODE_MASS = 5,   /* lumped mass, repeated on the 3 components */
   DNL_NODE_FORCE = 6,  /* assembled internal force of the last element pass */
-  DNL_NODE_SPEED_PREV = 7 /* field1->speed: the speed before the last increment */
+  DNL_NODE_SPEED_PREV = 7, /* field1->speed: the speed before the last increment */
+  DNL_NODE_U_PREV = 8,     /* field1->u: the displacement increment before the last increment */
+  DNL_NODE_ACCEL_PREV = 9  /* field1->acceleration: the acceleration before the last increment */
 };
+/* The _PREV fields are what the reference's writers read inside an increment:
+ * Explicit::endStep (Explicit.C:539-552) writes the history and result files
+ * before Model::transfertQuantities swaps field0 and field1, so that their
+ * field0 values are those of the start of the increment. */
 
 /* Johnson-Cook elasto-plastic material (Material.h:26-100 + JohnsonCookLaw.C:132-143). */
 typedef struct dnl_material {
@@ -232,6 +238,43 @@ typedef struct
 } dnl_item;
 int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_t *n_values);
 int dnl_engine_gather_items(dnl_engine *h, double *out);
+
+/* Nodal values of point-state quantities, extracted as the reference does for
+ * its node fields and result files (Node::fieldScalar / fieldSymTensor2,
+ * Node.C:244-365): at each node, the values of the Gauss points of every
+ * element around it, extrapolated to the node (ElementData
+ * integrationPointsToNode, ElHex8N3D.C:40-90, ElQua4NAx.C:37-58), summed
+ * and divided by the number of those elements, in FP64.  comps[k] is a
+ * point-state component DNL_IP_* or DNL_NODE_AVG_VON_MISES (the von Mises
+ * stress of each point, SymTensor2::vonMises).  out: [n][n_nodes] doubles,
+ * all instances. */
+#define DNL_NODE_AVG_VON_MISES 64
+int dnl_engine_node_averages(dnl_engine *h, const int32_t *comps, int32_t n, double *out);
+
+/* Result file of one instance in the reference's format (DynELA::writeVTKFile
+ * -> VtkInterface::write, DynELA.C:688-711, VtkInterface.C:68-221): legacy
+ * ASCII VTK unstructured grid with the title, the time, the nodes, the cells
+ * and, as point data, the fields listed (DNL_VTK_*, in the list's order),
+ * numbers printed as the reference's streams print them (6 significant
+ * digits).  prev = 1 writes the displacement increments, speeds and
+ * accelerations of before the last increment, which is what the reference's
+ * files written inside an increment hold (Explicit::endStep writes them
+ * before the field swap); prev = 0 the current ones (its initial and final
+ * files).  No counterpart for the field list's storage: the reference reads
+ * it from its settings file (VtkFields, VtkInterface::initFields). */
+enum {
+  /* nodal vectors (Node::fieldVec3D, Node.C:380-401) */
+  DNL_VTK_COORDS = 0, DNL_VTK_DISP = 1, DNL_VTK_DISP_INC = 2, DNL_VTK_SPEED = 3, DNL_VTK_SPEED_INC = 4,
+  /* point-state scalars averaged at the nodes (Node::fieldScalar) */
+  DNL_VTK_DENSITY = 5, DNL_VTK_GAMMA = 6, DNL_VTK_GAMMA_CUMULATE = 7, DNL_VTK_INTERNAL_ENERGY = 8,
+  DNL_VTK_PLASTIC_STRAIN = 9, DNL_VTK_PLASTIC_STRAIN_RATE = 10, DNL_VTK_PRESSURE = 11, DNL_VTK_T = 12,
+  DNL_VTK_VON_MISES = 13, DNL_VTK_YIELD = 14, DNL_VTK_MASS = 15,
+  /* point-state tensors averaged at the nodes (Node::fieldSymTensor2) */
+  DNL_VTK_PLASTIC_STRAIN_TENSOR = 16, DNL_VTK_STRAIN_TENSOR = 17, DNL_VTK_STRESS_TENSOR = 18,
+  DNL_VTK_NFIELDS = 19
+};
+int dnl_engine_write_vtk(dnl_engine *h, int32_t instance, const char *path, const char *title,
+                         const int32_t *fields, int32_t n_fields, int32_t prev);
 
 /* Energies of one instance, FP64 sums: [0] kinetic (Model.C:612-626, field0
  * speeds), [1] internal = sum rho0*detJ0*w*e_int (x 2 pi for axisymmetric),

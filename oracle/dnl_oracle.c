@@ -1359,6 +1359,8 @@ int orc_get_nodes(orc_model *m, int field, double *out)
   case DNL_NODE_SPEED: src = m->fv[m->f0]; break;
   case DNL_NODE_ACCEL: src = m->fa[m->f0]; break;
   case DNL_NODE_SPEED_PREV: src = m->fv[1 - m->f0]; break;
+  case DNL_NODE_U_PREV: src = m->fu[1 - m->f0]; break;
+  case DNL_NODE_ACCEL_PREV: src = m->fa[1 - m->f0]; break;
   case DNL_NODE_FORCE: src = m->fint; break;
   case DNL_NODE_MASS:
     for (long i = 0; i < m->nN; i++)

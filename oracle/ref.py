@@ -67,6 +67,8 @@ def lib():
         L.ref_timer.restype = ctypes.c_double
         L.ref_timer.argtypes = [vp, ctypes.c_char_p]
         L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_enable_vtk.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.ref_write_final_vtk.argtypes = [vp]
         L.ref_destroy.argtypes = [vp]
         _lib = L
     return _lib
@@ -135,6 +137,21 @@ class RefModel:
         wv = np.zeros(self.desc.n_elems)
         lib().ref_element_lengths(self.h, _pd(ln), _pd(wv))
         return ln, wv
+
+    @property
+    def workdir(self):
+        """Directory where the reference writes its files (ref000.vtk, ...)."""
+        return self._tmp
+
+    def enable_vtk(self, start, end, inc):
+        """The reference's own result files at its save times (written in
+        `workdir` by its Explicit::endStep during run()), the initial one now.
+        Their fields come from the reference's settings file when the model
+        was created with DNL_REF_SETTINGS set."""
+        assert lib().ref_enable_vtk(self.h, float(start), float(end), float(inc)) == 0
+
+    def write_final_vtk(self):
+        assert lib().ref_write_final_vtk(self.h) == 0
 
     def solver_seconds(self):
         return lib().ref_solver_seconds(self.h)

@@ -85,7 +85,24 @@ struct RefModel
   double tEnd = 0.0;
   double solverSeconds = 0.0;
   long loopIncrements = 0;
+  // Explicit::explicitSolve (Explicit.C:501) overwrites Model::internalForces
+  // with M^-1 f; after a run the last increment's forces are rebuilt here
+  std::vector<double> fint;
+  bool fintValid = false;
+  std::string workdir; // where the reference writes its files
+  bool vtk = false;    // result files enabled (ref_enable_vtk)
 };
+
+// Run `fn` with the working directory set to the model's (the reference
+// writes its result files in the current directory).
+template <typename F> void inWorkdir(RefModel *m, F fn)
+{
+  char cwd[4096] = "";
+  const bool move = !m->workdir.empty() && getcwd(cwd, sizeof(cwd)) != nullptr && chdir(m->workdir.c_str()) == 0;
+  fn();
+  if (move && chdir(cwd) != 0)
+    fprintf(stderr, "ref_harness: cannot return to %s\n", cwd);
+}
 
 RefModel *g_model = nullptr;
 char g_err[512] = "";
@@ -162,8 +179,15 @@ void *ref_create(const dnl_model_desc *d, const char *workdir)
   // An empty DYNELA_BIN makes Settings::Settings (Settings.C:30-43) skip its
   // configuration file: the solver keeps the defaults of Solver.h, which the
   // harness overrides below.  (Unset, System::env returns a placeholder path
-  // and the settings loader prints an error on every model.)
-  setenv("DYNELA_BIN", "", 1);
+  // and the settings loader prints an error on every model.)  DNL_REF_SETTINGS
+  // names the reference's settings directory (Sources/dnlSettings) instead,
+  // for runs that write result files: their fields and title come from it.
+  {
+    const char *sdir = getenv("DNL_REF_SETTINGS");
+    setenv("DYNELA_BIN", sdir ? sdir : "", 1);
+  }
+  if (workdir != nullptr)
+    m->workdir = workdir;
   dynelaData = nullptr;
   m->dyn = new DynELA((char *)"ref");
   if (workdir != nullptr && cwd[0] && chdir(cwd) != 0)
@@ -422,6 +446,8 @@ long ref_run(void *h, double t_stop, long max_incs)
   Explicit *s = m->solver;
   double upTo = s->_solveUpToTime;
   long k = 0;
+  char cwd[4096] = "";
+  const bool moved = m->vtk && getcwd(cwd, sizeof(cwd)) != nullptr && chdir(m->workdir.c_str()) == 0;
   auto t0 = std::chrono::steady_clock::now();
   m->dyn->cpuTimes.timer("Solver")->start();
   while (model->currentTime < upTo && model->currentTime < t_stop && (max_incs <= 0 || k < max_incs))
@@ -447,7 +473,46 @@ long ref_run(void *h, double t_stop, long max_incs)
   m->dyn->cpuTimes.timer("Solver")->stop();
   m->solverSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   m->loopIncrements += k;
+  if (moved && chdir(cwd) != 0)
+    fprintf(stderr, "ref_harness: cannot return to %s\n", cwd);
+  if (k > 0)
+  {
+    // internal forces of the last increment: M (M^-1 f), outside the timing
+    const long n = (long)m->nN * m->dim;
+    m->fint.resize(n);
+    for (long i = 0; i < n; i++)
+      m->fint[i] = model->internalForces(i) * model->massMatrix(i);
+    m->fintValid = true;
+  }
   return k;
+}
+
+/* The reference's own result files: save times set (DynELA::setSaveTimes,
+ * DynELA.C:479-487) and the initial file written now, as DynELA::solve does
+ * after initSolve (DynELA.C:745, writeResultFile, DynELA.C:489-504); the
+ * reference's Explicit::endStep then writes the files of the save times
+ * during ref_run (Explicit.C:548), as <workdir>/<model name>NNN.vtk with the
+ * fields of its settings (VtkInterface::initFields, VtkInterface.C:224-242;
+ * see DNL_REF_SETTINGS in ref_create). */
+int ref_enable_vtk(void *h, double start, double end, double inc)
+{
+  RefModel *m = (RefModel *)h;
+  if (m == nullptr || m != g_model || m->workdir.empty())
+    return DNL_ERR_ARG;
+  m->dyn->setSaveTimes(start, end, inc);
+  m->vtk = true;
+  inWorkdir(m, [&] { m->dyn->writeResultFile(); });
+  return DNL_OK;
+}
+
+/* The last result file of DynELA::solve (DynELA.C:770, writeVTKFile). */
+int ref_write_final_vtk(void *h)
+{
+  RefModel *m = (RefModel *)h;
+  if (m == nullptr || m != g_model || !m->vtk)
+    return DNL_ERR_ARG;
+  inWorkdir(m, [&] { m->dyn->writeVTKFile(); });
+  return DNL_OK;
 }
 
 /* The reference's own Explicit::solve(upTo) (pre-loop part + loop), used to pin
@@ -494,8 +559,12 @@ int ref_get_nodes(void *h, int field, double *out)
       case DNL_NODE_SPEED: v = n->field0->speed(c); break;
       case DNL_NODE_ACCEL: v = n->field0->acceleration(c); break;
       case DNL_NODE_MASS: v = n->mass; break;
-      case DNL_NODE_FORCE: v = (c < m->dim) ? model.internalForces(i * m->dim + c) : 0.0; break;
+      case DNL_NODE_FORCE:
+        v = (c >= m->dim) ? 0.0 : m->fintValid ? m->fint[i * m->dim + c] : model.internalForces(i * m->dim + c);
+        break;
       case DNL_NODE_SPEED_PREV: v = n->field1->speed(c); break;
+      case DNL_NODE_U_PREV: v = n->field1->u(c); break;
+      case DNL_NODE_ACCEL_PREV: v = n->field1->acceleration(c); break;
       default: return DNL_ERR_ARG;
       }
       out[3 * i + c] = v;
@@ -608,6 +677,7 @@ int ref_element_pass(void *h, double timeStep)
   model.computeStress(timeStep);
   model.computeFinalRotation();
   model.computeInternalForces();
+  m->fintValid = false; // Model::internalForces holds f itself
   m->solver->computeDensity();
   return DNL_OK;
 }

@@ -82,6 +82,169 @@ def published_case():
     print("taylor_axi_sample", rows)
 
 
+# ---------------------------------------------------------------- full size
+#
+# The measured workloads at their full size.  Their arrays are too large to
+# commit, so a fixture keeps (a) a seeded sample of nodes and integration
+# points with every field of them, compared entry by entry, and (b) sums over
+# every node and point of each field component (signed, absolute and the
+# largest magnitude), which catch an error anywhere in the mesh.  The mesh is
+# rebuilt by its generator (dnlPython.meshes) from the recorded arguments; a
+# digest of the coordinates and connectivity guards against a generator change.
+
+FULL_MESHES = {
+    "taylor3d_153600": ("taylor_3d", {}),
+    "bar_necking_1198080": ("bar_necking", {}),
+    "plate_necking_491520": ("plate_necking", {}),
+}
+NODE_FIELDS = (("coords", _abi.NODE_COORDS), ("disp", _abi.NODE_DISP), ("speed", _abi.NODE_SPEED),
+               ("u", _abi.NODE_U), ("accel", _abi.NODE_ACCEL), ("force", _abi.NODE_FORCE))
+
+
+def full_desc(mesh):
+    name, kw = FULL_MESHES[mesh]
+    return getattr(meshes, name)(precision=_abi.PREC_FP64, **kw)
+
+
+def full_sample(desc, n_nodes=4096, n_ips=8192, seed=20261204):
+    rng = np.random.default_rng(seed)
+    nodes = np.unique(np.concatenate([rng.choice(desc.n_nodes, min(n_nodes, desc.n_nodes), replace=False),
+                                      [0, desc.n_nodes - 1, int(np.argmax(desc.coords[:, 1]))]]))
+    ips = np.unique(np.concatenate([rng.choice(desc.n_ips, min(n_ips, desc.n_ips), replace=False),
+                                    [0, desc.n_ips - 1]]))
+    return nodes.astype(np.int64), ips.astype(np.int64)
+
+
+def full_snapshot(r, prefix, nodes, ips):
+    out = {}
+    for name, f in NODE_FIELDS:
+        a = r.nodes(f)
+        out[prefix + name] = a[nodes]
+        out[prefix + name + "_sums"] = helpers.field_sums(a)
+    ip = r.ips()
+    out[prefix + "ips"] = ip[:, ips]
+    out[prefix + "ips_sums"] = helpers.field_sums(ip.T)
+    c = r.control()
+    out[prefix + "control"] = np.array([c["time"], c["time_step"], c["increment"]])
+    return out
+
+
+def full_run_case(mesh, checkpoints, threads=None):
+    """The first increments of a full-size workload (FP64, from t = 0)."""
+    desc = full_desc(mesh)
+    nodes, ips = full_sample(desc)
+    data = {"mesh": np.array(mesh), "digest": np.array(helpers.mesh_digest(desc)), "sample_nodes": nodes,
+            "sample_ips": ips, "checkpoints": np.array(checkpoints)}
+    with ref.RefModel(desc, threads=threads or os.cpu_count()) as r:
+        r.init()
+        data.update(full_snapshot(r, "init_", nodes, ips))
+        done = 0
+        for k in checkpoints:
+            r.run(max_incs=k - done)
+            done = k
+            data.update(full_snapshot(r, f"inc{k}_", nodes, ips))
+            print(f"fullsize_{mesh}_incs: increment {k}", flush=True)
+    np.savez_compressed(os.path.join(HERE, f"fullsize_{mesh}_incs.npz"), **data)
+    print(f"fullsize_{mesh}_incs ok")
+
+
+def full_pass_case(mesh, seed, dt=4e-9, threads=None):
+    """One element pass of a full-size mesh on a seeded plastic state and
+    displacement increment (helpers.random_point_state / random_increment,
+    regenerated by the test from the same seeds)."""
+    desc = full_desc(mesh)
+    nodes, ips = full_sample(desc)
+    data = {"mesh": np.array(mesh), "digest": np.array(helpers.mesh_digest(desc)), "sample_nodes": nodes,
+            "sample_ips": ips, "seed": np.array(seed), "dt": np.array(dt)}
+    with ref.RefModel(desc, threads=threads or os.cpu_count()) as r:
+        r.init()
+        st = helpers.random_point_state(desc, r.ips(), seed)
+        u = helpers.random_increment(desc, seed + 1)
+        r.set_ips(st)
+        r.set_nodes(_abi.NODE_U, u)
+        del st, u
+        r.element_pass(dt)
+        f = r.nodes(_abi.NODE_FORCE)
+        data["out_force"] = f[nodes]
+        data["out_force_sums"] = helpers.field_sums(f)
+        ip = r.ips()
+        data["out_ips"] = ip[:, ips]
+        data["out_ips_sums"] = helpers.field_sums(ip.T)
+    np.savez_compressed(os.path.join(HERE, f"fullsize_{mesh}_elempass.npz"), **data)
+    print(f"fullsize_{mesh}_elempass ok")
+
+
+def config0_case():
+    """The axisymmetric copper bar of 10 x 80 ElQua4NAx at 227 m/s run to
+    80 us by the reference, with the power-iteration time step every
+    increment (the method of the reference's Taylor-Axi sample) and with the
+    Courant time step every 10 increments: the final nodal fields and point
+    state whole (891 nodes, 3,200 points), and the increment count."""
+    data = {}
+    for tag, method, freq in (("pi1", _abi.TS_POWER_ITERATION, 1), ("courant10", _abi.TS_COURANT, 10)):
+        d = meshes.taylor_axi(ts_method=method, ts_freq=freq, precision=_abi.PREC_FP64)
+        if tag == "pi1":
+            data.update(helpers.desc_to_npz(d))
+        with ref.RefModel(d, threads=1) as r:
+            r.init()
+            n = r.run()
+            for name, f in NODE_FIELDS[:5]:
+                data[f"{tag}_{name}"] = r.nodes(f)
+            data[f"{tag}_ips"] = r.ips()
+            c = r.control()
+            data[f"{tag}_control"] = np.array([c["time"], c["time_step"], c["increment"], n])
+        x = data[f"{tag}_coords"]
+        ep = data[f"{tag}_ips"][_abi.IP_EPSP].reshape(-1, 4).mean(1).max()
+        print(f"config0 {tag}: {n} increments, height {x[d.n_nodes - 11, 1]:.4f}, radius {x[10, 0]:.4f}, "
+              f"max element-mean eps_p {ep:.4f}", flush=True)
+    np.savez_compressed(os.path.join(HERE, "config0_whole.npz"), **data)
+
+
+def vtk_case(name, desc, n_saves):
+    """The reference's own result files (its VtkInterface, fields from its
+    settings file) for a run with setSaveTimes(0, t_end, t_end / n_saves):
+    the text of every file, and the reference's state when it wrote each one
+    (the run stops at the increment that writes a file), for the checks of
+    the restatement oracle/vtk_ref.py and of the engine's writer."""
+    sdir = os.path.join(ref.reference_dir(), "Sources", "dnlSettings")
+    os.environ["DNL_REF_SETTINGS"] = sdir
+    data = helpers.desc_to_npz(desc)
+    inc = desc.t_end / n_saves
+    snaps = []
+
+    def snap(r, prev):
+        pick = (lambda f: _abi.NODE_PREV[f]) if prev else (lambda f: f)
+        snaps.append({"time": r.control()["time"], "coords": r.nodes(_abi.NODE_COORDS),
+                      "disp": r.nodes(_abi.NODE_DISP), "u": r.nodes(pick(_abi.NODE_U)),
+                      "speed": r.nodes(pick(_abi.NODE_SPEED)), "accel": r.nodes(pick(_abi.NODE_ACCEL)),
+                      "mass": r.nodes(_abi.NODE_MASS), "ips": r.ips(), "increment": r.control()["increment"]})
+
+    with ref.RefModel(desc) as r:
+        r.init()
+        r.enable_vtk(0.0, desc.t_end, inc)  # writes the initial file
+        snap(r, False)
+        nxt = inc
+        while r.control()["time"] < desc.t_end:
+            t = r.control()["time"]
+            r.run(max_incs=1) if t >= nxt else r.run(t_stop=nxt)
+            t = r.control()["time"]
+            if t >= nxt and t <= desc.t_end:  # DynELA::writeResultFile's test
+                snap(r, True)
+                nxt += inc
+        r.write_final_vtk()
+        snap(r, False)
+        files = sorted(f for f in os.listdir(r.workdir) if f.endswith(".vtk"))
+        texts = [open(os.path.join(r.workdir, f)).read() for f in files]
+    assert len(texts) == len(snaps), (len(texts), len(snaps))
+    data["vtk_text"] = np.array(texts)
+    data["vtk_increment"] = np.array([s_["increment"] for s_ in snaps])
+    data["vtk_prev"] = np.array([0] + [1] * (len(snaps) - 2) + [0])
+    for k in ("time", "coords", "disp", "u", "speed", "accel", "mass", "ips"):
+        data["vtk_" + k] = np.array([s_[k] for s_ in snaps])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+    print(name, len(texts), "files")
+
+
 CASES = {
     "axi_run": lambda: run_case("axi_run", helpers.case_axi_small(), [1, 10, 200]),
     "hex_run": lambda: run_case("hex_run", helpers.case_hex_small(), [1, 10, 60]),
@@ -99,9 +262,26 @@ CASES = {
     "plane_run": lambda: run_case("plane_run", helpers.case_plane_small(), [1, 10, 60]),
     "plane_pass": lambda: pass_case("plane_pass", helpers.case_plane_small(), seed=8),
     "taylor_axi_sample": published_case,
+    "config0_whole": config0_case,
+    # result files of the reference (VtkInterface) at its save times
+    "vtk_axi": lambda: vtk_case("vtk_axi", helpers.case_axi_small(), 4),
+    "vtk_hex": lambda: vtk_case("vtk_hex", helpers.case_hex_speed(), 4),
+    "fullsize_taylor3d_153600_incs": lambda: full_run_case("taylor3d_153600", [1, 10, 50]),
+    "fullsize_taylor3d_153600_elempass": lambda: full_pass_case("taylor3d_153600", seed=51),
+    "fullsize_plate_necking_491520_incs": lambda: full_run_case("plate_necking_491520", [1, 5, 10]),
+    "fullsize_plate_necking_491520_elempass": lambda: full_pass_case("plate_necking_491520", seed=53),
+    "fullsize_bar_necking_1198080_incs": lambda: full_run_case("bar_necking_1198080", [1, 5, 10]),
+    "fullsize_bar_necking_1198080_elempass": lambda: full_pass_case("bar_necking_1198080", seed=52),
 }
 
 if __name__ == "__main__":
     # python tests/golden/make_golden.py [case ...]   (all cases by default)
-    for name in (sys.argv[1:] or list(CASES)):
-        CASES[name]()
+    names = sys.argv[1:] or list(CASES)
+    if len(names) == 1:
+        CASES[names[0]]()
+    else:
+        # one process per case: the reference keeps its model in process-wide
+        # state, and a large model built after another one can crash it
+        import subprocess
+        for name in names:
+            subprocess.run([sys.executable, os.path.abspath(__file__), name], check=True)

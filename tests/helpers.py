@@ -122,6 +122,44 @@ def field_errors(ga, gb):
     return err / np.maximum(scale, 1e-300)
 
 
+def field_sums(a):
+    """Per component (column) of a [n, k] field: signed sum, sum of magnitudes
+    and largest magnitude over every row, FP64 ([3, k])."""
+    a = np.asarray(a, dtype=np.float64)
+    return np.stack([a.sum(0), np.abs(a).sum(0), np.abs(a).max(0)])
+
+
+def mesh_digest(desc):
+    """Digest of a model's coordinates and connectivity (a fixture records it
+    so that a test knows it rebuilt the same mesh)."""
+    import hashlib
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(desc.coords, dtype=np.float64).tobytes())
+    h.update(np.ascontiguousarray(desc.conn, dtype=np.int32).tobytes())
+    return h.hexdigest()
+
+
+def entry_errors(a, b, scale):
+    """Entry by entry: |a - b| / (|b| + 1e-6 * scale), the largest over the
+    entries of each row (a [k, n] array of k components); `scale` is the
+    component's largest magnitude over the whole field, so that entries at
+    the rounding level of their field (cancellations to ~1e-16 of it) are
+    not divided by themselves."""
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    scale = np.asarray(scale, dtype=np.float64).reshape(-1, 1)
+    return (np.abs(a - b) / (np.abs(b) + 1e-6 * scale + 1e-300)).max(axis=1)
+
+
+def sums_errors(a_sums, b_sums):
+    """Whole-field checks from field_sums: the sums of magnitudes and the
+    largest magnitudes relative to themselves, the signed sums relative to
+    the sum of magnitudes (a signed sum may cancel)."""
+    a, b = np.asarray(a_sums), np.asarray(b_sums)
+    den = np.maximum(b[1], 1e-300)
+    return np.concatenate([np.abs(a[0] - b[0]) / den, np.abs(a[1] - b[1]) / den,
+                           np.abs(a[2] - b[2]) / np.maximum(b[2], 1e-300)])
+
+
 # model cases shared by the golden fixtures and the parity tests
 def case_axi_small(precision=_abi.PREC_FP64):
     return meshes.taylor_axi(nr=5, nz=20, radius=3.2, length=8.1, speed=227000.0, t_end=4e-6, ts_freq=1,

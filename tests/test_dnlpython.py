@@ -71,6 +71,8 @@ def taylor_axi_script(nr=5, nz=50, speed=287000.0, method=None, save_dir=None, p
         solver.setComputeTimeStepFrequency(1)
         solver.setTimeStepMethod(method)
     if save_dir is not None:
+        # result files, as the sample script asks for them (Taylor.py:120)
+        model.setSaveTimes(0, stop, stop / 10)
         hist = dnl.ElementSet("ES_Hist")
         model.add(hist, 1)
         rad, hei = dnl.NodeSet("NS_R"), dnl.NodeSet("NS_H")
@@ -267,6 +269,7 @@ class OracleEngine:
         from oracle import OracleModel
         self.o = OracleModel(desc)
         self.o.init()
+        self.desc = desc
         self.t_end = desc.t_end
         self.last_dt = None
 
@@ -296,6 +299,16 @@ class OracleEngine:
     def set_items(self, items):
         self.items = list(items)
 
+    def write_vtk(self, path, fields, prev=False, instance=0, title="DynELA FEM Code v.4.0"):
+        """The engine's result file restated (oracle/vtk_ref.py)."""
+        import vtk_ref
+        pick = (lambda f: _abi.NODE_PREV[f]) if prev else (lambda f: f)
+        nf = {"disp": self.o.nodes(_abi.NODE_DISP), "u": self.o.nodes(pick(_abi.NODE_U)),
+              "speed": self.o.nodes(pick(_abi.NODE_SPEED)), "accel": self.o.nodes(pick(_abi.NODE_ACCEL)),
+              "mass": self.o.nodes(_abi.NODE_MASS)}
+        vtk_ref.write(path, self.o.control()["time"], self.o.nodes(_abi.NODE_COORDS), self.desc.conn,
+                      12 if self.desc.nodes_per_element == 8 else 9, nf, self.o.ips(), fields, title)
+
     def gather_items(self):
         """The engine's item gather restated from the full arrays."""
         out = []
@@ -319,7 +332,12 @@ def read_history(path):
 
 def run_api_taylor(save_dir, **kw):
     model, n_nodes = taylor_axi_script(method=dnl.Explicit.PowerIteration, save_dir=str(save_dir), **kw)
-    model.solve()
+    cwd = os.getcwd()
+    os.chdir(save_dir)  # the result files go to the current directory, as the reference's
+    try:
+        model.solve()
+    finally:
+        os.chdir(cwd)
     out = {k: read_history(os.path.join(save_dir, k + ".plot")) for k in ("radius", "height", "plasticStrain", "dt", "ke")}
     return model, out
 
@@ -352,6 +370,17 @@ def test_history_files_through_oracle(tmp_path, monkeypatch):
     np.savez_compressed(os.path.join(tmp_path, "hist.npz"), **{k: v[1] for k, v in out.items()})
     n = model.getNodeByNum(6)
     assert n.coords[0] == pytest.approx(row[3], rel=1e-9)
+    # result files: the initial one, one per save time reached (the next
+    # save time accumulates as DynELA::writeResultFile adds it), the final one
+    nxt, saves = 80e-6 / 10, 0
+    while nxt <= 80e-6:
+        saves, nxt = saves + 1, nxt + 80e-6 / 10
+    names = sorted(f for f in os.listdir(tmp_path) if f.endswith(".vtk"))
+    assert names == [f"Taylor{k:03d}.vtk" for k in range(saves + 2)]
+    import vtk_ref
+    last = vtk_ref.parse(open(os.path.join(tmp_path, names[-1])).read())
+    assert last["order"] == vtk_ref.DEFAULT_FIELDS and last["time"] == pytest.approx(80e-6)
+    assert last["points"][5, 0] == pytest.approx(row[3], rel=1e-5)
 
 
 @pytest.mark.gpu
@@ -370,6 +399,16 @@ def test_history_files_on_engine_match_oracle(tmp_path, monkeypatch):
         assert np.allclose(a[:, 0], b[:, 0], rtol=1e-12, atol=0), k
         scale = np.abs(b[:, 1:]).max() + 1e-300
         assert np.abs(a[:, 1:] - b[:, 1:]).max() <= 2e-7 * scale, k
+    # the result files: written by the engine library, by the restatement on CPU
+    import vtk_ref
+    names = sorted(f for f in os.listdir(tmp_path / "cpu") if f.endswith(".vtk"))
+    assert len(names) >= 11 and names == sorted(f for f in os.listdir(tmp_path / "gpu") if f.endswith(".vtk"))
+    for n in names:
+        g = vtk_ref.parse(open(tmp_path / "gpu" / n).read())
+        c = vtk_ref.parse(open(tmp_path / "cpu" / n).read())
+        assert g["header"] == c["header"]
+        worst = vtk_ref.compare(g, c)
+        assert max(worst.values()) < 2e-5, (n, worst)
 
 
 @pytest.mark.gpu

@@ -1,0 +1,198 @@
+"""Parity of the engine with the compiled reference on the measured workloads
+at their full size (fixtures made by tests/golden/make_golden.py from
+oracle/_ref):
+
+* the 3-D copper Taylor bar of 153,600 ElHex8N3D (the workload of the bench's
+  headline figure), its first 50 increments;
+* the necking round bar of 1,198,080 and the necking plate of 491,520
+  ElHex8N3D, their first 10 increments;
+* one element pass of each of the three on a seeded plastic state and
+  displacement increment (the radial return of every point yields or not as
+  the state says, which the first increments of a run do not exercise);
+* the axisymmetric copper bar of 800 ElQua4NAx run to its end time, with the
+  power-iteration time step every increment and with the Courant time step
+  every 10 increments.
+
+Tolerances.  FP64 path: every sampled entry of every nodal field and of the
+point state within 1e-6 of the reference relative to the entry itself
+(helpers.entry_errors: |a - b| / (|b| + 1e-6 * the component's largest
+magnitude), so that values at the rounding level of their field do not divide
+by themselves), and the sums over the whole field within 1e-9.  Mixed path
+(FP32 element math and point state, FP64 coordinates, displacements, time and
+energy sums): coordinates within 1e-5 of the bar's span, stresses within
+5e-3 and plastic strain within 1e-3 of their tensor's largest component after
+a run; one element pass within helpers.MIXED_PASS_RTOL; whole runs within
+1e-4 on the bar's height and foot radius and 1e-3 on the plastic strain.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import helpers
+from helpers import _abi, meshes
+
+pytestmark = pytest.mark.gpu
+
+FP64_ENTRY_RTOL = 1e-6
+SUMS_RTOL = 1e-9
+
+RUNS = sorted(glob.glob(os.path.join(helpers.GOLDEN, "fullsize_*_incs.npz")))
+PASSES = sorted(glob.glob(os.path.join(helpers.GOLDEN, "fullsize_*_elempass.npz")))
+CONFIG0 = os.path.join(helpers.GOLDEN, "config0_whole.npz")
+
+NODE_FIELDS = (("coords", _abi.NODE_COORDS), ("disp", _abi.NODE_DISP), ("speed", _abi.NODE_SPEED),
+               ("u", _abi.NODE_U), ("accel", _abi.NODE_ACCEL), ("force", _abi.NODE_FORCE))
+MESHES = {"taylor3d_153600": meshes.taylor_3d, "bar_necking_1198080": meshes.bar_necking,
+          "plate_necking_491520": meshes.plate_necking}
+
+
+def engine(desc):
+    from dnlPython.engine import Engine
+    return Engine(desc)
+
+
+def rebuild(z, precision):
+    desc = MESHES[str(z["mesh"])](precision=precision)
+    assert helpers.mesh_digest(desc) == str(z["digest"]), "the mesh generator no longer builds the fixture's mesh"
+    return desc
+
+
+def check_fp64(e, z, prefix, what):
+    nodes, ips = z["sample_nodes"], z["sample_ips"]
+    worst = {}
+    for name, f in NODE_FIELDS:
+        a = e.nodes(f)
+        sums = z[f"{prefix}{name}_sums"]
+        err = helpers.entry_errors(a[nodes].T, z[f"{prefix}{name}"].T, sums[2])
+        serr = helpers.sums_errors(helpers.field_sums(a), sums)
+        worst[name] = (err.max(), serr.max())
+        assert err.max() < FP64_ENTRY_RTOL, (what, name, err)
+        assert serr.max() < SUMS_RTOL, (what, name, serr)
+    ip = e.ips()
+    sums = z[f"{prefix}ips_sums"]
+    err = helpers.entry_errors(ip[:, ips], z[f"{prefix}ips"], sums[2])
+    serr = helpers.sums_errors(helpers.field_sums(ip.T), sums)
+    worst["ips"] = (err.max(), serr.max())
+    assert err.max() < FP64_ENTRY_RTOL, (what, "ips", err)
+    assert serr.max() < SUMS_RTOL, (what, "ips", serr)
+    print(what, {k: f"{v[0]:.1e}/{v[1]:.1e}" for k, v in worst.items()})
+
+
+@pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
+def test_full_size_fp64_runs_match_reference(path):
+    """The first increments of each full-size workload, FP64 path, at every
+    checkpoint: time, time step and increment, every nodal field and the point
+    state."""
+    z = np.load(path)
+    desc = rebuild(z, _abi.PREC_FP64)
+    with engine(desc) as e:
+        e.init()
+        c0 = z["init_control"]
+        assert abs(e.control()["time_step"] - c0[1]) <= 1e-12 * c0[1]
+        done = 0
+        for k in z["checkpoints"]:
+            n = e.run(max_incs=int(k) - done)
+            done += n
+            ck = z[f"inc{k}_control"]
+            c = e.control()
+            assert c["increment"] == int(ck[2]) == done
+            assert abs(c["time"] - ck[0]) <= 1e-12 * ck[0]
+            assert abs(c["time_step"] - ck[1]) <= 1e-11 * ck[1]
+            check_fp64(e, z, f"inc{k}_", f"{os.path.basename(path)} increment {k}")
+
+
+@pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
+def test_full_size_mixed_runs_track_reference(path):
+    z = np.load(path)
+    desc = rebuild(z, _abi.PREC_MIXED)
+    k = int(z["checkpoints"][-1])
+    nodes, ips = z["sample_nodes"], z["sample_ips"]
+    with engine(desc) as e:
+        e.init()
+        e.run(max_incs=k)
+        assert e.control()["increment"] == int(z[f"inc{k}_control"][2])
+        x = e.nodes(_abi.NODE_COORDS)
+        span = np.ptp(desc.coords, axis=0).max()
+        assert np.abs(x[nodes] - z[f"inc{k}_coords"]).max() < 1e-5 * span
+        sx = helpers.sums_errors(helpers.field_sums(x), z[f"inc{k}_coords_sums"])
+        assert sx[3:].max() < 1e-6, sx
+        ip = e.ips()[:, ips]
+    want = z[f"inc{k}_ips"]
+    scale = z[f"inc{k}_ips_sums"][2].copy()
+    for b in (0, 6, 12):
+        scale[b:b + 6] = scale[b:b + 6].max()
+    err = np.abs(ip - want).max(axis=1) / np.maximum(scale, 1e-300)
+    assert err[:6].max() < 5e-3, err
+    assert err[_abi.IP_EPSP] < 1e-3 and err[_abi.IP_T] < 1e-4, err
+
+
+@pytest.mark.parametrize("path", PASSES, ids=[os.path.basename(p) for p in PASSES])
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_full_size_element_pass_matches_reference(path, precision):
+    z = np.load(path)
+    desc = rebuild(z, precision)
+    nodes, ips = z["sample_nodes"], z["sample_ips"]
+    seed = int(z["seed"])
+    with engine(desc) as e:
+        e.init()
+        st = helpers.random_point_state(desc, e.ips(), seed)
+        e.set_ips(st)
+        del st
+        e.set_nodes(_abi.NODE_U, helpers.random_increment(desc, seed + 1))
+        e.element_pass(float(z["dt"]))
+        f = e.nodes(_abi.NODE_FORCE)
+        ip = e.ips()
+    fs, ipsums = z["out_force_sums"], z["out_ips_sums"]
+    if precision == _abi.PREC_FP64:
+        ferr = helpers.entry_errors(f[nodes].T, z["out_force"].T, fs[2])
+        ierr = helpers.entry_errors(ip[:, ips], z["out_ips"], ipsums[2])
+        assert ferr.max() < FP64_ENTRY_RTOL, ferr
+        assert ierr.max() < FP64_ENTRY_RTOL, ierr
+        assert helpers.sums_errors(helpers.field_sums(f), fs).max() < SUMS_RTOL
+        assert helpers.sums_errors(helpers.field_sums(ip.T), ipsums).max() < SUMS_RTOL
+        print(os.path.basename(path), f"fp64 per entry: forces {ferr.max():.1e}, point state {ierr.max():.1e}")
+    else:
+        assert helpers.rel_err(f[nodes], z["out_force"]) < helpers.MIXED_PASS_RTOL
+        errs = helpers.field_errors(ip[:, ips], z["out_ips"])
+        assert errs.max() < helpers.MIXED_PASS_RTOL, errs
+
+
+def _summary(desc, x, ip):
+    """Height of the bar's top on the axis, foot radius, largest element-mean
+    plastic strain (the figures of the reference's Taylor-Axi sample)."""
+    return np.array([x[desc.n_nodes - 11, 1], x[10, 0], ip[_abi.IP_EPSP].reshape(-1, 4).mean(1).max()])
+
+
+@pytest.mark.skipif(not os.path.exists(CONFIG0), reason="fixture not generated")
+@pytest.mark.parametrize("tag", ["pi1", "courant10"])
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_config0_whole_run_matches_reference(tag, precision):
+    """Copper Taylor bar, 10 x 80 ElQua4NAx, 227 m/s, to 80 us, against the
+    compiled reference's own whole run."""
+    z = np.load(CONFIG0)
+    method, freq = (_abi.TS_POWER_ITERATION, 1) if tag == "pi1" else (_abi.TS_COURANT, 10)
+    desc = meshes.taylor_axi(ts_method=method, ts_freq=freq, precision=precision)
+    want_x, want_ip, ctl = z[f"{tag}_coords"], z[f"{tag}_ips"], z[f"{tag}_control"]
+    want = _summary(desc, want_x, want_ip)
+    if tag == "pi1":
+        # the reference's answer for this case: height 19.0956 mm, foot radius
+        # 7.2517 mm, largest element-mean plastic strain 3.0045
+        assert np.allclose(np.round(want, 4), [19.0956, 7.2517, 3.0045])
+    with engine(desc) as e:
+        e.init()
+        n = e.run()
+        c = e.control()
+        x, ip = e.nodes(_abi.NODE_COORDS), e.ips()
+    got = _summary(desc, x, ip)
+    assert c["done"]
+    if precision == _abi.PREC_FP64:
+        assert n == int(ctl[3]) and c["increment"] == int(ctl[2])
+        assert abs(c["time"] - ctl[0]) <= 1e-12 * ctl[0]
+        assert helpers.rel_err(x, want_x) < 1e-9
+        assert helpers.field_errors(ip, want_ip).max() < 1e-6
+        assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max()
+    else:
+        assert abs(got[0] - want[0]) < 1e-4 * want[0] and abs(got[1] - want[1]) < 1e-4 * want[1]
+        assert abs(got[2] - want[2]) < 1e-3 * want[2]
