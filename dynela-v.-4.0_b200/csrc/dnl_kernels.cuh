@@ -2433,6 +2433,16 @@ template <typename R> __global__ void k_ips_out(DevModel M, int c0, int nc, doub
   dst[k] = (double)ipv<R>(M, c, q);
 }
 
+// The whole point state, tile-major in R, to a component-major array in R.
+template <typename R> __global__ void k_ips_out_native(DevModel M, R *dst)
+{
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (long long)DNL_IP_NCOMP * M.nIP)
+    return;
+  const int c = (int)(k / M.nIP), q = (int)(k % M.nIP);
+  dst[k] = ipv<R>(M, c, q);
+}
+
 // --------------------------------------------------------- history items
 
 // One thread per item (DNL_ITEM_*): the selected nodal vector, point state or

@@ -1562,6 +1562,29 @@ int dnl_engine_write_vtk(dnl_engine *h, int32_t inst, const char *path, const ch
   return DNL_OK;
 }
 
+int dnl_engine_get_ips_native(dnl_engine *h, void *out, int32_t word)
+{
+  if (!h || !out)
+    return DNL_ERR_ARG;
+  const int native = h->precision == DNL_PREC_MIXED ? 4 : 8;
+  if (word != native)
+    return fail(h, DNL_ERR_ARG, "the point state is kept in %d-byte words, not %d", native, word);
+  const long long items = (long long)DNL_IP_NCOMP * h->nIP;
+  const size_t bytes = (size_t)items * native;
+  void *st = nullptr;
+  int rc = staging(h, bytes, &st);
+  if (rc)
+    return rc;
+  const unsigned blocks = (unsigned)((items + 255) / 256);
+  if (native == 4)
+    k_ips_out_native<float><<<blocks, 256, 0, h->stream>>>(h->M, (float *)st);
+  else
+    k_ips_out_native<double><<<blocks, 256, 0, h->stream>>>(h->M, (double *)st);
+  CK(cudaGetLastError());
+  h->launches++;
+  return copy(h, out, st, bytes, cudaMemcpyDeviceToHost);
+}
+
 int dnl_engine_set_ips(dnl_engine *h, const double *in)
 {
   if (!h || !in)

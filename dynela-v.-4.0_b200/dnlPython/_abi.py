@@ -294,6 +294,7 @@ def load_library():
         "dnl_engine_get_nodes": (ctypes.c_int, [vp, i32, pd]),
         "dnl_engine_set_nodes": (ctypes.c_int, [vp, i32, pd]),
         "dnl_engine_get_ips": (ctypes.c_int, [vp, pd]),
+        "dnl_engine_get_ips_native": (ctypes.c_int, [vp, vp, i32]),
         "dnl_engine_set_ips": (ctypes.c_int, [vp, pd]),
         "dnl_engine_energies": (ctypes.c_int, [vp, i32, pd]),
         "dnl_engine_set_items": (ctypes.c_int, [vp, ctypes.POINTER(Item), i32, ctypes.POINTER(i64)]),

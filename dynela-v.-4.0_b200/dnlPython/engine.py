@@ -95,6 +95,19 @@ class Engine:
         self._check(self._lib.dnl_engine_get_ips(self.h, _pd(out)))
         return out
 
+    def ips_native(self, out=None):
+        """The point state in the engine's own precision (float32 on the
+        mixed path, float64 on the FP64 path), [IP_NCOMP, n_ips]."""
+        dt = np.float32 if self.descs[0].precision == _abi.PREC_MIXED else np.float64
+        shape = (_abi.IP_NCOMP, self.n_ips)
+        if out is None:
+            out = np.empty(shape, dtype=dt)
+        elif out.shape != shape or out.dtype != dt or not out.flags.c_contiguous:
+            raise ValueError(f"output array must be C-contiguous {np.dtype(dt).name} of shape {shape}")
+        self._check(self._lib.dnl_engine_get_ips_native(self.h, out.ctypes.data_as(ctypes.c_void_p),
+                                                         out.dtype.itemsize))
+        return out
+
     def set_ips(self, values):
         a = np.ascontiguousarray(values, dtype=np.float64).reshape(_abi.IP_NCOMP, self.n_ips)
         self._check(self._lib.dnl_engine_set_ips(self.h, _pd(a)))

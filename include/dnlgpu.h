@@ -212,6 +212,11 @@ int dnl_engine_set_nodes(dnl_engine *h, int32_t field, const double *in);
  * component-major (converted from/to FP32 on the mixed path). */
 int dnl_engine_get_ips(dnl_engine *h, double *out);
 int dnl_engine_set_ips(dnl_engine *h, const double *in);
+/* The point state in the precision the engine keeps it in, same layout:
+ * word = 4 (float) on the mixed path, 8 (double) on the FP64 path; another
+ * word size returns DNL_ERR_ARG.  Nothing is widened, so the mixed path's
+ * state crosses to the host in half the bytes of dnl_engine_get_ips. */
+int dnl_engine_get_ips_native(dnl_engine *h, void *out, int32_t word);
 
 /* History items (replaces the per-save reads of HistoryFile::save,
  * HistoryFile.C:289-317, and of the Field extraction it calls,

@@ -139,15 +139,18 @@ def mesh_digest(desc):
     return h.hexdigest()
 
 
-def entry_errors(a, b, scale):
-    """Entry by entry: |a - b| / (|b| + 1e-6 * scale), the largest over the
+def entry_errors(a, b, scale, floor=1e-4):
+    """Entry by entry: |a - b| / (|b| + floor * scale), the largest over the
     entries of each row (a [k, n] array of k components); `scale` is the
-    component's largest magnitude over the whole field, so that entries at
-    the rounding level of their field (cancellations to ~1e-16 of it) are
-    not divided by themselves."""
+    component's largest magnitude over the whole field.  A bound tol on it
+    reads |a - b| <= tol |b| for every entry above `floor` of its field's
+    largest magnitude, and |a - b| <= tol * floor * scale below: values that
+    are themselves at the rounding level of their field (shear components
+    cancelling to 1e-8 of the stress, say) are held to that absolute level
+    instead of being divided by themselves."""
     a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
     scale = np.asarray(scale, dtype=np.float64).reshape(-1, 1)
-    return (np.abs(a - b) / (np.abs(b) + 1e-6 * scale + 1e-300)).max(axis=1)
+    return (np.abs(a - b) / (np.abs(b) + floor * scale + 1e-300)).max(axis=1)
 
 
 def sums_errors(a_sums, b_sums):

@@ -14,10 +14,13 @@ oracle/_ref):
   every 10 increments.
 
 Tolerances.  FP64 path: every sampled entry of every nodal field and of the
-point state within 1e-6 of the reference relative to the entry itself
-(helpers.entry_errors: |a - b| / (|b| + 1e-6 * the component's largest
-magnitude), so that values at the rounding level of their field do not divide
-by themselves), and the sums over the whole field within 1e-9.  Mixed path
+point state within 1e-6 of the reference relative to the entry itself, for
+entries above 1e-4 of their component's largest magnitude, and within 1e-10
+of that magnitude below (helpers.entry_errors: |a - b| / (|b| + 1e-4 * the
+component's largest magnitude) < 1e-6; the reference's own FP64 rounding
+differences, between its eigen-solver and the C restatement's, reach 4e-11 of
+the largest shear stress after 10 increments of the 153,600-element bar), and
+the sums over the whole field within 1e-9.  Mixed path
 (FP32 element math and point state, FP64 coordinates, displacements, time and
 energy sums): coordinates within 1e-5 of the bar's span, stresses within
 5e-3 and plastic strain within 1e-3 of their tensor's largest component after

@@ -321,3 +321,19 @@ def test_power_iteration_vs_oracle(case):
         e.run(max_incs=30)
         assert abs(e.control()["time_step"] - o.control()["time_step"]) < 1e-11 * o.control()["time_step"]
         assert helpers.rel_err(e.nodes(_abi.NODE_COORDS), o.nodes(_abi.NODE_COORDS)) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_native_state_read_equals_widened(precision):
+    """dnl_engine_get_ips_native gives the point state in the engine's own
+    precision: widened, it equals dnl_engine_get_ips; the other word size is
+    refused."""
+    d = helpers.case_hex_small(precision)
+    with engine(d) as e:
+        e.init()
+        e.run(max_incs=15)
+        nat = e.ips_native()
+        assert nat.dtype == (np.float32 if precision == _abi.PREC_MIXED else np.float64)
+        assert np.array_equal(nat.astype(np.float64), e.ips())
+        other = np.empty(nat.shape, np.float64 if precision == _abi.PREC_MIXED else np.float32)
+        assert e._lib.dnl_engine_get_ips_native(e.h, other.ctypes.data, other.dtype.itemsize) == -1
