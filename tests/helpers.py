@@ -163,6 +163,37 @@ def sums_errors(a_sums, b_sums):
                            np.abs(a[2] - b[2]) / np.maximum(b[2], 1e-300)])
 
 
+FULL_NODE_FIELDS = (("coords", _abi.NODE_COORDS), ("disp", _abi.NODE_DISP), ("speed", _abi.NODE_SPEED),
+                    ("u", _abi.NODE_U), ("accel", _abi.NODE_ACCEL), ("force", _abi.NODE_FORCE))
+FULL_ENTRY_RTOL = 1e-6
+FULL_SUMS_RTOL = 1e-9
+
+
+def check_full_size(m, z, prefix, what):
+    """A model (engine or oracle: nodes(field), ips()) against a full-size
+    fixture's checkpoint `prefix`: the sampled entries of every nodal field
+    and of the point state by entry_errors < FULL_ENTRY_RTOL, the sums over
+    the whole field by sums_errors < FULL_SUMS_RTOL.  Returns the worst errors."""
+    nodes, ips = z["sample_nodes"], z["sample_ips"]
+    worst = {}
+    for name, f in FULL_NODE_FIELDS:
+        a = m.nodes(f)
+        sums = z[f"{prefix}{name}_sums"]
+        err = entry_errors(a[nodes].T, z[f"{prefix}{name}"].T, sums[2])
+        serr = sums_errors(field_sums(a), sums)
+        worst[name] = (err.max(), serr.max())
+        assert err.max() < FULL_ENTRY_RTOL, (what, name, err)
+        assert serr.max() < FULL_SUMS_RTOL, (what, name, serr)
+    ip = m.ips()
+    sums = z[f"{prefix}ips_sums"]
+    err = entry_errors(ip[:, ips], z[f"{prefix}ips"], sums[2])
+    serr = sums_errors(field_sums(ip.T), sums)
+    worst["ips"] = (err.max(), serr.max())
+    assert err.max() < FULL_ENTRY_RTOL, (what, "ips", err)
+    assert serr.max() < FULL_SUMS_RTOL, (what, "ips", serr)
+    return worst
+
+
 # model cases shared by the golden fixtures and the parity tests
 def case_axi_small(precision=_abi.PREC_FP64):
     return meshes.taylor_axi(nr=5, nz=20, radius=3.2, length=8.1, speed=227000.0, t_end=4e-6, ts_freq=1,

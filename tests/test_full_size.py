@@ -38,15 +38,13 @@ from helpers import _abi, meshes
 
 pytestmark = pytest.mark.gpu
 
-FP64_ENTRY_RTOL = 1e-6
-SUMS_RTOL = 1e-9
+FP64_ENTRY_RTOL = helpers.FULL_ENTRY_RTOL
+SUMS_RTOL = helpers.FULL_SUMS_RTOL
 
 RUNS = sorted(glob.glob(os.path.join(helpers.GOLDEN, "fullsize_*_incs.npz")))
 PASSES = sorted(glob.glob(os.path.join(helpers.GOLDEN, "fullsize_*_elempass.npz")))
 CONFIG0 = os.path.join(helpers.GOLDEN, "config0_whole.npz")
 
-NODE_FIELDS = (("coords", _abi.NODE_COORDS), ("disp", _abi.NODE_DISP), ("speed", _abi.NODE_SPEED),
-               ("u", _abi.NODE_U), ("accel", _abi.NODE_ACCEL), ("force", _abi.NODE_FORCE))
 MESHES = {"taylor3d_153600": meshes.taylor_3d, "bar_necking_1198080": meshes.bar_necking,
           "plate_necking_491520": meshes.plate_necking}
 
@@ -63,23 +61,7 @@ def rebuild(z, precision):
 
 
 def check_fp64(e, z, prefix, what):
-    nodes, ips = z["sample_nodes"], z["sample_ips"]
-    worst = {}
-    for name, f in NODE_FIELDS:
-        a = e.nodes(f)
-        sums = z[f"{prefix}{name}_sums"]
-        err = helpers.entry_errors(a[nodes].T, z[f"{prefix}{name}"].T, sums[2])
-        serr = helpers.sums_errors(helpers.field_sums(a), sums)
-        worst[name] = (err.max(), serr.max())
-        assert err.max() < FP64_ENTRY_RTOL, (what, name, err)
-        assert serr.max() < SUMS_RTOL, (what, name, serr)
-    ip = e.ips()
-    sums = z[f"{prefix}ips_sums"]
-    err = helpers.entry_errors(ip[:, ips], z[f"{prefix}ips"], sums[2])
-    serr = helpers.sums_errors(helpers.field_sums(ip.T), sums)
-    worst["ips"] = (err.max(), serr.max())
-    assert err.max() < FP64_ENTRY_RTOL, (what, "ips", err)
-    assert serr.max() < SUMS_RTOL, (what, "ips", serr)
+    worst = helpers.check_full_size(e, z, prefix, what)
     print(what, {k: f"{v[0]:.1e}/{v[1]:.1e}" for k, v in worst.items()})
 
 

@@ -237,3 +237,35 @@ def test_oracle_power_iteration_reproduces_taylor_axi_sample():
     assert n == int(row[2])
     assert abs(c[5, 0] - row[3]) < 1e-9 and abs(c[d.n_nodes - 6, 1] - row[4]) < 1e-9
     assert abs(ip[_abi.IP_EPSP].reshape(-1, 4).mean(1).max() - row[5]) < 1e-9
+
+
+def test_oracle_matches_full_size_bar():
+    """The C restatement on the 153,600-element bar of the bench's headline
+    figure against the compiled reference's fixture: its first 10
+    increments (every nodal field and the point state, sampled entries and
+    whole-field sums, with the bounds of the engine's full-size parity test)
+    and one element pass on a seeded plastic state."""
+    z = np.load(os.path.join(helpers.GOLDEN, "fullsize_taylor3d_153600_incs.npz"))
+    desc = meshes.taylor_3d(precision=_abi.PREC_FP64)
+    assert helpers.mesh_digest(desc) == str(z["digest"])
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        assert abs(o.control()["time_step"] - z["init_control"][1]) <= 1e-12 * z["init_control"][1]
+        done = 0
+        for k in z["checkpoints"][:2]:
+            done += o.run(max_incs=int(k) - done)
+            assert o.control()["increment"] == int(z[f"inc{k}_control"][2])
+            helpers.check_full_size(o, z, f"inc{k}_", f"oracle increment {k}")
+    z = np.load(os.path.join(helpers.GOLDEN, "fullsize_taylor3d_153600_elempass.npz"))
+    seed = int(z["seed"])
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        o.set_ips(helpers.random_point_state(desc, o.ips(), seed))
+        o.set_nodes(_abi.NODE_U, helpers.random_increment(desc, seed + 1))
+        o.element_pass(float(z["dt"]))
+        f, ip = o.nodes(_abi.NODE_FORCE), o.ips()
+    nodes, ips = z["sample_nodes"], z["sample_ips"]
+    assert helpers.entry_errors(f[nodes].T, z["out_force"].T, z["out_force_sums"][2]).max() < helpers.FULL_ENTRY_RTOL
+    assert helpers.entry_errors(ip[:, ips], z["out_ips"], z["out_ips_sums"][2]).max() < helpers.FULL_ENTRY_RTOL
+    assert helpers.sums_errors(helpers.field_sums(f), z["out_force_sums"]).max() < helpers.FULL_SUMS_RTOL
+    assert helpers.sums_errors(helpers.field_sums(ip.T), z["out_ips_sums"]).max() < helpers.FULL_SUMS_RTOL
