@@ -48,11 +48,12 @@ def parse():
                    help="element-pass variant (0-7); default: chosen by the autotuner")
     p.add_argument("--no-accuracy", action="store_true", help="skip the whole-run mixed/FP64 comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
-    p.add_argument("--no-guess", action="store_true", help="skip the learned Newton initial guess block")
+    p.add_argument("--guess", action="store_true",
+                   help="also run the learned Newton initial guess block (harvest, training, comparison; ~1 min)")
     p.add_argument("--no-necking", action="store_true", help="skip the necking workloads block")
     p.add_argument("--no-config0", action="store_true", help="skip the axisymmetric Taylor bar block")
-    p.add_argument("--batch-fp64-sample", type=int, default=32,
-                   help="instances of the batch timed one by one on the FP64 path")
+    p.add_argument("--batch-fp64-sample", type=int, default=256,
+                   help="instances of the batch timed one by one on the FP64 path (default: all 256)")
     p.add_argument("--axial", type=int, default=160,
                    help="axial element layers (160 = the measured workload; fewer for profiling captures)")
     return p.parse_args()
@@ -315,9 +316,14 @@ def batch_run(sample, dist=None, world=1, rank=0):
                 s_steps += d.n_elems * e.control()["increment"]
         rate = s_steps / (t_ms / 1e3)
         est_s = steps / rate
+        every = len(pick) == len(descs)
         out["fp64_one_by_one"] = {"instances_timed": int(len(pick)), "elem_steps_per_s": rate,
-                                  "est_seconds_all": est_s, "est_sims_per_s": len(descs) / est_s,
-                                  "how": "every instance of a size-ordered stride timed alone to its end time; "
+                                  "seconds_all" if every else "est_seconds_all": est_s if not every else t_ms / 1e3,
+                                  "sims_per_s" if every else "est_sims_per_s":
+                                      len(descs) / (t_ms / 1e3 if every else est_s),
+                                  "how": "every instance of the batch run alone to its end time on the FP64 path, "
+                                         "device time of each run summed" if every else
+                                         "every instance of a size-ordered stride timed alone to its end time; "
                                          "all-instance time extrapolated by elem-steps"}
         out["batched_mixed_over_one_by_one_fp64"] = out["elem_steps_per_s"] / rate
     return out
@@ -540,7 +546,9 @@ def run_engine_arm(args, rank, world, dist):
     if not args.no_e2e:
         # the caller's result buffers, page-locked and allocated once (outside the timing)
         import torch
-        ips_host = torch.empty((_abi.IP_NCOMP, desc.n_ips), dtype=torch.float64, pin_memory=True).numpy()
+        # the point state in the engine's own precision (FP32 on the mixed path: nothing widened)
+        ips_host = torch.empty((_abi.IP_NCOMP, desc.n_ips), pin_memory=True,
+                               dtype=torch.float32 if args.precision == "mixed" else torch.float64).numpy()
         coords_host = torch.empty((desc.n_nodes, 3), dtype=torch.float64, pin_memory=True).numpy()
         # three repetitions, the median reported (host-side times vary from
         # one run to the next with the state of the host's memory)
@@ -556,7 +564,7 @@ def run_engine_arm(args, rank, world, dist):
             e.run(max_incs=args.steps)
             tc = time.perf_counter()
             coords = e.nodes(_abi.NODE_COORDS, out=coords_host)
-            ips = e.ips(out=ips_host)
+            ips = e.ips_native(out=ips_host)
             t1 = time.perf_counter()
             e.close()
             reps.append((max_over_ranks(t1 - t0),
@@ -567,8 +575,9 @@ def run_engine_arm(args, rank, world, dist):
         d2h = coords.nbytes + ips.nbytes
         e2e = {"value": world * desc.n_elems * args.steps / wall, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "what": "model upload + start of the solve + K increments + coordinates and point state read back "
-                       "into page-locked host arrays allocated before the timing; median of 3 runs",
+               "what": "model upload and build + start of the solve + K increments + coordinates (FP64) and "
+                       "point state (in the path's own precision) read back into page-locked host arrays "
+                       "allocated before the timing; median of 3 runs",
                "seconds": secs, "walls_s": [r[0] for r in reps]}
 
     batched = None
@@ -613,7 +622,7 @@ def run_engine_arm(args, rank, world, dist):
         out["necking"] = necking_run()
     if world == 1 and not args.no_config0:
         out["taylor_axi_800"] = config0_run()
-    if world == 1 and AXIAL == 160 and not args.no_guess:
+    if world == 1 and AXIAL == 160 and args.guess:
         out["learned_guess"] = guess_run()
     print(json.dumps(out))
 

@@ -2306,6 +2306,202 @@ __global__ void __launch_bounds__(TILE) k_power_iteration(DevModel M, int force)
   }
 }
 
+// ------------------------------------------------------------ model build
+//
+// The model is built on the device from the caller's arrays as they come
+// (uploaded into scratch): node vectors in the double4 layout, boundary codes,
+// connectivity with each instance's node offset, element materials, and the
+// node -> slot lists (CSR) of the force assembly.
+
+// Per instance: first node, first element, first material, first function.
+struct BuildRaw
+{
+  const double *coords, *vinit, *bcval; // [3 nN]
+  const int8_t *bccode;                 // [3 nN]
+  const int *bcfun;                     // [3 nN], -1 none
+  const int *conn;                      // [nIP], instance-local node indices
+  const int *emat;                      // [nE], instance-local material indices
+  const int4 *base;                     // [nInst]: node, element, material, function bases
+  int *speedCount;                      // nodes with an imposed speed (list fill)
+  int *cursor;                          // [nN] CSR fill cursors
+  int *list;                            // [nIP] incidences grouped by node
+  int *blockSums;                       // scan partials
+  int npe;
+};
+
+// Nodes: coordinates, initial speed (the description's, then the imposed
+// speed of a constant condition, Model.C:429 / BoundarySpeed.C:63-73), zero
+// displacement, increments and accelerations, boundary codes (an imposed zero
+// speed restrains the component), imposed speeds and their functions.
+__global__ void k_build_nodes(DevModel M, BuildRaw R, int hasSpeed)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nN)
+    return;
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
+  const int fbase = R.base[inst].w;
+  const double4 zero = make_double4(0, 0, 0, 0);
+  double4 v = make_double4(R.vinit[3 * i], R.vinit[3 * i + 1], R.vinit[3 * i + 2], 0.0);
+  double4 sv = zero;
+  int4 sf = make_int4(-1, -1, -1, -1);
+  unsigned code = 0;
+  bool speed = false;
+  for (int c = 0; c < 3; c++)
+  {
+    int cc = R.bccode[3 * i + c];
+    const double val = R.bcval[3 * i + c];
+    const int fn = R.bcfun[3 * i + c];
+    if (cc == DNL_BC_SPEED && val == 0.0)
+      cc = DNL_BC_RESTRAIN;
+    if (cc == DNL_BC_SPEED)
+    {
+      speed = true;
+      comp(sv, c) = val;
+      (c == 0 ? sf.x : (c == 1 ? sf.y : sf.z)) = fn >= 0 ? fn + fbase : -1;
+    }
+    if (cc == DNL_BC_RESTRAIN || cc == DNL_BC_SPEED)
+      code |= (unsigned)cc << (2 * c);
+  }
+  if (speed)
+  {
+    v = sv;
+    const_cast<int *>(M.speed_nodes)[atomicAdd(R.speedCount, 1)] = i;
+  }
+  M.x[i] = make_double4(R.coords[3 * i], R.coords[3 * i + 1], R.coords[3 * i + 2], 0.0);
+  M.v[0][i] = v;
+  M.v[1][i] = v;
+  M.disp[i] = zero;
+  M.u[0][i] = M.u[1][i] = zero;
+  M.a[0][i] = M.a[1][i] = zero;
+  const_cast<uint8_t *>(M.bc)[i] = (uint8_t)code;
+  if (hasSpeed)
+  {
+    const_cast<double4 *>(M.bcval)[i] = sv;
+    const_cast<int4 *>(M.bcfun)[i] = sf;
+  }
+}
+
+// Connectivity (with the instance's node offset; whole tiles, the padding
+// zero), element materials, and each node's slot count in csr_off[node + 1].
+__global__ void k_build_elems(DevModel M, BuildRaw R, int nIPpad)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nIPpad)
+    return;
+  int *conn = const_cast<int *>(M.conn);
+  int *off = const_cast<int *>(M.csr_off);
+  int *emat = const_cast<int *>(M.emat);
+  const int e = k / R.npe;
+  if (k >= M.nIP)
+  {
+    conn[k] = 0;
+    const_cast<int *>(M.slot_pos)[k] = 0;
+    if (k % R.npe == 0)
+      emat[e] = 0;
+    return;
+  }
+  const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, e) : 0;
+  const int4 b = R.base[inst];
+  const int node = R.conn[k] + b.x;
+  conn[k] = node;
+  atomicAdd(&off[node + 1], 1);
+  if (k % R.npe == 0)
+    emat[e] = b.z + R.emat[e];
+}
+
+// Inclusive scan of csr_off[1 .. nN] in three launches: per-block scans with
+// their totals, a scan of the totals (one block), the totals added back.
+constexpr int SCAN_BLOCK = 1024;
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_blocks(int *a, int n, int *blockSums)
+{
+  __shared__ int wsum[32];
+  const int i = blockIdx.x * SCAN_BLOCK + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int v = i < n ? a[i] : 0;
+  for (int o = 1; o < 32; o <<= 1)
+  {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o)
+      v += y;
+  }
+  if (lane == 31)
+    wsum[w] = v;
+  __syncthreads();
+  if (w == 0)
+  {
+    int x = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1)
+    {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o)
+        x += y;
+    }
+    wsum[lane] = x;
+  }
+  __syncthreads();
+  if (w > 0)
+    v += wsum[w - 1];
+  if (i < n)
+    a[i] = v;
+  if (threadIdx.x == SCAN_BLOCK - 1)
+    blockSums[blockIdx.x] = v;
+}
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_sums(int *blockSums, int nb)
+{
+  if (threadIdx.x == 0)
+  {
+    int run = 0;
+    for (int b = 0; b < nb; b++)
+    {
+      run += blockSums[b];
+      blockSums[b] = run;
+    }
+  }
+}
+__global__ void k_scan_add(int *a, int n, const int *blockSums)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && i >= SCAN_BLOCK)
+    a[i] += blockSums[i / SCAN_BLOCK - 1];
+}
+
+// Slot lists: each incidence appended to its node's run (any order), then
+// each run sorted by incidence (the element order of the reference's
+// scatter-add, Model.C:881-898) and slot_pos[k] set to k's place.
+__global__ void k_slot_cursor(DevModel M, BuildRaw R)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < M.nN)
+    R.cursor[i] = M.csr_off[i];
+}
+__global__ void k_slot_fill(DevModel M, BuildRaw R)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < M.nIP)
+    R.list[atomicAdd(&R.cursor[M.conn[k]], 1)] = k;
+}
+__global__ void k_slot_sort(DevModel M, BuildRaw R)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nN)
+    return;
+  const int b = M.csr_off[i], n = M.csr_off[i + 1] - b;
+  int *L = R.list + b;
+  for (int j = 1; j < n; j++)
+  {
+    const int v = L[j];
+    int k = j - 1;
+    while (k >= 0 && L[k] > v)
+    {
+      L[k + 1] = L[k];
+      k--;
+    }
+    L[k + 1] = v;
+  }
+  int *pos = const_cast<int *>(M.slot_pos);
+  for (int j = 0; j < n; j++)
+    pos[L[j]] = b + j;
+}
+
 // ------------------------------------------------------- state read-back
 
 // Nodal vector `field` (DNL_NODE_*) of node i, on the parity of the two-buffer
@@ -2473,6 +2669,123 @@ __global__ void k_gather_items(DevModel M, const int4 *items, const long long *o
   o[0] = v.x;
   o[1] = v.y;
   o[2] = v.z;
+}
+
+// ----------------------------------------------------- history records
+
+// History records kept on the device while a single model runs: the save
+// rule of HistoryFile::save (HistoryFile.C:292-317) per schedule j — a
+// record is due when !(t > start_j && t < next_j), and next_j then moves on by
+// save_j — evaluated at the end of every increment, after the time update, as
+// Explicit::endStep calls Model::writeHistoryFiles (Explicit.C:539-552).
+// A due increment appends one record of HIST_HEAD header words (time,
+// increment, the increment's time step, the 64-bit mask of the due
+// schedules as two 32-bit halves) and the values of the registered items.
+constexpr int HIST_HEAD = DNL_HIST_HEAD;
+struct HistRing
+{
+  int nSched, cap;
+  double *start, *next, *save; // [nSched]
+  int *count;                  // records since the last drain
+  int *overflow;               // set when a record found the ring full
+  long long *last;             // last increment checked
+  double *rec;                 // [cap][HIST_HEAD + nValues]
+};
+
+// Kinetic energy of instance 0 on speed buffer fsel: the loop and tree of
+// k_energies (same order, same bits).  Called by a whole block of 256.
+__device__ __forceinline__ double block_kinetic(const DevModel &M, int fsel, double *sh)
+{
+  const Ctl &c = M.ctl[0];
+  double ke = 0.0;
+  for (int i = c.node_begin + threadIdx.x; i < c.node_end; i += blockDim.x)
+  {
+    const double4 v = M.v[fsel][i];
+    ke += M.mass[i] * (v.x * v.x + v.y * v.y + v.z * v.z) / 2.0;
+  }
+  sh[threadIdx.x] = ke;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1)
+  {
+    if (threadIdx.x < s)
+      sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// One block of 256 after the end of the increment (single models).
+template <typename R>
+__global__ void __launch_bounds__(256) k_history_ring(DevModel M, HistRing H, const int4 *items,
+                                                      const long long *off, int nItems, int nValues, int kin)
+{
+  pdl_wait();
+  __shared__ double sh[256];
+  __shared__ int slot;
+  const Ctl &c = M.ctl[0];
+  if (threadIdx.x == 0)
+  {
+    slot = -1;
+    unsigned long long mask = 0ull;
+    const long long committed = c.inc - ((c.prepared && c.active) ? 1 : 0);
+    if (committed != *H.last)
+    {
+      *H.last = committed;
+      const double t = c.t;
+      for (int j = 0; j < H.nSched; j++)
+        if (!(t > H.start[j] && t < H.next[j]))
+        {
+          H.next[j] += H.save[j];
+          mask |= 1ull << j;
+        }
+      if (mask)
+      {
+        const int k = *H.count;
+        if (k < H.cap)
+        {
+          slot = k;
+          *H.count = k + 1;
+          double *r = H.rec + (size_t)k * (HIST_HEAD + nValues);
+          r[0] = t;
+          r[1] = (double)committed;
+          r[2] = c.dt_last;
+          r[3] = (double)(unsigned)(mask & 0xffffffffull);
+          r[4] = (double)(unsigned)(mask >> 32);
+        }
+        else
+          *H.overflow = 1;
+      }
+    }
+  }
+  __syncthreads();
+  if (slot < 0)
+    return;
+  double kinv[2] = {0.0, 0.0};
+  if (kin)
+  {
+    kinv[0] = block_kinetic(M, c.f0, sh);
+    kinv[1] = block_kinetic(M, 1 - c.f0, sh);
+  }
+  double *vals = H.rec + (size_t)slot * (HIST_HEAD + nValues) + HIST_HEAD;
+  for (int k = threadIdx.x; k < nItems; k += blockDim.x)
+  {
+    const int4 it = items[k];
+    double *o = vals + off[k];
+    if (it.x == DNL_ITEM_POINT)
+      for (int q = 0; q < DNL_IP_NCOMP; q++)
+        o[q] = (double)ipv<R>(M, q, it.z);
+    else if (it.x == DNL_ITEM_KINETIC)
+      o[0] = kinv[it.y == DNL_NODE_SPEED_PREV ? 1 : 0];
+    else
+    {
+      const double4 v = node_vec(M, it.y, it.z);
+      o[0] = v.x;
+      o[1] = v.y;
+      o[2] = v.z;
+    }
+  }
 }
 
 // -------------------------------------------------------------- energies

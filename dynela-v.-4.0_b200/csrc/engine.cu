@@ -39,7 +39,7 @@ struct dnl_engine
   std::vector<void *> allocs;
   std::vector<int> elemBegin, nodeBegin;
   std::vector<Ctl> ctlInit;
-  Ctl *hctl = nullptr; // pinned mirror of the control blocks
+  Ctl *hctl = nullptr; // host mirror of the control blocks
   double *denergy = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graphExec = nullptr;
@@ -71,6 +71,11 @@ struct dnl_engine
   void *dstage = nullptr;
   size_t stageBytes = 0;
   int *dslotInc = nullptr; // incidence of each force slot (node averages)
+  // history records kept on the device (dnl_engine_set_history)
+  bool histOn = false;
+  HistRing hist{};
+  void *histMem = nullptr;
+  std::vector<double> histHost; // records drained from the device, oldest first
   std::string err;
 };
 
@@ -534,6 +539,23 @@ int launch_step_end(dnl_engine *h)
   return DNL_OK;
 }
 
+// History records of the increment that just ended (single models with
+// dnl_engine_set_history): one block after the end of the increment.
+int launch_history(dnl_engine *h)
+{
+  if (!h->histOn)
+    return DNL_OK;
+  const int kin = h->itemsKinetic ? 1 : 0;
+  if (h->precision == DNL_PREC_MIXED)
+    launch_pdl(h, k_history_ring<float>, 1, 256, 0, h->M, h->hist, (const int4 *)h->ditems,
+               (const long long *)h->ditemOff, h->nItems, (int)h->nValues, kin);
+  else
+    launch_pdl(h, k_history_ring<double>, 1, 256, 0, h->M, h->hist, (const int4 *)h->ditems,
+               (const long long *)h->ditemOff, h->nItems, (int)h->nValues, kin);
+  h->launches++;
+  return DNL_OK;
+}
+
 // One increment: the kernels of the graph.
 int enqueue_step(dnl_engine *h)
 {
@@ -541,6 +563,36 @@ int enqueue_step(dnl_engine *h)
   launch_element_any(h, 0);
   launch_nodal(h);
   launch_step_end(h);
+  launch_history(h);
+  return DNL_OK;
+}
+
+// Increments a run replays between two looks at the device: every replay can
+// add a history record, so no more than the ring holds.
+int poll_chunk(const dnl_engine *h, int dflt)
+{
+  return h->histOn ? std::min(dflt, h->hist.cap) : dflt;
+}
+
+// Records written on the device since the last look, appended on the host.
+int drain_history(dnl_engine *h)
+{
+  if (!h->histOn)
+    return DNL_OK;
+  int cnt[2] = {0, 0}; // count, overflow (adjacent in the ring's memory)
+  CK(cudaMemcpyAsync(cnt, h->hist.count, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (cnt[1])
+    return fail(h, DNL_ERR_ARG, "history ring overflow (capacity %d records)", h->hist.cap);
+  if (cnt[0] > 0)
+  {
+    const size_t width = HIST_HEAD + (size_t)h->nValues, old = h->histHost.size();
+    h->histHost.resize(old + width * cnt[0]);
+    CK(cudaMemcpyAsync(h->histHost.data() + old, h->hist.rec, sizeof(double) * width * cnt[0],
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemsetAsync(h->hist.count, 0, sizeof(int), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
   return DNL_OK;
 }
 
@@ -633,92 +685,29 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   h->precision = descs[0]->precision;
   h->nInst = n;
 
-  // ---- concatenate the instances
-  std::vector<double4> x, v;
-  std::vector<int> conn, emat;
+  // ---- per instance (host, O(instances)): its first node, element, material
+  // and function, the materials, the time functions and the control blocks;
+  // the node and element arrays themselves are built on the device below
+  std::vector<int4> base(n);
   std::vector<MatDev> mats;
-  std::vector<uint8_t> bc;
-  std::vector<double4> bcval;
-  std::vector<int4> bcfun;
-  std::vector<int> speedNodes;
   std::vector<double> fx, fy;
   std::vector<int> foff(1, 0);
   h->elemBegin.assign(1, 0);
   h->nodeBegin.assign(1, 0);
-  {
-    long long nn = 0, ne = 0;
-    bool anySpeed = false;
-    for (int i = 0; i < n; i++)
-    {
-      nn += descs[i]->n_nodes;
-      ne += descs[i]->n_elems;
-      if (descs[i]->bc_code)
-        for (long long k = 0; k < 3LL * descs[i]->n_nodes && !anySpeed; k++)
-          anySpeed = descs[i]->bc_code[k] == DNL_BC_SPEED;
-    }
-    x.reserve(nn);
-    v.reserve(nn);
-    bc.reserve(nn);
-    conn.reserve(((size_t)ne * h->npe + TILE - 1) / TILE * TILE);
-    emat.reserve(ne + TILE);
-    // per-node imposed speeds only when some node has one (the nodal pass
-    // reads them only where a component's code is DNL_BC_SPEED)
-    if (anySpeed)
-    {
-      bcval.reserve(nn);
-      bcfun.reserve(nn);
-    }
-    h->hasSpeed = anySpeed;
-  }
+  long long nn = 0, ne = 0;
+  bool anySpeed = false;
   for (int i = 0; i < n; i++)
   {
     const dnl_model_desc *d = descs[i];
-    const int nb = (int)x.size(), eb = (int)(conn.size() / h->npe), mb = (int)mats.size(), fb = (int)foff.size() - 1;
-    for (int k = 0; k < d->n_nodes; k++)
-    {
-      x.push_back(make_double4(d->coords[3 * k], d->coords[3 * k + 1], d->coords[3 * k + 2], 0.0));
-      if (d->v_init)
-        v.push_back(make_double4(d->v_init[3 * k], d->v_init[3 * k + 1], d->v_init[3 * k + 2], 0.0));
-      else
-        v.push_back(make_double4(0, 0, 0, 0));
-      uint8_t code = 0;
-      double4 sv = make_double4(0, 0, 0, 0);
-      int4 sf = make_int4(-1, -1, -1, -1);
-      bool speed = false;
-      if (d->bc_code)
-        for (int c = 0; c < 3; c++)
+    base[i] = make_int4((int)nn, (int)ne, (int)mats.size(), (int)foff.size() - 1);
+    // an imposed speed other than zero (an imposed zero restrains the component)
+    if (d->bc_code && d->bc_value && !anySpeed)
+      for (long long k = 0; k < 3LL * d->n_nodes; k++)
+        if (d->bc_code[k] == DNL_BC_SPEED && d->bc_value[k] != 0.0)
         {
-          int cc = d->bc_code[3 * k + c];
-          double val = d->bc_value ? d->bc_value[3 * k + c] : 0.0;
-          int fn = d->bc_func ? d->bc_func[3 * k + c] : -1;
-          if (cc == DNL_BC_SPEED && val == 0.0)
-            cc = DNL_BC_RESTRAIN; // an imposed zero speed restrains the component
-          if (cc == DNL_BC_SPEED)
-          {
-            speed = true;
-            comp(sv, c) = val;
-            (c == 0 ? sf.x : (c == 1 ? sf.y : sf.z)) = fn >= 0 ? fn + fb : -1;
-          }
-          if (cc == DNL_BC_RESTRAIN || cc == DNL_BC_SPEED)
-            code |= (uint8_t)(cc << (2 * c));
+          anySpeed = true;
+          break;
         }
-      bc.push_back(code);
-      if (h->hasSpeed)
-      {
-        bcval.push_back(sv);
-        bcfun.push_back(sf);
-      }
-      if (speed)
-        speedNodes.push_back(nb + k);
-    }
-    {
-      const size_t c0 = conn.size(), cn = (size_t)d->n_elems * h->npe;
-      conn.resize(c0 + cn);
-      for (size_t k = 0; k < cn; k++)
-        conn[c0 + k] = d->conn[k] + nb;
-    }
-    for (int e = 0; e < d->n_elems; e++)
-      emat.push_back(mb + (d->elem_mat ? d->elem_mat[e] : 0));
     for (int m = 0; m < d->n_materials; m++)
       mats.push_back(make_mat(d->materials[m]));
     for (int f = 0; f < d->n_functions; f++)
@@ -730,9 +719,6 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
       }
       foff.push_back((int)fx.size());
     }
-    h->elemBegin.push_back(eb + d->n_elems);
-    h->nodeBegin.push_back(nb + d->n_nodes);
-
     Ctl c;
     memset(&c, 0, sizeof(c));
     double rb = (d->rho_b >= 0.0 && d->rho_b <= 1.0) ? d->rho_b : 0.8182;
@@ -751,25 +737,27 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     c.t_stop = d->t_end;
     c.min_bits = INF_BITS;
     c.inc_stop = 0x7fffffffffffffffll;
-    c.elem_begin = eb;
-    c.elem_end = eb + d->n_elems;
-    c.node_begin = nb;
-    c.node_end = nb + d->n_nodes;
+    c.elem_begin = (int)ne;
+    c.elem_end = (int)(ne + d->n_elems);
+    c.node_begin = (int)nn;
+    c.node_end = (int)(nn + d->n_nodes);
     h->ctlInit.push_back(c);
+    nn += d->n_nodes;
+    ne += d->n_elems;
+    h->elemBegin.push_back((int)ne);
+    h->nodeBegin.push_back((int)nn);
   }
-  h->nN = (int)x.size();
-  h->nE = (int)(conn.size() / h->npe);
+  if (nn * 3 > 0x3fffffffLL || ne * h->npe > 0x3fffffffLL)
+  {
+    dnl_engine_destroy(h);
+    return fail(nullptr, DNL_ERR_ARG, "model too large for 32-bit point indices");
+  }
+  h->nN = (int)nn;
+  h->nE = (int)ne;
   h->nIP = h->nE * h->npe;
   h->nTiles = (h->nIP + TILE - 1) / TILE;
   h->nIPpad = h->nTiles * TILE;
-  conn.resize((size_t)h->nIPpad, 0); // whole tiles for the bulk copies (padding lanes are inactive)
-  h->nSpeed = (int)speedNodes.size();
-  h->hasSpeed = h->nSpeed > 0;
-  if (!h->hasSpeed)
-  {
-    bcval.assign(1, make_double4(0, 0, 0, 0)); // never read without imposed speeds
-    bcfun.assign(1, make_int4(-1, -1, -1, -1));
-  }
+  h->hasSpeed = anySpeed;
   h->nFunc = (int)foff.size() - 1;
   if (fx.empty())
   {
@@ -777,136 +765,219 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     fy.push_back(0.0);
   }
 
-  // ---- node -> (element, local node) slots, in element order
-  // slot of incidence k = e*npe + n in node order; within a node, elements in
-  // increasing order (the order of the reference's scatter-add, Model.C:881-898)
-  std::vector<int> off(h->nN + 1, 0), pos((size_t)h->nIP);
-  for (size_t k = 0; k < (size_t)h->nIP; k++)
-    off[conn[k] + 1]++;
-  for (int i = 0; i < h->nN; i++)
-    off[i + 1] += off[i];
+  // ---- device memory of the model: one allocation, carved in 256-byte aligned parts
+  const size_t rsz = h->precision == DNL_PREC_MIXED ? 4 : 8;
+  const size_t nN = (size_t)h->nN, nI = (size_t)n, nIPpad = (size_t)h->nIPpad, nSp = anySpeed ? nN : 1;
+  size_t total = 0;
+  auto reserve = [&](size_t bytes) {
+    const size_t o = total;
+    total += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  const size_t o_eb = reserve(sizeof(int) * (nI + 1)), o_nb = reserve(sizeof(int) * (nI + 1)),
+               o_conn = reserve(sizeof(int) * nIPpad), o_emat = reserve(sizeof(int) * (nIPpad / h->npe)),
+               o_mat = reserve(sizeof(MatDev) * mats.size()), o_off = reserve(sizeof(int) * (nN + 1)),
+               o_pos = reserve(sizeof(int) * nIPpad), o_bc = reserve(nN), o_bcval = reserve(sizeof(double4) * nSp),
+               o_bcfun = reserve(sizeof(int4) * nSp), o_speed = reserve(sizeof(int) * nSp),
+               o_fx = reserve(sizeof(double) * fx.size()), o_fy = reserve(sizeof(double) * fy.size()),
+               o_foff = reserve(sizeof(int) * foff.size()), o_nodes = reserve(sizeof(double4) * nN * 9),
+               o_mass = reserve(sizeof(double) * nN), o_ctl = reserve(sizeof(Ctl) * nI),
+               // zeroed at creation, from here to o_ip
+               o_energy = reserve(sizeof(double) * 3 * nI), o_err = reserve(sizeof(int)),
+               o_stats = reserve(sizeof(unsigned long long) * 5), o_done = reserve(sizeof(unsigned) * 2),
+               o_act = reserve(sizeof(int)), o_actlist = reserve(sizeof(int) * nI),
+               o_acttile = reserve(sizeof(int) * (nI + 1)), o_actnode = reserve(sizeof(int) * (nI + 1)),
+               o_actelem = reserve(sizeof(int) * (nI + 1)), o_due = reserve(sizeof(int)),
+               o_duelist = reserve(sizeof(int) * nI), o_dueelem = reserve(sizeof(int) * (nI + 1)),
+               o_ip = reserve((size_t)DNL_IP_NCOMP * nIPpad * rsz), o_slot = reserve((size_t)h->nIP * 4 * rsz);
+  char *A = nullptr;
   {
-    std::vector<int> fill(off.begin(), off.end() - 1);
-    for (size_t k = 0; k < (size_t)h->nIP; k++)
-      pos[k] = fill[conn[k]]++;
+    cudaError_t e = cudaMalloc((void **)&A, total);
+    if (e != cudaSuccess)
+    {
+      dnl_engine_destroy(h);
+      return fail(nullptr, DNL_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s", total, cudaGetErrorString(e));
+    }
+    h->allocs.push_back(A);
   }
-  // whole tiles for the bulk copies of the staged element pass (padding unused)
-  pos.resize((size_t)h->nIPpad, 0);
-  emat.resize((size_t)h->nIPpad / h->npe, 0);
-
-  int rc = DNL_OK;
   DevModel &M = h->M;
   M.nInst = h->nInst;
   M.nN = h->nN;
   M.nE = h->nE;
   M.nIP = h->nIP;
   M.nIPpad = h->nIPpad;
-  M.nSpeed = h->nSpeed;
   M.nFunc = h->nFunc;
-  const size_t rsz = h->precision == DNL_PREC_MIXED ? 4 : 8;
-  int *d_eb = nullptr, *d_nb = nullptr, *d_conn = nullptr, *d_emat = nullptr, *d_off = nullptr, *d_pos = nullptr;
-  int *d_speed = nullptr, *d_foff = nullptr;
-  MatDev *d_mat = nullptr;
-  uint8_t *d_bc = nullptr;
-  double4 *d_bcval = nullptr;
-  int4 *d_bcfun = nullptr;
-  double *d_fx = nullptr, *d_fy = nullptr;
-  if ((rc = upload(h, &d_eb, h->elemBegin)) || (rc = upload(h, &d_nb, h->nodeBegin)) ||
-      (rc = upload(h, &d_conn, conn)) || (rc = upload(h, &d_emat, emat)) || (rc = upload(h, &d_mat, mats)) ||
-      (rc = upload(h, &d_off, off)) || (rc = upload(h, &d_pos, pos)) || (rc = upload(h, &d_bc, bc)) ||
-      (rc = upload(h, &d_bcval, bcval)) || (rc = upload(h, &d_bcfun, bcfun)) ||
-      (rc = upload(h, &d_speed, speedNodes)) || (rc = upload(h, &d_fx, fx)) || (rc = upload(h, &d_fy, fy)) ||
-      (rc = upload(h, &d_foff, foff)) || (rc = upload(h, &M.x, x)) || (rc = dalloc(h, &M.disp, h->nN)) ||
-      (rc = dalloc(h, &M.u[0], h->nN)) || (rc = dalloc(h, &M.u[1], h->nN)) || (rc = upload(h, &M.v[0], v)) ||
-      (rc = dalloc(h, &M.v[1], h->nN)) || (rc = dalloc(h, &M.a[0], h->nN)) || (rc = dalloc(h, &M.a[1], h->nN)) ||
-      (rc = dalloc(h, &M.mass, h->nN)) || (rc = dalloc(h, &M.fout, h->nN)) ||
-      (rc = upload(h, &M.ctl, h->ctlInit)) || (rc = dalloc(h, &h->denergy, 3 * h->nInst)) ||
-      (rc = dalloc(h, &h->derr, 1)))
-  {
-    std::string e = h->err;
-    dnl_engine_destroy(h);
-    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
-    return rc;
-  }
-  // the zero node fields are cleared on the device, the second speed buffer copied there
-  {
-    const size_t nb4 = sizeof(double4) * h->nN;
-    cudaError_t e = cudaSuccess;
-    for (double4 *p : {M.disp, M.u[0], M.u[1], M.a[0], M.a[1]})
-      if (e == cudaSuccess)
-        e = cudaMemsetAsync(p, 0, nb4, h->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(M.v[1], M.v[0], nb4, cudaMemcpyDeviceToDevice, h->stream);
-    if (e != cudaSuccess)
-    {
-      dnl_engine_destroy(h);
-      return fail(nullptr, DNL_ERR_CUDA, "clearing the node fields failed: %s", cudaGetErrorString(e));
-    }
-  }
-  void *ip = nullptr, *slot = nullptr;
-  if ((rc = dalloc(h, (char **)&ip, (size_t)DNL_IP_NCOMP * h->nIPpad * rsz)) ||
-      (rc = dalloc(h, (char **)&slot, (size_t)h->nIP * 4 * rsz)))
-  {
-    std::string e = h->err;
-    dnl_engine_destroy(h);
-    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
-    return rc;
-  }
-  M.inst_elem_begin = d_eb;
-  M.inst_node_begin = d_nb;
-  M.conn = d_conn;
-  M.emat = d_emat;
-  M.mat = d_mat;
-  M.csr_off = d_off;
-  M.slot_pos = d_pos;
-  M.bc = d_bc;
-  M.bcval = d_bcval;
-  M.bcfun = d_bcfun;
-  M.speed_nodes = d_speed;
-  M.fx = d_fx;
-  M.fy = d_fy;
-  M.foff = d_foff;
-  M.ip = ip;
-  M.slot = slot;
-  cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
-  cudaMemsetAsync(h->derr, 0, sizeof(int), h->stream);
-  if ((rc = dalloc(h, &h->dstats, 5)))
-  {
-    std::string e = h->err;
-    dnl_engine_destroy(h);
-    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
-    return rc;
-  }
-  cudaMemsetAsync(h->dstats, 0, 5 * sizeof(unsigned long long), h->stream);
-  if ((rc = dalloc(h, &M.done_count, 2)))
-  {
-    std::string e = h->err;
-    dnl_engine_destroy(h);
-    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
-    return rc;
-  }
-  cudaMemsetAsync(M.done_count, 0, 2 * sizeof(unsigned), h->stream);
+  M.inst_elem_begin = (const int *)(A + o_eb);
+  M.inst_node_begin = (const int *)(A + o_nb);
+  M.conn = (const int *)(A + o_conn);
+  M.emat = (const int *)(A + o_emat);
+  M.mat = (const MatDev *)(A + o_mat);
+  M.csr_off = (const int *)(A + o_off);
+  M.slot_pos = (const int *)(A + o_pos);
+  M.bc = (const uint8_t *)(A + o_bc);
+  M.bcval = (const double4 *)(A + o_bcval);
+  M.bcfun = (const int4 *)(A + o_bcfun);
+  M.speed_nodes = (const int *)(A + o_speed);
+  M.fx = (const double *)(A + o_fx);
+  M.fy = (const double *)(A + o_fy);
+  M.foff = (const int *)(A + o_foff);
+  double4 *nodes = (double4 *)(A + o_nodes);
+  M.x = nodes;
+  M.disp = nodes + nN;
+  M.u[0] = nodes + 2 * nN;
+  M.u[1] = nodes + 3 * nN;
+  M.v[0] = nodes + 4 * nN;
+  M.v[1] = nodes + 5 * nN;
+  M.a[0] = nodes + 6 * nN;
+  M.a[1] = nodes + 7 * nN;
+  M.fout = nodes + 8 * nN;
+  M.mass = (double *)(A + o_mass);
+  M.ctl = (Ctl *)(A + o_ctl);
+  h->denergy = (double *)(A + o_energy);
+  h->derr = (int *)(A + o_err);
+  h->dstats = (unsigned long long *)(A + o_stats);
+  M.done_count = (unsigned *)(A + o_done);
   M.step_due = M.done_count + 1;
-  if ((rc = dalloc(h, &M.act_count, 1)) || (rc = dalloc(h, &M.act_list, h->nInst)) ||
-      (rc = dalloc(h, &M.act_tile_pre, h->nInst + 1)) || (rc = dalloc(h, &M.act_node_pre, h->nInst + 1)) ||
-      (rc = dalloc(h, &M.act_elem_pre, h->nInst + 1)) || (rc = dalloc(h, &M.due_count, 1)) ||
-      (rc = dalloc(h, &M.due_list, h->nInst)) || (rc = dalloc(h, &M.due_elem_pre, h->nInst + 1)))
-  {
-    std::string e = h->err;
-    dnl_engine_destroy(h);
-    snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
-    return rc;
-  }
-  cudaMemsetAsync(M.act_count, 0, sizeof(int), h->stream);
-  cudaMemsetAsync(M.act_tile_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
-  cudaMemsetAsync(M.act_node_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
-  cudaMemsetAsync(M.act_elem_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
-  cudaMemsetAsync(M.due_count, 0, sizeof(int), h->stream);
-  cudaMemsetAsync(M.due_elem_pre, 0, sizeof(int) * (h->nInst + 1), h->stream);
+  M.act_count = (int *)(A + o_act);
+  M.act_list = (int *)(A + o_actlist);
+  M.act_tile_pre = (int *)(A + o_acttile);
+  M.act_node_pre = (int *)(A + o_actnode);
+  M.act_elem_pre = (int *)(A + o_actelem);
+  M.due_count = (int *)(A + o_due);
+  M.due_list = (int *)(A + o_duelist);
+  M.due_elem_pre = (int *)(A + o_dueelem);
+  M.ip = A + o_ip;
+  M.slot = A + o_slot;
   M.stats = h->dstats;
   M.harvest_count = h->dstats + 4;
   M.harvest_stride = 1;
   M.guess_scope = DNL_GUESS_ALL;
+  cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
+
+  // ---- the caller's arrays as they come, into the read-back staging (reused later)
+  size_t rtotal = 0;
+  auto rreserve = [&](size_t bytes) {
+    const size_t o = rtotal;
+    rtotal += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  const int nScan = (h->nN + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  const size_t r_coords = rreserve(sizeof(double) * 3 * nN), r_vinit = rreserve(sizeof(double) * 3 * nN),
+               r_bcval = rreserve(sizeof(double) * 3 * nN), r_bccode = rreserve(3 * nN),
+               r_bcfun = rreserve(sizeof(int) * 3 * nN), r_conn = rreserve(sizeof(int) * (size_t)h->nIP),
+               r_emat = rreserve(sizeof(int) * (size_t)h->nE), r_base = rreserve(sizeof(int4) * nI),
+               r_count = rreserve(sizeof(int)), r_cursor = rreserve(sizeof(int) * nN),
+               r_list = rreserve(sizeof(int) * (size_t)h->nIP), r_sums = rreserve(sizeof(int) * (nScan + 1));
+  char *Rw = nullptr;
+  // a single model reserves the staging at its point state's size, so that
+  // reading the state back later needs no allocation
+  const size_t stateBytes = (size_t)DNL_IP_NCOMP * h->nIP * rsz;
+  int rc = staging(h, n == 1 ? std::max(rtotal, stateBytes) : rtotal, (void **)&Rw);
+  if (rc)
+  {
+    std::string e = h->err;
+    dnl_engine_destroy(h);
+    return fail(nullptr, rc, "%s", e.c_str());
+  }
+  BuildRaw R;
+  R.coords = (const double *)(Rw + r_coords);
+  R.vinit = (const double *)(Rw + r_vinit);
+  R.bcval = (const double *)(Rw + r_bcval);
+  R.bccode = (const int8_t *)(Rw + r_bccode);
+  R.bcfun = (const int *)(Rw + r_bcfun);
+  R.conn = (const int *)(Rw + r_conn);
+  R.emat = (const int *)(Rw + r_emat);
+  R.base = (const int4 *)(Rw + r_base);
+  R.speedCount = (int *)(Rw + r_count);
+  R.cursor = (int *)(Rw + r_cursor);
+  R.list = (int *)(Rw + r_list);
+  R.blockSums = (int *)(Rw + r_sums);
+  R.npe = h->npe;
+  cudaError_t e = cudaSuccess;
+  auto put = [&](size_t off, const void *src, size_t bytes) {
+    if (e == cudaSuccess && bytes)
+      e = cudaMemcpyAsync(Rw + off, src, bytes, cudaMemcpyHostToDevice, h->stream);
+  };
+  auto fill = [&](size_t off, int byte, size_t bytes) {
+    if (e == cudaSuccess && bytes)
+      e = cudaMemsetAsync(Rw + off, byte, bytes, h->stream);
+  };
+  for (int i = 0; i < n; i++)
+  {
+    const dnl_model_desc *d = descs[i];
+    const size_t nb = (size_t)base[i].x, nni = (size_t)d->n_nodes, k3 = 3 * nb, n3 = 3 * nni;
+    put(r_coords + sizeof(double) * k3, d->coords, sizeof(double) * n3);
+    if (d->v_init)
+      put(r_vinit + sizeof(double) * k3, d->v_init, sizeof(double) * n3);
+    else
+      fill(r_vinit + sizeof(double) * k3, 0, sizeof(double) * n3);
+    if (d->bc_code)
+      put(r_bccode + k3, d->bc_code, n3);
+    else
+      fill(r_bccode + k3, 0, n3);
+    if (d->bc_value)
+      put(r_bcval + sizeof(double) * k3, d->bc_value, sizeof(double) * n3);
+    else
+      fill(r_bcval + sizeof(double) * k3, 0, sizeof(double) * n3);
+    if (d->bc_func)
+      put(r_bcfun + sizeof(int) * k3, d->bc_func, sizeof(int) * n3);
+    else
+      fill(r_bcfun + sizeof(int) * k3, 0xff, sizeof(int) * n3); // -1: no function
+    const size_t eb = (size_t)base[i].y;
+    put(r_conn + sizeof(int) * eb * h->npe, d->conn, sizeof(int) * (size_t)d->n_elems * h->npe);
+    if (d->elem_mat)
+      put(r_emat + sizeof(int) * eb, d->elem_mat, sizeof(int) * (size_t)d->n_elems);
+    else
+      fill(r_emat + sizeof(int) * eb, 0, sizeof(int) * (size_t)d->n_elems);
+  }
+  put(r_base, base.data(), sizeof(int4) * nI);
+  fill(r_count, 0, sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_eb, h->elemBegin.data(), sizeof(int) * (nI + 1), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_nb, h->nodeBegin.data(), sizeof(int) * (nI + 1), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_mat, mats.data(), sizeof(MatDev) * mats.size(), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_fx, fx.data(), sizeof(double) * fx.size(), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_fy, fy.data(), sizeof(double) * fy.size(), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_foff, foff.data(), sizeof(int) * foff.size(), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A + o_ctl, h->ctlInit.data(), sizeof(Ctl) * nI, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(A + o_energy, 0, o_ip - o_energy, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(A + o_off, 0, sizeof(int) * (nN + 1), h->stream);
+
+  // ---- the model built on the device
+  if (e == cudaSuccess)
+  {
+    const int tb = 256;
+    k_build_nodes<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(M, R, anySpeed ? 1 : 0);
+    k_build_elems<<<(h->nIPpad + tb - 1) / tb, tb, 0, h->stream>>>(M, R, h->nIPpad);
+    int *offp = const_cast<int *>(M.csr_off) + 1;
+    k_scan_blocks<<<nScan, SCAN_BLOCK, 0, h->stream>>>(offp, h->nN, R.blockSums);
+    k_scan_sums<<<1, 32, 0, h->stream>>>(R.blockSums, nScan);
+    k_scan_add<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(offp, h->nN, R.blockSums);
+    k_slot_cursor<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(M, R);
+    k_slot_fill<<<(h->nIP + tb - 1) / tb, tb, 0, h->stream>>>(M, R);
+    k_slot_sort<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(M, R);
+    e = cudaGetLastError();
+  }
+  int nSpeed = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&nSpeed, R.speedCount, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+  {
+    dnl_engine_destroy(h);
+    return fail(nullptr, DNL_ERR_CUDA, "model build failed: %s", cudaGetErrorString(e));
+  }
+  h->nSpeed = nSpeed;
+  M.nSpeed = nSpeed;
   // batches start on a persistent variant: the plain one launches a block per
   // tile of the whole batch, which the tail of a batch (few instances still
   // running) cannot afford
@@ -936,22 +1007,19 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     if ((rc = upload(h, &M.pv, pv)) || (rc = upload(h, &M.pv2, pv)) || (rc = dalloc(h, &M.pislot, h->nIP)) ||
         (rc = dalloc(h, &M.blockmax, h->piGrid)))
     {
-      std::string e = h->err;
+      std::string em = h->err;
       dnl_engine_destroy(h);
-      snprintf(g_create_err, sizeof(g_create_err), "%s", e.c_str());
+      snprintf(g_create_err, sizeof(g_create_err), "%s", em.c_str());
       return rc;
     }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+    {
+      dnl_engine_destroy(h);
+      return fail(nullptr, DNL_ERR_CUDA, "upload failed");
+    }
   }
-  if (cudaMallocHost((void **)&h->hctl, sizeof(Ctl) * h->nInst) != cudaSuccess)
-  {
-    dnl_engine_destroy(h);
-    return fail(nullptr, DNL_ERR_CUDA, "cudaMallocHost failed");
-  }
-  if (cudaStreamSynchronize(h->stream) != cudaSuccess)
-  {
-    dnl_engine_destroy(h);
-    return fail(nullptr, DNL_ERR_CUDA, "upload failed");
-  }
+  // host mirror of the control blocks (small: plain memory)
+  h->hctl = new Ctl[h->nInst];
   *out = h;
   return DNL_OK;
 }
@@ -965,6 +1033,7 @@ int dnl_engine_create(const dnl_model_desc *desc, dnl_engine **out)
 namespace
 {
 void free_items(dnl_engine *h);
+void drop_graph(dnl_engine *h);
 }
 
 int dnl_engine_destroy(dnl_engine *h)
@@ -981,9 +1050,10 @@ int dnl_engine_destroy(dnl_engine *h)
     cudaFree(p);
   if (h->dstage)
     cudaFree(h->dstage);
+  if (h->histMem)
+    cudaFree(h->histMem);
   free_items(h);
-  if (h->hctl)
-    cudaFreeHost(h->hctl);
+  delete[] h->hctl;
   if (h->stream)
     cudaStreamDestroy(h->stream);
   delete h;
@@ -1047,7 +1117,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
     long long steps = 0;
     for (;;)
     {
-      const int chunk = 16;
+      const int chunk = poll_chunk(h, 16);
       for (int s = 0; s < chunk; s++)
       {
         launch_bc_prep(h);
@@ -1057,6 +1127,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
         launch_nodal(h);
         CK(cudaEventRecord(e[2], h->stream));
         launch_step_end(h);
+        launch_history(h);
         CK(cudaEventRecord(e[3], h->stream));
         CK(cudaEventSynchronize(e[3]));
         float t01, t12, t23;
@@ -1070,7 +1141,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
         if (max_incs > 0 && steps >= max_incs)
           break;
       }
-      if ((rc = sync_ctl(h)))
+      if ((rc = sync_ctl(h)) || (rc = drain_history(h)))
         return rc;
       bool any = false;
       for (int i = 0; i < h->nInst; i++)
@@ -1084,7 +1155,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
     h->times[1] = acc[1];
     h->times[2] = acc[2];
   }
-  else if (max_incs > 0)
+  else if (max_incs > 0 && !h->histOn)
   {
     // known number of increments: replay the graph without polling
     for (int64_t s = 0; s < max_incs; s++)
@@ -1095,7 +1166,9 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
   }
   else
   {
-    const int chunk = 64;
+    // until every instance stops (its end time, the pause time, or the
+    // increment budget that CTL_LIMITS set), looking at the device every chunk
+    const int chunk = poll_chunk(h, 64);
     for (;;)
     {
       for (int s = 0; s < chunk; s++)
@@ -1103,7 +1176,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
         CK(cudaGraphLaunch(h->graphExec, h->stream));
         h->launches += h->launchesPerStep;
       }
-      if ((rc = sync_ctl(h)))
+      if ((rc = sync_ctl(h)) || (rc = drain_history(h)))
         return rc;
       // an instance that fails stops alone; the others of a batch go on
       bool any = false;
@@ -1648,6 +1721,13 @@ int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_
   if (!h || n < 0 || (n > 0 && !items))
     return DNL_ERR_ARG;
   CK(cudaStreamSynchronize(h->stream));
+  if (h->histOn)
+  {
+    // the records hold the items: a new list needs dnl_engine_set_history again
+    drop_graph(h);
+    h->histOn = false;
+    h->histHost.clear();
+  }
   free_items(h);
   std::vector<int4> it(n);
   std::vector<long long> off(n);
@@ -1660,7 +1740,7 @@ int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_
     switch (a.kind)
     {
     case DNL_ITEM_NODE:
-      if (a.index < 0 || a.index >= h->nN || a.field < DNL_NODE_COORDS || a.field > DNL_NODE_SPEED_PREV)
+      if (a.index < 0 || a.index >= h->nN || a.field < DNL_NODE_COORDS || a.field > DNL_NODE_ACCEL_PREV)
         return fail(h, DNL_ERR_ARG, "item %d: node %d / field %d out of range", k, a.index, a.field);
       width = 3;
       break;
@@ -1726,6 +1806,80 @@ int dnl_engine_gather_items(dnl_engine *h, double *out)
   CK(cudaMemcpyAsync(h->hvalues, h->dvalues, sizeof(double) * h->nValues, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   memcpy(out, h->hvalues, sizeof(double) * h->nValues);
+  return DNL_OK;
+}
+
+int dnl_engine_set_history(dnl_engine *h, const dnl_history_schedule *sched, int32_t n, int32_t capacity)
+{
+  if (!h || n < 0 || n > 64 || (n > 0 && !sched) || capacity < 0)
+    return DNL_ERR_ARG;
+  if (n > 0 && h->nInst != 1)
+    return fail(h, DNL_ERR_UNSUPPORTED, "history records on the device are kept for single models");
+  int rc = sync_ctl(h);
+  if (rc)
+    return rc;
+  drop_graph(h); // the increment's graph gains or loses the history kernel
+  h->histOn = false;
+  h->histHost.clear();
+  if (h->histMem)
+  {
+    cudaFree(h->histMem);
+    h->histMem = nullptr;
+  }
+  if (n == 0)
+    return DNL_OK;
+  const int cap = capacity > 0 ? capacity : 64;
+  const size_t width = HIST_HEAD + (size_t)h->nValues;
+  // one allocation: count, overflow, last increment, the schedules, the records
+  const size_t offLast = 16, offSched = 32, offRec = offSched + ((sizeof(double) * 3 * n + 255) / 256) * 256;
+  const size_t bytes = offRec + sizeof(double) * width * cap;
+  CK(cudaMalloc(&h->histMem, bytes));
+  char *base = (char *)h->histMem;
+  HistRing &H = h->hist;
+  H.nSched = n;
+  H.cap = cap;
+  H.count = (int *)base;
+  H.overflow = (int *)base + 1;
+  H.last = (long long *)(base + offLast);
+  H.start = (double *)(base + offSched);
+  H.next = H.start + n;
+  H.save = H.next + n;
+  H.rec = (double *)(base + offRec);
+  std::vector<double> tab(3 * (size_t)n);
+  for (int j = 0; j < n; j++)
+  {
+    tab[j] = sched[j].start;
+    tab[n + j] = sched[j].next;
+    tab[2 * n + j] = sched[j].save;
+  }
+  const Ctl &c = h->hctl[0];
+  const long long committed = c.inc - ((c.prepared && c.active) ? 1 : 0);
+  CK(cudaMemsetAsync(base, 0, offSched, h->stream));
+  CK(cudaMemcpyAsync(H.last, &committed, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(H.start, tab.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->histOn = true;
+  return DNL_OK;
+}
+
+int dnl_engine_history_records(dnl_engine *h, double *out, int64_t max_records, int64_t *n_records)
+{
+  if (!h || !n_records)
+    return DNL_ERR_ARG;
+  const size_t width = HIST_HEAD + (size_t)h->nValues;
+  const int64_t pending = h->histOn ? (int64_t)(h->histHost.size() / width) : 0;
+  if (!out)
+  {
+    *n_records = pending;
+    return DNL_OK;
+  }
+  const int64_t k = std::max<int64_t>(0, std::min(pending, max_records));
+  if (k > 0)
+  {
+    memcpy(out, h->histHost.data(), sizeof(double) * width * k);
+    h->histHost.erase(h->histHost.begin(), h->histHost.begin() + (ptrdiff_t)(width * k));
+  }
+  *n_records = k;
   return DNL_OK;
 }
 

@@ -503,6 +503,8 @@ class DynELA:
         self._engine = None
         self._cache = {}
         self._node_index = {}
+        # history records kept on the device (False: the run stops at every save time)
+        self._use_history_ring = True
 
     # ---- model building (DynELA.C:160-297, 380-476)
     def createNode(self, number, x, y=None, z=None):
@@ -690,6 +692,11 @@ class DynELA:
                        + "\n")
         self._plan_items()
         self._write_histories(initial=True)
+        # the history records of the increments are kept on the device and the
+        # run does not stop at their save times (dnl_engine_set_history)
+        ring = self._use_history_ring and 0 < len(self._histories) <= 64
+        if ring:
+            eng.set_history([(h.startTime, h.nextTime, h.saveTime) for h in self._histories], capacity=256)
         self._vtk_index = 0
         # the initial result file (DynELA::solve -> writeResultFile after initSolve, DynELA.C:745)
         self._write_result_file(prev=False)
@@ -699,17 +706,20 @@ class DynELA:
             if c["done"] or c["time"] >= t_end:
                 break
             t = c["time"]
-            if any(h.saveTime > 0 and h.nextTime <= t for h in self._histories) or self._result_due(t):
+            if (not ring and any(h.saveTime > 0 and h.nextTime <= t for h in self._histories)) or self._result_due(t):
                 # an increment passed more than one save time: the reference writes
                 # again after the next increment (its next time lags behind)
                 eng.run(t_pause=t_end, max_incs=1)
             else:
-                pauses = [h.nextTime for h in self._histories if h.saveTime > 0]
+                pauses = [] if ring else [h.nextTime for h in self._histories if h.saveTime > 0]
                 if self._next_save <= self.saveTimes[1]:
                     pauses.append(self._next_save)
                 eng.run(t_pause=min(pauses) if pauses else t_end)
             self._cache = {}
-            self._write_histories()
+            if ring:
+                self._write_history_records()
+            else:
+                self._write_histories()
             self._write_result_file(prev=True)
         c = eng.control()
         print(f"{self.name} inc={c['increment']} time={c['time']:8.4E} timeStep={c['time_step']:8.4E}")
@@ -806,12 +816,14 @@ class DynELA:
         o = self._item_off[key]
         return self._cache["items"][o:o + _abi.ITEM_WIDTH[key[0]]]
 
-    def _item_value(self, kind, target, ip, field):
+    def _item_value(self, kind, target, ip, field, rec=None):
+        """An item's value now (rec None) or in a device record (dict of
+        increment, time_step; the values are in self._cache["items"])."""
         eng = self._engine
+        c = rec if rec is not None else eng.control()
         if kind == "global":
-            c = eng.control()
             if field in (Field.timeStep, Field.realTimeStep):
-                return c["last_time_step"]
+                return c["time_step"] if rec is not None else c["last_time_step"]
             if field == Field.kineticEnergy:
                 # Model::getTotalKineticEnergy on field0, written before the swap (Explicit.C:539-552)
                 f = _abi.NODE_SPEED_PREV if c["increment"] > 0 else _abi.NODE_SPEED
@@ -821,7 +833,7 @@ class DynELA:
             f, suf = self._node_item(field)
             # inside the loop the reference writes before its field swap
             # (Explicit.C:539-552): field0 is then the start of the increment
-            if f in _abi.NODE_PREV and eng.control()["increment"] > 0:
+            if f in _abi.NODE_PREV and c["increment"] > 0:
                 f = _abi.NODE_PREV[f]
             row = self._gathered((_abi.ITEM_NODE, f, self._node_index[target]))
             return float(np.linalg.norm(row)) if suf == "" else float(row["XYZ".index(suf)])
@@ -853,6 +865,22 @@ class DynELA:
                 sym = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
                 return t[sym[i][j]]
         raise NotImplementedError(f"point field {name}")
+
+    def _write_history_records(self):
+        """The lines of the records the device kept since the last look: for
+        each record, every file whose schedule was due (its bit in the mask)."""
+        for t, inc, dt, mask, values in self._engine.history_records():
+            self._cache = {"items": values}
+            rec = {"increment": inc, "time_step": dt}
+            for j, h in enumerate(self._histories):
+                if not (mask >> j) & 1:
+                    continue
+                h.nextTime += h.saveTime
+                vals = [self._item_value(kind, target, ip, field, rec) for _, kind, target, ip, field in h.items]
+                h._f.write("%10.7E " % t + "".join("%10.7E " % x for x in vals) + "\n")
+            self._cache = {}
+        for h in self._histories:
+            h._f.flush()
 
     def _write_histories(self, initial=False):
         t = self._engine.control()["time"]

@@ -52,6 +52,14 @@ NODE_U_PREV, NODE_ACCEL_PREV = 8, 9
 # (before its field swap): the buffer of before the last increment
 NODE_PREV = {NODE_U: NODE_U_PREV, NODE_SPEED: NODE_SPEED_PREV, NODE_ACCEL: NODE_ACCEL_PREV}
 
+# device history records (dnl_engine_set_history): header words of a record
+HIST_HEAD = 5
+
+
+class HistorySchedule(ctypes.Structure):
+    _fields_ = [("start", ctypes.c_double), ("next", ctypes.c_double), ("save", ctypes.c_double)]
+
+
 # node averages of the point state (dnl_engine_node_averages)
 NODE_AVG_VON_MISES = 64
 
@@ -300,6 +308,8 @@ def load_library():
         "dnl_engine_set_items": (ctypes.c_int, [vp, ctypes.POINTER(Item), i32, ctypes.POINTER(i64)]),
         "dnl_engine_gather_items": (ctypes.c_int, [vp, pd]),
         "dnl_engine_node_averages": (ctypes.c_int, [vp, ctypes.POINTER(i32), i32, pd]),
+        "dnl_engine_set_history": (ctypes.c_int, [vp, ctypes.POINTER(HistorySchedule), i32, i32]),
+        "dnl_engine_history_records": (ctypes.c_int, [vp, pd, i64, ctypes.POINTER(i64)]),
         "dnl_engine_write_vtk": (ctypes.c_int, [vp, i32, ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(i32),
                                                 i32, i32]),
         "dnl_engine_set_timing": (ctypes.c_int, [vp, i32]),

@@ -146,6 +146,25 @@ class Engine:
         self._check(self._lib.dnl_engine_write_vtk(self.h, int(instance), os.fsencode(path), title.encode(), c,
                                                    len(codes), int(bool(prev))))
 
+    def set_history(self, schedules, capacity=0):
+        """History records on the device: schedules [(start, next, save)],
+        the save rule of HistoryFile::save evaluated after every increment;
+        a record holds the items of set_items()."""
+        arr = (_abi.HistorySchedule * max(1, len(schedules)))(*[_abi.HistorySchedule(*map(float, s))
+                                                                for s in schedules])
+        self._check(self._lib.dnl_engine_set_history(self.h, arr, len(schedules), int(capacity)))
+
+    def history_records(self):
+        """The records waiting, oldest first: a list of (time, increment,
+        time step, due mask, values)."""
+        n = ctypes.c_int64()
+        self._check(self._lib.dnl_engine_history_records(self.h, None, 0, ctypes.byref(n)))
+        width = _abi.HIST_HEAD + getattr(self, "_n_values", 0)
+        buf = np.zeros((max(1, n.value), width))
+        self._check(self._lib.dnl_engine_history_records(self.h, _pd(buf), n.value, ctypes.byref(n)))
+        return [(r[0], int(r[1]), r[2], int(r[3]) | (int(r[4]) << 32), r[_abi.HIST_HEAD:])
+                for r in buf[:n.value]]
+
     def energies(self, instance=0):
         out = np.zeros(3)
         self._check(self._lib.dnl_engine_energies(self.h, int(instance), _pd(out)))

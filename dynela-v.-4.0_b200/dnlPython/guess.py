@@ -126,7 +126,10 @@ def compare(desc, net, warm_incs, incs, scope=_abi.GUESS_ALL):
     Returns, per mode, the Newton evaluations per yielding point and per point
     of the scope, the FP64 re-solves and the element-pass time per increment,
     and the relative differences of the guessed run's stress, plastic strain
-    and coordinates from the plain run's."""
+    and coordinates from the plain run's.  `perfect_guess_bound`: what a
+    perfect network that costs nothing could save at most — every point of
+    the scope down to the one evaluation that confirms the root — as a
+    fraction of all the return's evaluations in the plain run."""
     out, ref = {}, None
     for name, mode in (("plain", _abi.MODE_STATS), ("guess", _abi.MODE_GUESS)):
         with Engine(desc) as e:
@@ -146,6 +149,9 @@ def compare(desc, net, warm_incs, incs, scope=_abi.GUESS_ALL):
                              evals_per_scope_point=sev / max(sc, 1),
                              fp64_resolve_rate=c["fp64_resolves"] / max(pl, 1),
                              element_ms=tm["element_ms"] / max(incs, 1))
+            if name == "plain":
+                out["perfect_guess_bound"] = dict(evaluations_saved=int(sev - sc),
+                                                  fraction_of_all_evaluations=(sev - sc) / max(ev, 1))
             ips = e.ips()
             s = ips[_abi.IP_STRESS:_abi.IP_STRESS + 6]
             ep = ips[_abi.IP_EPSP]

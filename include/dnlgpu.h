@@ -244,6 +244,29 @@ typedef struct
 int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_t *n_values);
 int dnl_engine_gather_items(dnl_engine *h, double *out);
 
+/* History records kept on the device, so that a run does not stop at save
+ * times (single models).  Each schedule follows HistoryFile::save
+ * (HistoryFile.C:292-317): at the end of every increment, after the time
+ * update (Explicit::endStep, Explicit.C:539-552), it is due when
+ * !(time > start && time < next), and next then moves on by save.  An
+ * increment with a schedule due appends one record to a ring of `capacity`
+ * records on the device (0: 64): DNL_HIST_HEAD doubles — time, increment,
+ * the increment's time step, the mask of the due schedules as two 32-bit
+ * halves (schedule j is bit j, j < 64) — then the values of the items of
+ * dnl_engine_set_items, as dnl_engine_gather_items lays them out.  Runs
+ * look at the device at least every `capacity` increments and move the
+ * records to the host; dnl_engine_history_records hands them out, oldest
+ * first (out = NULL: only the number waiting).  Calling dnl_engine_set_items
+ * again stops the records (their width changes); n = 0 stops them.  No
+ * counterpart in the reference, which writes its history files on the host
+ * inside every increment. */
+#define DNL_HIST_HEAD 5
+typedef struct dnl_history_schedule {
+  double start, next, save; /* HistoryFile _startTime, _nextTime, _saveTime */
+} dnl_history_schedule;
+int dnl_engine_set_history(dnl_engine *h, const dnl_history_schedule *schedules, int32_t n, int32_t capacity);
+int dnl_engine_history_records(dnl_engine *h, double *out, int64_t max_records, int64_t *n_records);
+
 /* Nodal values of point-state quantities, extracted as the reference does for
  * its node fields and result files (Node::fieldScalar / fieldSymTensor2,
  * Node.C:244-365): at each node, the values of the Gauss points of every

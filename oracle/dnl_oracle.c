@@ -215,6 +215,19 @@ orc_model *orc_create(const dnl_model_desc *d)
   if (d->v_init)
     for (long k = 0; k < n3; k++)
       m->fv[0][k] = m->fv[1][k] = d->v_init[k];
+  /* Model::initSolve then applies the constant conditions too (Model.C:429,
+     BoundaryCondition.C:131-150, constant after initial): a node under an
+     imposed speed takes that condition's whole vector (its imposed components,
+     zero elsewhere, before any time function). */
+  for (long i = 0; i < m->nN; i++)
+  {
+    int speed = 0;
+    for (int c = 0; c < 3; c++)
+      speed |= m->bc[3 * i + c] == DNL_BC_SPEED;
+    if (speed)
+      for (int c = 0; c < 3; c++)
+        m->fv[0][3 * i + c] = m->fv[1][3 * i + c] = m->bc[3 * i + c] == DNL_BC_SPEED ? m->bcv[3 * i + c] : 0.0;
+  }
   m->f0 = 0;
 
   /* Solver settings and Chung-Hulbert parameters (Explicit.C:86-104). */

@@ -67,6 +67,8 @@ def lib():
         L.ref_timer.restype = ctypes.c_double
         L.ref_timer.argtypes = [vp, ctypes.c_char_p]
         L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_point_kinematics.argtypes = [vp, ctypes.c_long, pd]
+        L.ref_rotation_orthogonality.argtypes = [vp, pd]
         L.ref_enable_vtk.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.ref_write_final_vtk.argtypes = [vp]
         L.ref_destroy.argtypes = [vp]
@@ -128,6 +130,18 @@ class RefModel:
 
     def element_pass(self, dt):
         assert lib().ref_element_pass(self.h, float(dt)) == 0
+
+    def point_kinematics(self, q):
+        """StrainInc (6) and R (3x3) of point q after the last element pass."""
+        out = np.zeros(15)
+        assert lib().ref_point_kinematics(self.h, int(q), _pd(out)) == 0
+        return out[:6], out[6:].reshape(3, 3)
+
+    def rotation_orthogonality(self):
+        """(max |R^T R - I| over the points after the last element pass, that point)."""
+        out = np.zeros(2)
+        assert lib().ref_rotation_orthogonality(self.h, _pd(out)) == 0
+        return out[0], int(out[1])
 
     def courant(self):
         return lib().ref_courant(self.h)

@@ -641,6 +641,54 @@ int ref_get_ips(void *h, double *out)
   return DNL_OK;
 }
 
+/* Intermediate values of one integration point after the last element pass,
+ * for inspection: StrainInc (6, SymTensor2 order) then R (9, row-major). */
+int ref_point_kinematics(void *h, long q, double *out15)
+{
+  RefModel *m = (RefModel *)h;
+  if (m == nullptr || m != g_model || q < 0 || q >= m->nE * m->npe)
+    return DNL_ERR_ARG;
+  IntegrationPoint *ip = m->dyn->model.elements(q / m->npe)->integrationPoints(q % m->npe);
+  for (int k = 0; k < 6; k++)
+    out15[k] = symComp(ip->StrainInc, k);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      out15[6 + 3 * i + j] = ip->R(i, j);
+  return DNL_OK;
+}
+
+/* The largest departure from orthogonality, max |R^T R - I|, of the rotation
+ * of every integration point after the last element pass (Tensor2::
+ * polarCuppenLnU, Tensor2.C:1442-1457); out2 = {value, point}. */
+int ref_rotation_orthogonality(void *h, double *out2)
+{
+  RefModel *m = (RefModel *)h;
+  if (m == nullptr || m != g_model)
+    return DNL_ERR_ARG;
+  double worst = 0.0;
+  long at = -1;
+  for (long e = 0; e < m->nE; e++)
+    for (int g = 0; g < m->npe; g++)
+    {
+      const Tensor2 &R = m->dyn->model.elements(e)->integrationPoints(g)->R;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+        {
+          double s = (i == j) ? -1.0 : 0.0;
+          for (int k = 0; k < 3; k++)
+            s += R(k, i) * R(k, j);
+          if (fabs(s) > worst)
+          {
+            worst = fabs(s);
+            at = e * m->npe + g;
+          }
+        }
+    }
+  out2[0] = worst;
+  out2[1] = (double)at;
+  return DNL_OK;
+}
+
 int ref_set_ips(void *h, const double *in)
 {
   RefModel *m = (RefModel *)h;

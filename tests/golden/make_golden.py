@@ -148,6 +148,66 @@ def full_run_case(mesh, checkpoints, threads=None):
     print(f"fullsize_{mesh}_incs ok")
 
 
+def oracle_values(mesh):
+    """The C restatement (oracle/dnl_oracle.c, FP64) on a full-size run
+    fixture's model, stored in the fixture at every checkpoint: its values at
+    the sampled nodes and points and its whole-field sums (`*_orc`,
+    `*_orc_sums`), and its distance to the reference measured as the tests
+    measure the engine's (`*_onoise`, `*_osums`, helpers.full_size_errors).
+    The reference's rotation is inaccurate where two principal stretches
+    nearly coincide (polar_defect_case), which moves its runs away from any
+    accurate polar decomposition; the restatement's values are the strict
+    yardstick of the engine's runs, its distance the bound against the
+    reference."""
+    import oracle
+    path = os.path.join(HERE, f"fullsize_{mesh}_incs.npz")
+    data = {k: v for k, v in np.load(path).items() if not k.endswith(("_onoise", "_osums", "_orc", "_orc_sums"))}
+    desc = full_desc(mesh)
+    nodes, ips = data["sample_nodes"], data["sample_ips"]
+    with oracle.OracleModel(desc) as o:
+        o.init()
+        done = 0
+        for k in data["checkpoints"]:
+            done += o.run(max_incs=int(k) - done)
+            clean = dict(data)
+            for name, (err, serr) in helpers.full_size_errors(o, clean, f"inc{k}_").items():
+                data[f"inc{k}_{name}_onoise"] = err
+                data[f"inc{k}_{name}_osums"] = serr
+            for name, f in helpers.FULL_NODE_FIELDS:
+                a = o.nodes(f)
+                data[f"inc{k}_{name}_orc"] = a[nodes]
+                data[f"inc{k}_{name}_orc_sums"] = helpers.field_sums(a)
+            ip = o.ips()
+            data[f"inc{k}_ips_orc"] = ip[:, ips]
+            data[f"inc{k}_ips_orc_sums"] = helpers.field_sums(ip.T)
+            print(f"oracle {mesh} increment {k}: distance to the reference " +
+                  " ".join(f"{n} {data[f'inc{k}_{n}_onoise'].max():.1e}" for n in ("disp", "speed", "force", "ips")),
+                  flush=True)
+    np.savez_compressed(path, **data)
+
+
+def polar_defect_case():
+    """One element cut from the reference's own run of the 153,600-element
+    bar at increment 17 (element 3090: its nodes' coordinates and increments,
+    its points' state, the time step).  At its Gauss point 0 the two lateral
+    principal stretches differ by ~1e-12 (uniaxial compression in the impact
+    zone) and the reference's eigen-solver returns eigenvectors that are not
+    orthonormal, so its U, and the rotation R = F U^-1 (Tensor2::
+    polarExtractLnU, Tensor2.C:1237-1313), are off by ~2e-3."""
+    desc = full_desc("taylor3d_153600")
+    e = 3090
+    with ref.RefModel(desc, threads=os.cpu_count()) as r:
+        r.init()
+        r.run(max_incs=17)
+        x, u = r.nodes(_abi.NODE_COORDS), r.nodes(_abi.NODE_U)
+        ips = r.ips()[:, e * 8:(e + 1) * 8]
+        dt = r.control()["time_step"]
+    nodes = desc.conn[e]
+    np.savez_compressed(os.path.join(HERE, "polar_defect_element.npz"), coords=x[nodes], u=u[nodes], ips=ips,
+                        dt=np.array(dt), element=np.array(e), increment=np.array(17))
+    print("polar_defect_element ok")
+
+
 def full_pass_case(mesh, seed, dt=4e-9, threads=None):
     """One element pass of a full-size mesh on a seeded plastic state and
     displacement increment (helpers.random_point_state / random_increment,
@@ -268,6 +328,12 @@ CASES = {
     "vtk_hex": lambda: vtk_case("vtk_hex", helpers.case_hex_speed(), 4),
     "fullsize_taylor3d_153600_incs": lambda: full_run_case("taylor3d_153600", [1, 10, 50]),
     "fullsize_taylor3d_153600_elempass": lambda: full_pass_case("taylor3d_153600", seed=51),
+    # the C oracle's values and distance to the reference at each checkpoint (added to the run fixtures)
+    "oracle_values_taylor3d_153600": lambda: oracle_values("taylor3d_153600"),
+    "oracle_values_plate_necking_491520": lambda: oracle_values("plate_necking_491520"),
+    "oracle_values_bar_necking_1198080": lambda: oracle_values("bar_necking_1198080"),
+    # the reference's inaccurate rotation at nearly repeated principal stretches
+    "polar_defect_element": polar_defect_case,
     "fullsize_plate_necking_491520_incs": lambda: full_run_case("plate_necking_491520", [1, 5, 10]),
     "fullsize_plate_necking_491520_elempass": lambda: full_pass_case("plate_necking_491520", seed=53),
     "fullsize_bar_necking_1198080_incs": lambda: full_run_case("bar_necking_1198080", [1, 5, 10]),

@@ -153,44 +153,80 @@ def entry_errors(a, b, scale, floor=1e-4):
     return (np.abs(a - b) / (np.abs(b) + floor * scale + 1e-300)).max(axis=1)
 
 
-def sums_errors(a_sums, b_sums):
+def group_scale(values, groups=()):
+    """Per component, the largest of `values` over its group: components
+    of one quantity (a nodal vector's 3, a point-state tensor's 6) share a
+    scale, so that a component that is itself at the noise level of the
+    quantity is measured against the quantity."""
+    out = np.array(values, dtype=np.float64)
+    for b, n in groups:
+        out[b:b + n] = out[b:b + n].max()
+    return out
+
+
+NODE_GROUPS = ((0, 3),)
+IP_GROUPS = ((0, 6), (6, 6), (12, 6))
+
+
+def sums_errors(a_sums, b_sums, groups=()):
     """Whole-field checks from field_sums: the sums of magnitudes and the
     largest magnitudes relative to themselves, the signed sums relative to
-    the sum of magnitudes (a signed sum may cancel)."""
+    the sum of magnitudes (a signed sum may cancel); with `groups`, relative
+    to their group's largest."""
     a, b = np.asarray(a_sums), np.asarray(b_sums)
-    den = np.maximum(b[1], 1e-300)
+    den = np.maximum(group_scale(b[1], groups), 1e-300)
     return np.concatenate([np.abs(a[0] - b[0]) / den, np.abs(a[1] - b[1]) / den,
-                           np.abs(a[2] - b[2]) / np.maximum(b[2], 1e-300)])
+                           np.abs(a[2] - b[2]) / np.maximum(group_scale(b[2], groups), 1e-300)])
 
 
 FULL_NODE_FIELDS = (("coords", _abi.NODE_COORDS), ("disp", _abi.NODE_DISP), ("speed", _abi.NODE_SPEED),
                     ("u", _abi.NODE_U), ("accel", _abi.NODE_ACCEL), ("force", _abi.NODE_FORCE))
 FULL_ENTRY_RTOL = 1e-6
 FULL_SUMS_RTOL = 1e-9
+# where the problem's conditioning puts the C restatement further than the
+# bounds above from the reference, the engine may be this many times as far
+FULL_NOISE_FACTOR = 4.0
 
 
-def check_full_size(m, z, prefix, what):
+def full_size_errors(m, z, prefix, source=""):
     """A model (engine or oracle: nodes(field), ips()) against a full-size
-    fixture's checkpoint `prefix`: the sampled entries of every nodal field
-    and of the point state by entry_errors < FULL_ENTRY_RTOL, the sums over
-    the whole field by sums_errors < FULL_SUMS_RTOL.  Returns the worst errors."""
+    fixture's checkpoint `prefix`: per field, the entry errors of its sampled
+    entries per component (entry_errors, the floor against its group's
+    largest magnitude) and the errors of its whole-field sums (sums_errors,
+    by group).  source "" compares with the reference's values, "_orc" with
+    the C restatement's stored beside them."""
     nodes, ips = z["sample_nodes"], z["sample_ips"]
-    worst = {}
+    out = {}
     for name, f in FULL_NODE_FIELDS:
         a = m.nodes(f)
-        sums = z[f"{prefix}{name}_sums"]
-        err = entry_errors(a[nodes].T, z[f"{prefix}{name}"].T, sums[2])
-        serr = sums_errors(field_sums(a), sums)
-        worst[name] = (err.max(), serr.max())
-        assert err.max() < FULL_ENTRY_RTOL, (what, name, err)
-        assert serr.max() < FULL_SUMS_RTOL, (what, name, serr)
+        sums = z[f"{prefix}{name}{source}_sums"]
+        scale = group_scale(z[f"{prefix}{name}_sums"][2], NODE_GROUPS)
+        out[name] = (entry_errors(a[nodes].T, z[f"{prefix}{name}{source}"].T, scale),
+                     sums_errors(field_sums(a), sums, NODE_GROUPS))
     ip = m.ips()
-    sums = z[f"{prefix}ips_sums"]
-    err = entry_errors(ip[:, ips], z[f"{prefix}ips"], sums[2])
-    serr = sums_errors(field_sums(ip.T), sums)
-    worst["ips"] = (err.max(), serr.max())
-    assert err.max() < FULL_ENTRY_RTOL, (what, "ips", err)
-    assert serr.max() < FULL_SUMS_RTOL, (what, "ips", serr)
+    sums = z[f"{prefix}ips{source}_sums"]
+    scale = group_scale(z[f"{prefix}ips_sums"][2], IP_GROUPS)
+    out["ips"] = (entry_errors(ip[:, ips], z[f"{prefix}ips{source}"], scale),
+                  sums_errors(field_sums(ip.T), sums, IP_GROUPS))
+    return out
+
+
+def check_full_size(m, z, prefix, what, noise=True, source=""):
+    """full_size_errors within their bounds, per component: FULL_ENTRY_RTOL
+    and FULL_SUMS_RTOL, or FULL_NOISE_FACTOR times the C oracle's own
+    distance to the reference measured the same way and stored in the
+    fixture (`*_onoise`, `*_osums`) where that is larger and `noise` is set.
+    Returns per field (largest entry error, largest sums error, largest
+    entry error over its bound)."""
+    worst = {}
+    for name, (err, serr) in full_size_errors(m, z, prefix, source).items():
+        eb, sb = np.full(err.size, FULL_ENTRY_RTOL), np.full(serr.size, FULL_SUMS_RTOL)
+        if noise and prefix + name + "_onoise" in z:
+            eb = np.maximum(eb, FULL_NOISE_FACTOR * z[prefix + name + "_onoise"])
+            sb = np.maximum(sb, FULL_NOISE_FACTOR * z[prefix + name + "_osums"])
+        worst[name] = (float(err.max()), float(serr.max()), float((err / eb).max()))
+        assert np.all(err <= eb), (what, name, err, eb)
+        assert np.all(serr <= sb), (what, name, serr, sb)
     return worst
 
 

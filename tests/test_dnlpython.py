@@ -283,6 +283,7 @@ class OracleEngine:
             self.o.run(max_incs=1)
             self.last_dt = self.o.control()["time"] - t0
             n += 1
+            self._record()
 
     def control(self):
         c = self.o.control()
@@ -298,6 +299,29 @@ class OracleEngine:
 
     def set_items(self, items):
         self.items = list(items)
+
+    def set_history(self, schedules, capacity=0):
+        """The device history records restated: after every increment, the
+        save rule of HistoryFile::save per schedule, a record when one is due."""
+        self.sched = [list(map(float, x)) for x in schedules]
+        self.recs = []
+
+    def _record(self):
+        if not getattr(self, "sched", None):
+            return
+        c = self.control()
+        mask = 0
+        for j, sch in enumerate(self.sched):
+            start, nxt, save = sch
+            if not (c["time"] > start and c["time"] < nxt):
+                sch[1] += save
+                mask |= 1 << j
+        if mask:
+            self.recs.append((c["time"], c["increment"], self.last_dt, mask, self.gather_items()))
+
+    def history_records(self):
+        out, self.recs = self.recs, []
+        return out
 
     def write_vtk(self, path, fields, prev=False, instance=0, title="DynELA FEM Code v.4.0"):
         """The engine's result file restated (oracle/vtk_ref.py)."""

@@ -20,7 +20,20 @@ of that magnitude below (helpers.entry_errors: |a - b| / (|b| + 1e-4 * the
 component's largest magnitude) < 1e-6; the reference's own FP64 rounding
 differences, between its eigen-solver and the C restatement's, reach 4e-11 of
 the largest shear stress after 10 increments of the 153,600-element bar), and
-the sums over the whole field within 1e-9.  Mixed path
+the sums over the whole field within 1e-9.  In the first increments of the
+necking pulls the deformation is ~1e-8 of the coordinates and FP64 rounding
+of coordinate differences dominates the lateral fields of any implementation:
+the C restatement itself is 2e-5 from the reference there.  And the
+reference's own rotation is inaccurate where two principal stretches nearly
+coincide (uniaxial compression in an impact zone): its eigen-solver returns
+eigenvectors that are not orthonormal and R = F U^-1 is off by up to 2e-3
+(tests/test_oracle.py::test_reference_rotation_inaccurate_at_nearly_repeated_stretches),
+which moves a few points' stresses by up to 0.2 % per increment and, through
+the dynamics, the run.  So each checkpoint of a run is held twice: to the C
+restatement's values (same algorithm, accurate rotations; stored in the
+fixture, `*_orc`) with the bounds above, and to the reference's values within
+the bounds above or 4 times the restatement's own distance to them
+(`*_onoise`, helpers.check_full_size), where that is larger.  Mixed path
 (FP32 element math and point state, FP64 coordinates, displacements, time and
 energy sums): coordinates within 1e-5 of the bar's span, stresses within
 5e-3 and plastic strain within 1e-3 of their tensor's largest component after
@@ -61,8 +74,14 @@ def rebuild(z, precision):
 
 
 def check_fp64(e, z, prefix, what):
+    # the C restatement's values (same algorithm, accurate rotations): strict bounds
+    if prefix + "ips_orc" in z:
+        worst = helpers.check_full_size(e, z, prefix, what + " vs restatement", noise=False, source="_orc")
+        print(what, "vs restatement", {k: f"{v[0]:.1e}/{v[1]:.1e}" for k, v in worst.items()})
+    # the reference: within its bounds, or 4x the restatement's distance to it
     worst = helpers.check_full_size(e, z, prefix, what)
-    print(what, {k: f"{v[0]:.1e}/{v[1]:.1e}" for k, v in worst.items()})
+    # entry error / sums error / entry error over its bound
+    print(what, "vs reference", {k: f"{v[0]:.1e}/{v[1]:.1e}/{v[2]:.2f}" for k, v in worst.items()})
 
 
 @pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
@@ -83,7 +102,9 @@ def test_full_size_fp64_runs_match_reference(path):
             ck = z[f"inc{k}_control"]
             c = e.control()
             assert c["increment"] == int(ck[2]) == done
-            assert abs(c["time"] - ck[0]) <= 1e-12 * ck[0]
+            # the time step is recomputed every 10 increments from a minimum
+            # over elements that rounds differently; the time sums it
+            assert abs(c["time"] - ck[0]) <= 1e-11 * ck[0]
             assert abs(c["time_step"] - ck[1]) <= 1e-11 * ck[1]
             check_fp64(e, z, f"inc{k}_", f"{os.path.basename(path)} increment {k}")
 

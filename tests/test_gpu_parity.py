@@ -75,6 +75,8 @@ def test_fp64_runs_match_reference(path):
         e.init()
         assert helpers.rel_err(e.nodes(_abi.NODE_MASS), z["init_mass"]) < 1e-13
         assert abs(e.control()["time_step"] - z["init_control"][1]) < 1e-12 * z["init_control"][1]
+        # initial speeds, imposed-speed conditions applied as Model::initSolve does
+        assert np.array_equal(e.nodes(_abi.NODE_SPEED), z["init_speed"])
         done = 0
         for k in z["checkpoints"]:
             n = e.run(max_incs=int(k) - done)
@@ -337,3 +339,61 @@ def test_native_state_read_equals_widened(precision):
         assert np.array_equal(nat.astype(np.float64), e.ips())
         other = np.empty(nat.shape, np.float64 if precision == _abi.PREC_MIXED else np.float32)
         assert e._lib.dnl_engine_get_ips_native(e.h, other.ctypes.data, other.dtype.itemsize) == -1
+
+
+def test_history_ring_equals_stopping_at_each_increment():
+    """dnl_engine_set_history keeps the records on the device while the run
+    goes on; they equal, bit for bit, what a run stopped after every
+    increment gathers when the save rule of HistoryFile::save
+    (HistoryFile.C:292-317) is due: same increments, times, masks, time steps
+    and item values (nodes of both buffers, points, kinetic energies)."""
+    d = helpers.case_hex_speed()
+    t_end = d.t_end
+    sched = [(0.0, 0.0, t_end / 7), (0.0, 0.0, 0.0), (0.3 * t_end, 0.3 * t_end, t_end / 5)]
+    fields = (_abi.NODE_COORDS, _abi.NODE_SPEED, _abi.NODE_SPEED_PREV, _abi.NODE_U_PREV, _abi.NODE_ACCEL_PREV)
+    items = [(_abi.ITEM_NODE, f, i) for f in fields for i in (0, 17, d.n_nodes - 1)]
+    items += [(_abi.ITEM_POINT, 0, q) for q in (0, 33, d.n_ips - 1)]
+    items += [(_abi.ITEM_KINETIC, f, 0) for f in (_abi.NODE_SPEED, _abi.NODE_SPEED_PREV)]
+    with engine(d) as a:
+        a.init()
+        a.set_items(items)
+        a.set_history(sched, capacity=16)
+        a.run()
+        rec = a.history_records()
+    want = []
+    nxt = [s[1] for s in sched]
+    with engine(d) as b:
+        b.init()
+        b.set_items(items)
+        while not b.control()["done"]:
+            b.run(max_incs=1)
+            c = b.control()
+            mask = 0
+            for j, (start, _, save) in enumerate(sched):
+                if not (c["time"] > start and c["time"] < nxt[j]):
+                    nxt[j] += save
+                    mask |= 1 << j
+            if mask:
+                want.append((c["time"], c["increment"], c["last_time_step"], mask, b.gather_items()))
+    assert len(rec) == len(want) > 20
+    for (t, inc, dt, mask, vals), (wt, winc, wdt, wmask, wvals) in zip(rec, want):
+        assert (t, inc, dt, mask) == (wt, winc, wdt, wmask)
+        assert np.array_equal(vals, wvals)
+
+
+def test_engine_rotation_accurate_at_nearly_repeated_stretches():
+    """On the element where the reference's rotation is not orthogonal
+    (tests/golden/polar_defect_element.npz, see test_oracle.py), the
+    engine's FP64 element pass equals the C restatement's (accurate polar
+    decomposition), not the reference's."""
+    z = np.load(os.path.join(helpers.GOLDEN, "polar_defect_element.npz"))
+    d = _abi.ModelDesc(_abi.ELHEX8N3D, z["coords"], np.arange(8)[None], [meshes.COPPER], t_end=1e-6)
+    with oracle.OracleModel(d) as o, engine(d) as e:
+        o.init()
+        e.init()
+        for m in (o, e):
+            m.set_ips(z["ips"])
+            m.set_nodes(_abi.NODE_U, z["u"])
+            m.element_pass(float(z["dt"]))
+        assert helpers.field_errors(e.ips(), o.ips()).max() < 1e-9
+        assert helpers.rel_err(e.nodes(_abi.NODE_FORCE), o.nodes(_abi.NODE_FORCE)) < 1e-9
