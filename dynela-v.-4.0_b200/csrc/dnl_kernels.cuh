@@ -68,7 +68,8 @@ template <> struct V4<float> { using type = float4; };
 
 struct DevModel
 {
-  int nInst, nN, nE, nIP, nIPpad, nSpeed, nFunc, pad;
+  int nInst, nN, nE, nIP, nIPpad, nSpeed, nFunc;
+  int slotW; // force slots per node in the fixed-stride layout (node i's at i * slotW), 0: CSR layout
   const int *inst_elem_begin; // [nInst+1]
   const int *inst_node_begin; // [nInst+1]
   Ctl *ctl;
@@ -80,7 +81,7 @@ struct DevModel
   const MatDev *mat;
   void *ip;
   void *slot;
-  const int *csr_off;      // [nN+1] first slot of each node
+  const int *csr_off;      // [nN+1] prefix sums of the nodes' slot counts (their first slots in the CSR layout)
   const int *slot_pos;     // [nE*npe] slot of (element, local node) in node order
   const uint8_t *bc;       // per node: 2 bits per component (DNL_BC_*)
   const double4 *bcval;    // per node imposed speed (only read where the code is DNL_BC_SPEED)
@@ -111,6 +112,15 @@ struct DevModel
   int *act_tile_pre, *act_node_pre, *act_elem_pre; // [nInst + 1]
   int *due_count, *due_list, *due_elem_pre;         // the same for the running instances whose time step is due
 };
+
+// Node i's first force slot: a fixed stride of slotW slots per node when every
+// node has at most that many (the padding slots hold zeros, which leave the
+// sums unchanged), else the CSR offsets.  The slots of node i are
+// [slot_begin(i), slot_begin(i) + csr_off[i+1] - csr_off[i]).
+__device__ __forceinline__ int slot_begin(const DevModel &M, int i)
+{
+  return M.slotW ? M.slotW * i : M.csr_off[i];
+}
 
 __device__ __forceinline__ int find_segment(const int *begin, int n, int v)
 {
@@ -394,30 +404,72 @@ __device__ __forceinline__ void walsh8(unsigned amask, int g, R (&v)[NC])
   }
 }
 
+// The coordinates and increment of the element's first node, which every
+// lane of the element subtracts: by shuffles from the element's first lane.
+__device__ __forceinline__ void first_node_by_shuffle(unsigned amask, int base, const double4 &X, const double4 &U,
+                                                      double4 &X0, double4 &U0)
+{
+  X0 = make_double4(__shfl_sync(amask, X.x, base), __shfl_sync(amask, X.y, base), __shfl_sync(amask, X.z, base), 0.0);
+  U0 = make_double4(__shfl_sync(amask, U.x, base), __shfl_sync(amask, U.y, base), __shfl_sync(amask, U.z, base), 0.0);
+}
+
 // J (and G) at this lane's Gauss point from the offsets of the element's nodes
 // (this lane's node offset in o[0..2] for x and o[3..5] for the increment).
+// After the butterfly, lane w holds the Walsh sums W_w of the six components;
+// every lane needs W_1..W_7 of each: they go through the element's shared
+// memory (grp, the rows of its 8 lanes, 16-byte aligned: 48 values written,
+// then read as vectors), or, without it, by register shuffles.
 template <typename R>
 __device__ __forceinline__ void hex_jacobians(unsigned amask, int g, int base, R xi0, R xi1, R xi2, R (&o)[6],
-                                              R (&J)[3][3], R (&G)[3][3])
+                                              R (&J)[3][3], R (&G)[3][3], R *grp)
 {
   walsh8<R, 6>(amask, g, o);
 #pragma unroll
   for (int c = 0; c < 6; c++)
     o[c] *= R(0.125);
   const R x01 = xi0 * xi1, x02 = xi0 * xi2, x12 = xi1 * xi2;
+  if (grp)
+  {
+    __syncwarp(amask); // the element's lanes are done with their rows (previous tile)
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      grp[8 * c + g] = o[c];
+    __syncwarp(amask);
+  }
 #pragma unroll
   for (int c = 0; c < 6; c++)
   {
-    const R w1 = __shfl_sync(amask, o[c], base + 1), w2 = __shfl_sync(amask, o[c], base + 2);
-    const R w3 = __shfl_sync(amask, o[c], base + 3), w4 = __shfl_sync(amask, o[c], base + 4);
-    const R w5 = __shfl_sync(amask, o[c], base + 5), w6 = __shfl_sync(amask, o[c], base + 6);
-    const R w7 = __shfl_sync(amask, o[c], base + 7);
+    R w1, w2, w3, w4, w5, w6, w7;
+    if (grp)
+    {
+      using R4 = typename V4<R>::type;
+      const R4 lo = reinterpret_cast<const R4 *>(grp + 8 * c)[0], hi = reinterpret_cast<const R4 *>(grp + 8 * c)[1];
+      w1 = lo.y;
+      w2 = lo.z;
+      w3 = lo.w;
+      w4 = hi.x;
+      w5 = hi.y;
+      w6 = hi.z;
+      w7 = hi.w;
+    }
+    else
+    {
+      w1 = __shfl_sync(amask, o[c], base + 1);
+      w2 = __shfl_sync(amask, o[c], base + 2);
+      w3 = __shfl_sync(amask, o[c], base + 3);
+      w4 = __shfl_sync(amask, o[c], base + 4);
+      w5 = __shfl_sync(amask, o[c], base + 5);
+      w6 = __shfl_sync(amask, o[c], base + 6);
+      w7 = __shfl_sync(amask, o[c], base + 7);
+    }
     R(&T)[3][3] = c < 3 ? J : G;
     const int i = c < 3 ? c : c - 3;
     T[i][0] = w1 * xi1 + w7 * xi2 - w5 * x12 - w3;
     T[i][1] = w1 * xi0 + w6 * xi2 - w5 * x02 - w2;
     T[i][2] = w7 * xi0 + w6 * xi1 - w5 * x01 - w4;
   }
+  if (grp)
+    __syncwarp(amask); // the rows are the lanes' own again from here on
 }
 
 // Nodal forces f_n = sum_g sum_k dN_n/dxi_k(xi_g) P_g[k][.] of the element,
@@ -523,6 +575,11 @@ template <typename R> struct EngineIo
   __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
   __device__ __forceinline__ void slot(const R4 &v) const { reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = v; }
   __device__ __forceinline__ const float *ip32() const { return reinterpret_cast<const float *>(M.ip); }
+  __device__ __forceinline__ void first_node(unsigned amask, int base, const double4 &X, const double4 &U,
+                                             double4 &X0, double4 &U0) const
+  {
+    first_node_by_shuffle(amask, base, X, U, X0, U0);
+  }
 };
 
 // Where the element update reads the old point state from: global memory, or
@@ -545,16 +602,17 @@ template <typename R> struct SharedTile
 // point from the element's nodes (lane g holds node g), then detJ, J^-1 and the
 // displacement gradient H = F - I = G J^-1 (+ the axisymmetric hoop term
 // F33 - 1 = sum N_n du_r,n / r, ElementAxi.C:78-100).
+// grp: the element's shared-memory rows (16-byte aligned, at least 48
+// values), or nullptr: see hex_jacobians.  X0, U0: the element's first node.
 template <typename R, int NPE>
-__device__ __forceinline__ void kinematics(unsigned amask, int g, int base, const double4 &X, const double4 &U, R &detJ,
-                                           R (&inv)[3][3], R &radius, R (&H)[9], bool axi)
+__device__ __forceinline__ void kinematics(unsigned amask, int g, int base, const double4 &X, const double4 &U,
+                                           const double4 &X0, const double4 &U0, R &detJ, R (&inv)[3][3], R &radius,
+                                           R (&H)[9], bool axi, R *grp)
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
   const bool AXI = ElemShape<NPE>::AXI && axi;
-  const double x0 = __shfl_sync(amask, X.x, base), y0 = __shfl_sync(amask, X.y, base),
-               z0 = __shfl_sync(amask, X.z, base);
-  const double ux0 = __shfl_sync(amask, U.x, base), uy0 = __shfl_sync(amask, U.y, base),
-               uz0 = __shfl_sync(amask, U.z, base);
+  const double x0 = X0.x, y0 = X0.y, z0 = X0.z;
+  const double ux0 = U0.x, uy0 = U0.y, uz0 = U0.z;
   // element-local offsets keep the FP32 path free of large-coordinate cancellation
   const R rx = R(X.x - x0), ry = R(X.y - y0), rz = R(X.z - z0);
   const R urx = R(U.x - ux0), ury = R(U.y - uy0), urz = R(U.z - uz0);
@@ -570,7 +628,7 @@ __device__ __forceinline__ void kinematics(unsigned amask, int g, int base, cons
   if constexpr (NPE == 8)
   {
     R o[6] = {rx, ry, rz, urx, ury, urz};
-    hex_jacobians<R>(amask, g, base, xi0, xi1, xi2, o, J, G);
+    hex_jacobians<R>(amask, g, base, xi0, xi1, xi2, o, J, G, grp);
   }
   else
     GatherJG<R, NPE, 0>::run(amask, base, xi0, xi1, xi2, rx, ry, rz, urx, ury, urz, J, G, Nr, Vr);
@@ -648,11 +706,13 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   const MatDev &mp = io.mat(e);
   const double4 X = io.x(node);
   const double4 U = io.u(node);
+  double4 X0, U0;
+  io.first_node(amask, base, X, U, X0, U0);
 
   R detJ, inv[3][3], radius, dE[6], Rot[9];
   {
     R H[9];
-    kinematics<R, NPE>(amask, g, base, X, U, detJ, inv, radius, H, !C->plane);
+    kinematics<R, NPE>(amask, g, base, X, U, X0, U0, detJ, inv, radius, H, !C->plane, grp);
     polar_lnU<R>(H, dE, Rot);
   }
   if (detJ < R(0))
@@ -798,17 +858,19 @@ template <typename R> struct Front
 // learned guess) in between.  Same arithmetic as element_update.
 template <typename R, int NPE, class Src, class Io>
 __device__ __forceinline__ void element_front(const Io &io, Ctl *C, int e, int g, int base, unsigned amask, int node,
-                                              const Src &old, R *row, Front<R> &f)
+                                              const Src &old, R *row, R *grp, Front<R> &f)
 {
   const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
   const MatDev &mp = io.mat(e);
   const double4 X = io.x(node);
   const double4 U = io.u(node);
+  double4 X0, U0;
+  io.first_node(amask, base, X, U, X0, U0);
 
   R inv[3][3], Rot[9];
   {
     R H[9];
-    kinematics<R, NPE>(amask, g, base, X, U, f.detJ, inv, f.radius, H, !C->plane);
+    kinematics<R, NPE>(amask, g, base, X, U, X0, U0, f.detJ, inv, f.radius, H, !C->plane, grp);
     polar_lnU<R>(H, f.dE, Rot);
   }
   if (f.detJ < R(0))
@@ -967,7 +1029,7 @@ __global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
 {
   constexpr int ROW = ElemShape<NPE>::ROW;
   using R4 = typename V4<R>::type;
-  __shared__ R sh[TILE * ROW];
+  __shared__ __align__(16) R sh[TILE * ROW];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int g = lane & (NPE - 1);
@@ -982,8 +1044,11 @@ __global__ void __launch_bounds__(TILE) k_element_start(DevModel M)
   const MatDev &mp = M.mat[M.emat[e]];
   const int node = M.conn[q];
   R detJ, inv[3][3], radius, H[9];
-  kinematics<R, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H,
-                    !M.ctl[inst].plane);
+  const double4 X = M.x[node], U = make_double4(0, 0, 0, 0);
+  double4 X0, U0;
+  first_node_by_shuffle(amask, base, X, U, X0, U0);
+  kinematics<R, NPE>(amask, g, base, X, U, X0, U0, detJ, inv, radius, H, !M.ctl[inst].plane,
+                     (R *)nullptr);
   if (detJ < R(0))
     raise_status(M.ctl + inst, DNL_ERR_NEG_JACOBIAN, e);
   R WxdJ = detJ;
@@ -1157,7 +1222,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M, int nTiles)
 {
   pdl_wait();
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
-  __shared__ R sh[TILE * ROW];
+  __shared__ __align__(16) R sh[TILE * ROW];
   const int lane = threadIdx.x & 31;
   const int g = lane & (NPE - 1);
   const int base = lane & ~(NPE - 1);
@@ -1323,10 +1388,10 @@ struct StagedVec
 {
   const double2 *xy;
   const double *z;
-  __device__ __forceinline__ double4 get() const
+  __device__ __forceinline__ double4 get(int back = 0) const
   {
-    const double2 a = *xy;
-    return make_double4(a.x, a.y, *z, 0.0);
+    const double2 a = xy[-back];
+    return make_double4(a.x, a.y, z[-back], 0.0);
   }
 };
 
@@ -1338,6 +1403,7 @@ template <typename R> struct StagedIo
   StagedVec nx, nu; // this lane's node
   int spos;
   const MatDev *mp;
+  int g; // this lane's place in its element
   __device__ __forceinline__ double4 x(int) const { return nx.get(); }
   __device__ __forceinline__ double4 u(int) const { return nu.get(); }
   __device__ __forceinline__ const MatDev &mat(int) const { return *mp; }
@@ -1345,6 +1411,13 @@ template <typename R> struct StagedIo
   __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
   __device__ __forceinline__ void slot(const R4 &v) const { reinterpret_cast<R4 *>(M.slot)[spos] = v; }
   __device__ __forceinline__ const float *ip32() const { return reinterpret_cast<const float *>(M.ip); }
+  // the element's first node is staged g entries before this lane's
+  __device__ __forceinline__ void first_node(unsigned, int, const double4 &, const double4 &, double4 &X0,
+                                             double4 &U0) const
+  {
+    X0 = nx.get(g);
+    U0 = nu.get(g);
+  }
 };
 
 // Element pass as a persistent kernel with three pipelines a tile apart: the
@@ -1499,7 +1572,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     {
       SharedTile<R> old{state(b), t};
       StagedIo<R> io{M, q, {nxy(b, 0) + t, nz(b, 0) + t}, {nxy(b, 1) + t, nz(b, 1) + t}, spos(b)[t],
-                     M.mat + emat(b)[t / NPE]};
+                     M.mat + emat(b)[t / NPE], g};
       element_update<R, NPE>(io, C, q, e, g, base, amask, 0, old, rows + t * ROW, rows + (t - g) * ROW);
     }
     __syncthreads(); // the buffers of this tile are refilled from the next iteration on
@@ -1527,7 +1600,7 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
 {
   using R = float;
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
-  __shared__ R sh[TILE * ROW];
+  __shared__ __align__(16) R sh[TILE * ROW];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tslot;
   extern __shared__ __align__(1024) unsigned char dyn[];
@@ -1557,7 +1630,7 @@ __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles
     bool plastic = false, scope = false;
     if (act)
     {
-      element_front<R, NPE>(io, C, e, g, base, amask, M.conn[q], old, row, f);
+      element_front<R, NPE>(io, C, e, g, base, amask, M.conn[q], old, row, grp, f);
       const MatDev &mp = io.mat(e);
       JC<R> jc;
       jc.load(mp);
@@ -1652,7 +1725,7 @@ template <typename R, int DIM>
 __device__ __forceinline__ void nodal_update(const DevModel &M, int i, int c, const Ctl *C)
 {
   constexpr int BATCH = 8; // slots loaded together
-  const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
+  constexpr int W = DIM == 3 ? 8 : 4; // the fixed-stride layout's slots per node
   const double m = M.mass[i];
   const unsigned code = (M.bc[i] >> (2 * c)) & 3u;
   const double X = reinterpret_cast<const double *>(M.x + i)[c];
@@ -1662,20 +1735,35 @@ __device__ __forceinline__ void nodal_update(const DevModel &M, int i, int c, co
   const int f0 = C->f0, f1 = 1 - f0;
   double v0 = reinterpret_cast<const double *>(M.v[f0] + i)[c];
   double a0 = reinterpret_cast<const double *>(M.a[f0] + i)[c];
-  // this component of the node's slots (4 values per slot)
+  // this component of the node's slots (4 values per slot), summed in element order
   const R *sc = reinterpret_cast<const R *>(M.slot) + c;
   double f = 0.0;
-  for (int k0 = kb; k0 < ke; k0 += BATCH)
+  if (M.slotW == W)
   {
-    R s[BATCH];
+    // fixed stride: no offsets to load first; the padding adds zeros
+    R s[W];
 #pragma unroll
-    for (int j = 0; j < BATCH; j++)
-      if (k0 + j < ke)
-        s[j] = sc[4 * (k0 + j)];
+    for (int j = 0; j < W; j++)
+      s[j] = sc[4 * (W * i + j)];
 #pragma unroll
-    for (int j = 0; j < BATCH; j++)
-      if (k0 + j < ke)
-        f += (double)s[j];
+    for (int j = 0; j < W; j++)
+      f += (double)s[j];
+  }
+  else
+  {
+    const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
+    for (int k0 = kb; k0 < ke; k0 += BATCH)
+    {
+      R s[BATCH];
+#pragma unroll
+      for (int j = 0; j < BATCH; j++)
+        if (k0 + j < ke)
+          s[j] = sc[4 * (k0 + j)];
+#pragma unroll
+      for (int j = 0; j < BATCH; j++)
+        if (k0 + j < ke)
+          f += (double)s[j];
+    }
   }
   const double dt = C->dt_eff, t = C->t;
   const double beta = C->beta, gam = C->gammaN, alphaM = C->alphaM;
@@ -1813,7 +1901,8 @@ __global__ void k_gather(DevModel M, int what)
     return;
   const R4 *slot = reinterpret_cast<const R4 *>(M.slot);
   double4 f = make_double4(0, 0, 0, 0);
-  for (int k = M.csr_off[i]; k < M.csr_off[i + 1]; k++)
+  const int kb = slot_begin(M, i), ke = kb + M.csr_off[i + 1] - M.csr_off[i];
+  for (int k = kb; k < ke; k++)
   {
     const R4 s = slot[k];
     f.x += (double)s.x;
@@ -2106,7 +2195,10 @@ __device__ __forceinline__ void element_Kv(const DevModel &M, int q, int e, int 
   const int node = M.conn[q];
   const MatDev &mp = M.mat[M.emat[e]];
   double detJ, inv[3][3], radius, H[9];
-  kinematics<double, NPE>(amask, g, base, M.x[node], make_double4(0, 0, 0, 0), detJ, inv, radius, H, AXI);
+  const double4 Xn = M.x[node], Un = make_double4(0, 0, 0, 0);
+  double4 X0, U0;
+  first_node_by_shuffle(amask, base, Xn, Un, X0, U0);
+  kinematics<double, NPE>(amask, g, base, Xn, Un, X0, U0, detJ, inv, radius, H, AXI, (double *)nullptr);
   double WxdJ = detJ;
   if (AXI)
     WxdJ *= 6.28318530717958647692 * radius;
@@ -2249,7 +2341,8 @@ __global__ void __launch_bounds__(TILE) k_power_iteration(DevModel M, int force)
     for (int i = blockIdx.x * blockDim.x + t; i < M.nN; i += gridDim.x * blockDim.x)
     {
       double acc[3] = {v[3 * i] * scale, v[3 * i + 1] * scale, v[3 * i + 2] * scale};
-      for (int k = M.csr_off[i]; k < M.csr_off[i + 1]; k++)
+      const int kb = slot_begin(M, i), ke = kb + M.csr_off[i + 1] - M.csr_off[i];
+      for (int k = kb; k < ke; k++)
       {
         const double4 y = M.pislot[k];
         acc[0] += y.x;
@@ -2326,6 +2419,9 @@ struct BuildRaw
   int *cursor;                          // [nN] CSR fill cursors
   int *list;                            // [nIP] incidences grouped by node
   int *blockSums;                       // scan partials
+  int *maxValence;                      // largest slot count of a node
+  const int *ext_of;                    // [nN] the caller's node of each engine node, or nullptr
+  const int *int_of;                    // [nN] the engine's node of each caller's node, or nullptr
   int npe;
 };
 
@@ -2341,16 +2437,17 @@ __global__ void k_build_nodes(DevModel M, BuildRaw R, int hasSpeed)
   const int inst = (M.nInst > 1) ? find_segment(M.inst_node_begin, M.nInst, i) : 0;
   const int fbase = R.base[inst].w;
   const double4 zero = make_double4(0, 0, 0, 0);
-  double4 v = make_double4(R.vinit[3 * i], R.vinit[3 * i + 1], R.vinit[3 * i + 2], 0.0);
+  const int r = R.ext_of ? R.ext_of[i] : i; // where the caller's arrays hold this node
+  double4 v = make_double4(R.vinit[3 * r], R.vinit[3 * r + 1], R.vinit[3 * r + 2], 0.0);
   double4 sv = zero;
   int4 sf = make_int4(-1, -1, -1, -1);
   unsigned code = 0;
   bool speed = false;
   for (int c = 0; c < 3; c++)
   {
-    int cc = R.bccode[3 * i + c];
-    const double val = R.bcval[3 * i + c];
-    const int fn = R.bcfun[3 * i + c];
+    int cc = R.bccode[3 * r + c];
+    const double val = R.bcval[3 * r + c];
+    const int fn = R.bcfun[3 * r + c];
     if (cc == DNL_BC_SPEED && val == 0.0)
       cc = DNL_BC_RESTRAIN;
     if (cc == DNL_BC_SPEED)
@@ -2367,7 +2464,7 @@ __global__ void k_build_nodes(DevModel M, BuildRaw R, int hasSpeed)
     v = sv;
     const_cast<int *>(M.speed_nodes)[atomicAdd(R.speedCount, 1)] = i;
   }
-  M.x[i] = make_double4(R.coords[3 * i], R.coords[3 * i + 1], R.coords[3 * i + 2], 0.0);
+  M.x[i] = make_double4(R.coords[3 * r], R.coords[3 * r + 1], R.coords[3 * r + 2], 0.0);
   M.v[0][i] = v;
   M.v[1][i] = v;
   M.disp[i] = zero;
@@ -2402,7 +2499,7 @@ __global__ void k_build_elems(DevModel M, BuildRaw R, int nIPpad)
   }
   const int inst = (M.nInst > 1) ? find_segment(M.inst_elem_begin, M.nInst, e) : 0;
   const int4 b = R.base[inst];
-  const int node = R.conn[k] + b.x;
+  const int node = R.int_of ? R.int_of[R.conn[k] + b.x] : R.conn[k] + b.x;
   conn[k] = node;
   atomicAdd(&off[node + 1], 1);
   if (k % R.npe == 0)
@@ -2497,9 +2594,21 @@ __global__ void k_slot_sort(DevModel M, BuildRaw R)
     }
     L[k + 1] = v;
   }
+  atomicMax(R.maxValence, n);
+}
+// slot_pos in the fixed-stride layout of W slots per node when no node has
+// more (the host reads the same decision back), else in the CSR layout
+__global__ void k_slot_pos(DevModel M, BuildRaw R, int W)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M.nN)
+    return;
+  const int b = M.csr_off[i], n = M.csr_off[i + 1] - b;
+  const int first = (*R.maxValence <= W) ? W * i : b;
+  const int *L = R.list + b;
   int *pos = const_cast<int *>(M.slot_pos);
   for (int j = 0; j < n; j++)
-    pos[L[j]] = b + j;
+    pos[L[j]] = first + j;
 }
 
 // ------------------------------------------------------- state read-back
@@ -2531,12 +2640,13 @@ __device__ __forceinline__ double4 node_vec(const DevModel &M, int field, int i)
 
 // Nodal vector `field` of nodes [n0, n0 + n) as [n][3] FP64 (the layout of
 // dnl_engine_get_nodes), packed on the device so that one copy brings it out.
-__global__ void k_nodes_out(DevModel M, int field, int n0, int n, double *dst)
+// perm: the engine's node of each caller's node, or nullptr (same numbering)
+__global__ void k_nodes_out(DevModel M, int field, int n0, int n, double *dst, const int *perm)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n)
     return;
-  const double4 v = node_vec(M, field, n0 + k);
+  const double4 v = node_vec(M, field, perm ? perm[n0 + k] : n0 + k);
   dst[3 * k] = v.x;
   dst[3 * k + 1] = v.y;
   dst[3 * k + 2] = v.z;
@@ -2584,14 +2694,15 @@ struct AvgComps
   int c[MAX];
 };
 template <typename R, int NPE>
-__global__ void k_node_average(DevModel M, const int *slot_inc, AvgComps comps, double *dst)
+__global__ void k_node_average(DevModel M, const int *slot_inc, AvgComps comps, double *dst, const int *perm)
 {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)comps.n * M.nN)
     return;
-  const int j = (int)(t / M.nN), i = (int)(t % M.nN);
+  const int j = (int)(t / M.nN), i = (int)(t % M.nN); // i: the caller's node
   const int comp = comps.c[j];
-  const int kb = M.csr_off[i], ke = M.csr_off[i + 1];
+  const int ni = perm ? perm[i] : i;
+  const int kb = slot_begin(M, ni), ke = kb + M.csr_off[ni + 1] - M.csr_off[ni];
   double acc = 0.0;
   for (int k = kb; k < ke; k++)
   {

@@ -38,6 +38,11 @@ struct dnl_engine
   DevModel M{};
   std::vector<void *> allocs;
   std::vector<int> elemBegin, nodeBegin;
+  // the engine's node numbering (DNL_ORDER_*): empty when every instance keeps
+  // the caller's; else intOf[caller's node] = engine's node and extOf the inverse
+  std::vector<int> intOf, extOf;
+  std::vector<int> nodeOrder; // per instance: DNL_ORDER_GIVEN or DNL_ORDER_RCM
+  const int *dIntOf = nullptr;
   std::vector<Ctl> ctlInit;
   Ctl *hctl = nullptr; // host mirror of the control blocks
   double *denergy = nullptr;
@@ -71,6 +76,7 @@ struct dnl_engine
   void *dstage = nullptr;
   size_t stageBytes = 0;
   int *dslotInc = nullptr; // incidence of each force slot (node averages)
+  size_t nSlotCap = 0;     // force slots allocated (fixed-stride or CSR layout)
   // history records kept on the device (dnl_engine_set_history)
   bool histOn = false;
   HistRing hist{};
@@ -195,7 +201,30 @@ int check_desc(const dnl_model_desc *d, int idx)
         return fail(nullptr, DNL_ERR_ARG, "model %d: function index out of range", idx);
   if (!(d->t_end > d->t_start))
     return fail(nullptr, DNL_ERR_ARG, "model %d: t_end must exceed t_start", idx);
+  if (d->node_order != DNL_ORDER_GIVEN && d->node_order != DNL_ORDER_RCM && d->node_order != DNL_ORDER_AUTO)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: unknown node order %d", idx, d->node_order);
   return DNL_OK;
+}
+
+// The engine's numbering of one model's nodes: order[k] = the caller's node
+// numbered k, or empty for the caller's numbering (DNL_ORDER_AUTO keeps it
+// unless reverse Cuthill-McKee at least halves the mean element span).
+std::vector<int> node_order_of(const dnl_model_desc *d, int npe)
+{
+  std::vector<int> order;
+  if (d->node_order == DNL_ORDER_GIVEN)
+    return order;
+  order.resize(d->n_nodes);
+  if (dnl_mesh_order_rcm(d->n_nodes, d->n_elems, npe, d->conn, order.data()) != DNL_OK)
+    return {};
+  if (d->node_order == DNL_ORDER_AUTO)
+  {
+    double given = 0.0, rcm = 0.0;
+    if (dnl_mesh_span(d->n_nodes, d->n_elems, npe, d->conn, nullptr, &given) != DNL_OK ||
+        dnl_mesh_span(d->n_nodes, d->n_elems, npe, d->conn, order.data(), &rcm) != DNL_OK || 2.0 * rcm > given)
+      return {};
+  }
+  return order;
 }
 
 
@@ -755,6 +784,29 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   h->nN = (int)nn;
   h->nE = (int)ne;
   h->nIP = h->nE * h->npe;
+  // the engine's node numbering, instance by instance (within its node range)
+  h->nodeOrder.assign(n, DNL_ORDER_GIVEN);
+  for (int i = 0; i < n; i++)
+  {
+    const std::vector<int> order = node_order_of(descs[i], h->npe);
+    if (order.empty())
+      continue;
+    if (h->intOf.empty())
+    {
+      h->intOf.resize(nn);
+      h->extOf.resize(nn);
+      for (int k = 0; k < (int)nn; k++)
+        h->intOf[k] = h->extOf[k] = k;
+    }
+    h->nodeOrder[i] = DNL_ORDER_RCM;
+    const int b = base[i].x;
+    for (int k = 0; k < descs[i]->n_nodes; k++)
+    {
+      h->extOf[b + k] = b + order[k];
+      h->intOf[b + order[k]] = b + k;
+    }
+  }
+  const bool renum = !h->intOf.empty();
   h->nTiles = (h->nIP + TILE - 1) / TILE;
   h->nIPpad = h->nTiles * TILE;
   h->hasSpeed = anySpeed;
@@ -768,6 +820,9 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   // ---- device memory of the model: one allocation, carved in 256-byte aligned parts
   const size_t rsz = h->precision == DNL_PREC_MIXED ? 4 : 8;
   const size_t nN = (size_t)h->nN, nI = (size_t)n, nIPpad = (size_t)h->nIPpad, nSp = anySpeed ? nN : 1;
+  // force slots: room for the fixed-stride layout (npe per node) or the CSR one
+  const size_t nSlotCap = std::max((size_t)h->nIP, nN * h->npe);
+  h->nSlotCap = nSlotCap;
   size_t total = 0;
   auto reserve = [&](size_t bytes) {
     const size_t o = total;
@@ -782,6 +837,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
                o_fx = reserve(sizeof(double) * fx.size()), o_fy = reserve(sizeof(double) * fy.size()),
                o_foff = reserve(sizeof(int) * foff.size()), o_nodes = reserve(sizeof(double4) * nN * 9),
                o_mass = reserve(sizeof(double) * nN), o_ctl = reserve(sizeof(Ctl) * nI),
+               o_perm = reserve(sizeof(int) * (renum ? nN : 1)),
                // zeroed at creation, from here to o_ip
                o_energy = reserve(sizeof(double) * 3 * nI), o_err = reserve(sizeof(int)),
                o_stats = reserve(sizeof(unsigned long long) * 5), o_done = reserve(sizeof(unsigned) * 2),
@@ -789,7 +845,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
                o_acttile = reserve(sizeof(int) * (nI + 1)), o_actnode = reserve(sizeof(int) * (nI + 1)),
                o_actelem = reserve(sizeof(int) * (nI + 1)), o_due = reserve(sizeof(int)),
                o_duelist = reserve(sizeof(int) * nI), o_dueelem = reserve(sizeof(int) * (nI + 1)),
-               o_ip = reserve((size_t)DNL_IP_NCOMP * nIPpad * rsz), o_slot = reserve((size_t)h->nIP * 4 * rsz);
+               o_ip = reserve((size_t)DNL_IP_NCOMP * nIPpad * rsz), o_slot = reserve(nSlotCap * 4 * rsz);
   char *A = nullptr;
   {
     cudaError_t e = cudaMalloc((void **)&A, total);
@@ -833,6 +889,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.fout = nodes + 8 * nN;
   M.mass = (double *)(A + o_mass);
   M.ctl = (Ctl *)(A + o_ctl);
+  h->dIntOf = renum ? (const int *)(A + o_perm) : nullptr;
   h->denergy = (double *)(A + o_energy);
   h->derr = (int *)(A + o_err);
   h->dstats = (unsigned long long *)(A + o_stats);
@@ -866,8 +923,9 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
                r_bcval = rreserve(sizeof(double) * 3 * nN), r_bccode = rreserve(3 * nN),
                r_bcfun = rreserve(sizeof(int) * 3 * nN), r_conn = rreserve(sizeof(int) * (size_t)h->nIP),
                r_emat = rreserve(sizeof(int) * (size_t)h->nE), r_base = rreserve(sizeof(int4) * nI),
-               r_count = rreserve(sizeof(int)), r_cursor = rreserve(sizeof(int) * nN),
-               r_list = rreserve(sizeof(int) * (size_t)h->nIP), r_sums = rreserve(sizeof(int) * (nScan + 1));
+               r_count = rreserve(2 * sizeof(int)), r_cursor = rreserve(sizeof(int) * nN),
+               r_list = rreserve(sizeof(int) * (size_t)h->nIP), r_sums = rreserve(sizeof(int) * (nScan + 1)),
+               r_ext = rreserve(sizeof(int) * (renum ? nN : 1));
   char *Rw = nullptr;
   // a single model reserves the staging at its point state's size, so that
   // reading the state back later needs no allocation
@@ -889,9 +947,12 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   R.emat = (const int *)(Rw + r_emat);
   R.base = (const int4 *)(Rw + r_base);
   R.speedCount = (int *)(Rw + r_count);
+  R.maxValence = R.speedCount + 1;
   R.cursor = (int *)(Rw + r_cursor);
   R.list = (int *)(Rw + r_list);
   R.blockSums = (int *)(Rw + r_sums);
+  R.ext_of = renum ? (const int *)(Rw + r_ext) : nullptr;
+  R.int_of = h->dIntOf;
   R.npe = h->npe;
   cudaError_t e = cudaSuccess;
   auto put = [&](size_t off, const void *src, size_t bytes) {
@@ -931,7 +992,13 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
       fill(r_emat + sizeof(int) * eb, 0, sizeof(int) * (size_t)d->n_elems);
   }
   put(r_base, base.data(), sizeof(int4) * nI);
-  fill(r_count, 0, sizeof(int));
+  fill(r_count, 0, 2 * sizeof(int));
+  if (renum)
+  {
+    put(r_ext, h->extOf.data(), sizeof(int) * nN);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(A + o_perm, h->intOf.data(), sizeof(int) * nN, cudaMemcpyHostToDevice, h->stream);
+  }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(A + o_eb, h->elemBegin.data(), sizeof(int) * (nI + 1), cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess)
@@ -950,6 +1017,8 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     e = cudaMemsetAsync(A + o_energy, 0, o_ip - o_energy, h->stream);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(A + o_off, 0, sizeof(int) * (nN + 1), h->stream);
+  if (e == cudaSuccess) // the padding slots of the fixed-stride layout stay zero
+    e = cudaMemsetAsync(A + o_slot, 0, nSlotCap * 4 * rsz, h->stream);
 
   // ---- the model built on the device
   if (e == cudaSuccess)
@@ -964,11 +1033,12 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     k_slot_cursor<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(M, R);
     k_slot_fill<<<(h->nIP + tb - 1) / tb, tb, 0, h->stream>>>(M, R);
     k_slot_sort<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(M, R);
+    k_slot_pos<<<(h->nN + tb - 1) / tb, tb, 0, h->stream>>>(M, R, h->npe);
     e = cudaGetLastError();
   }
-  int nSpeed = 0;
+  int counts[2] = {0, 0}; // nodes with an imposed speed, largest slot count of a node
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&nSpeed, R.speedCount, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    e = cudaMemcpyAsync(counts, R.speedCount, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
@@ -976,8 +1046,11 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
     dnl_engine_destroy(h);
     return fail(nullptr, DNL_ERR_CUDA, "model build failed: %s", cudaGetErrorString(e));
   }
+  const int nSpeed = counts[0];
   h->nSpeed = nSpeed;
   M.nSpeed = nSpeed;
+  // the layout k_slot_pos chose: npe slots per node when no node has more
+  M.slotW = counts[1] <= h->npe ? h->npe : 0;
   // batches start on a persistent variant: the plain one launches a block per
   // tile of the whole batch, which the tail of a batch (few instances still
   // running) cannot afford
@@ -1004,7 +1077,7 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_power_iteration<4>, TILE, 0);
     const int tiles = (h->nIP + TILE - 1) / TILE;
     h->piGrid = std::max(1, std::min(tiles, std::max(perSM, 1) * h->numSMs));
-    if ((rc = upload(h, &M.pv, pv)) || (rc = upload(h, &M.pv2, pv)) || (rc = dalloc(h, &M.pislot, h->nIP)) ||
+    if ((rc = upload(h, &M.pv, pv)) || (rc = upload(h, &M.pv2, pv)) || (rc = dalloc(h, &M.pislot, h->nSlotCap)) ||
         (rc = dalloc(h, &M.blockmax, h->piGrid)))
     {
       std::string em = h->err;
@@ -1265,6 +1338,14 @@ int dnl_engine_instance_offsets(const dnl_engine *h, int32_t i, int32_t *node0, 
   return DNL_OK;
 }
 
+int dnl_engine_node_order(const dnl_engine *h, int32_t i, int32_t *order)
+{
+  if (!h || !order || i < 0 || i >= h->nInst)
+    return DNL_ERR_ARG;
+  *order = h->nodeOrder[i];
+  return DNL_OK;
+}
+
 int dnl_engine_control(const dnl_engine *h, int32_t i, dnl_control *out)
 {
   if (!h || !out || i < 0 || i >= h->nInst)
@@ -1304,7 +1385,7 @@ int dnl_engine_get_nodes(dnl_engine *h, int32_t field, double *out)
   void *st = nullptr;
   if ((rc = staging(h, bytes, &st)))
     return rc;
-  k_nodes_out<<<(h->nN + 255) / 256, 256, 0, h->stream>>>(h->M, field, 0, h->nN, (double *)st);
+  k_nodes_out<<<(h->nN + 255) / 256, 256, 0, h->stream>>>(h->M, field, 0, h->nN, (double *)st, h->dIntOf);
   CK(cudaGetLastError());
   h->launches++;
   return copy(h, out, st, bytes, cudaMemcpyDeviceToHost);
@@ -1317,9 +1398,9 @@ int dnl_engine_set_nodes(dnl_engine *h, int32_t field, const double *in)
   int rc = sync_ctl(h);
   if (rc)
     return rc;
-  std::vector<double4> tmp(h->nN);
+  std::vector<double4> tmp(h->nN); // in the engine's numbering
   for (int i = 0; i < h->nN; i++)
-    tmp[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0);
+    tmp[h->intOf.empty() ? i : h->intOf[i]] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0);
   if (field == DNL_NODE_U || field == DNL_NODE_SPEED || field == DNL_NODE_ACCEL)
   {
     double4 **arr = field == DNL_NODE_U ? h->M.u : (field == DNL_NODE_SPEED ? h->M.v : h->M.a);
@@ -1389,7 +1470,7 @@ int node_averages_dev(dnl_engine *h, const int32_t *comps, int n, double *dst)
   int rc;
   if (!h->dslotInc)
   {
-    if ((rc = dalloc(h, &h->dslotInc, h->nIP)))
+    if ((rc = dalloc(h, &h->dslotInc, h->nSlotCap)))
       return rc;
     k_slot_incidence<<<(h->nIP + 255) / 256, 256, 0, h->stream>>>(h->M, h->dslotInc);
     h->launches++;
@@ -1405,11 +1486,11 @@ int node_averages_dev(dnl_engine *h, const int32_t *comps, int n, double *dst)
     double *o = dst + (size_t)b * h->nN;
     const bool f32 = h->precision == DNL_PREC_MIXED;
     if (h->npe == 8)
-      f32 ? k_node_average<float, 8><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o)
-          : k_node_average<double, 8><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o);
+      f32 ? k_node_average<float, 8><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o, h->dIntOf)
+          : k_node_average<double, 8><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o, h->dIntOf);
     else
-      f32 ? k_node_average<float, 4><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o)
-          : k_node_average<double, 4><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o);
+      f32 ? k_node_average<float, 4><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o, h->dIntOf)
+          : k_node_average<double, 4><<<blocks, 256, 0, h->stream>>>(h->M, h->dslotInc, ac, o, h->dIntOf);
     CK(cudaGetLastError());
     h->launches++;
   }
@@ -1520,7 +1601,8 @@ int dnl_engine_write_vtk(dnl_engine *h, int32_t inst, const char *path, const ch
   double *dvec = (double *)st, *davg = (double *)((char *)st + vecBytes);
   for (size_t v = 0; v < nodeFields.size(); v++)
   {
-    k_nodes_out<<<(nn + 255) / 256, 256, 0, h->stream>>>(h->M, nodeFields[v], n0, nn, dvec + v * 3 * (size_t)nn);
+    k_nodes_out<<<(nn + 255) / 256, 256, 0, h->stream>>>(h->M, nodeFields[v], n0, nn, dvec + v * 3 * (size_t)nn,
+                                                         h->dIntOf);
     CK(cudaGetLastError());
     h->launches++;
   }
@@ -1564,7 +1646,8 @@ int dnl_engine_write_vtk(dnl_engine *h, int32_t inst, const char *path, const ch
     o.str(" ");
     for (int j = 0; j < h->npe; j++)
     {
-      o.num((long)(conn[(size_t)e * h->npe + j] - n0));
+      const int c = conn[(size_t)e * h->npe + j];
+      o.num((long)((h->extOf.empty() ? c : h->extOf[c]) - n0));
       o.str(" ");
     }
     o.str("\n");
@@ -1758,7 +1841,8 @@ int dnl_engine_set_items(dnl_engine *h, const dnl_item *items, int32_t n, int64_
     default:
       return fail(h, DNL_ERR_ARG, "item %d: unknown kind %d", k, a.kind);
     }
-    it[k] = make_int4(a.kind, a.field, a.index, 0);
+    const int idx = (a.kind == DNL_ITEM_NODE && !h->intOf.empty()) ? h->intOf[a.index] : a.index;
+    it[k] = make_int4(a.kind, a.field, idx, 0);
     off[k] = total;
     total += width;
   }

@@ -77,6 +77,11 @@ struct StaticIo
   __device__ __forceinline__ void put(int c, double v) const { ip[(size_t)c * nIP + q] = v; }
   __device__ __forceinline__ void slot(const double4 &v) const { slots[q] = v; }
   __device__ __forceinline__ const float *ip32() const { return nullptr; }
+  __device__ __forceinline__ void first_node(unsigned amask, int base, const double4 &X, const double4 &U,
+                                             double4 &X0, double4 &U0) const
+  {
+    first_node_by_shuffle(amask, base, X, U, X0, U0);
+  }
 };
 
 struct PlainState

@@ -672,7 +672,10 @@ class DynELA:
                               bc_value=bcv, bc_func=bcf, functions=funcs, t_start=t0, t_end=t1,
                               ts_method=s.timeStepMethod, ts_freq=s.computeTimeStepFrequency,
                               ts_safety=s.timeStepSafetyFactor, rho_b=s.dissipation,
-                              precision=self.precision, stress_method=self.stress_method), node_nums, elem_nums
+                              precision=self.precision, stress_method=self.stress_method,
+                              # script meshes keep their createNode numbering unless
+                              # renumbering at least halves the element span
+                              node_order=_abi.ORDER_AUTO), node_nums, elem_nums
 
     # ---- solve (DynELA.C:727-773 -> Explicit::solve on the engine)
     def solve(self):

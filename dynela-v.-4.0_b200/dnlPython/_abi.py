@@ -21,6 +21,7 @@ NODES_PER_ELEMENT = {ELQUA4NAX: 4, ELHEX8N3D: 8, ELQUA4N2D: 4}
 DIMS = {ELQUA4NAX: 2, ELHEX8N3D: 3, ELQUA4N2D: 2}
 
 STRESS_NEWTON, STRESS_DIRECT = 0, 1
+ORDER_GIVEN, ORDER_RCM, ORDER_AUTO = 0, 1, 2
 NUM_VARIANTS = 8  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)
 TS_COURANT = 0
 TS_POWER_ITERATION = 1
@@ -116,6 +117,7 @@ class ModelDescC(ctypes.Structure):
         ("rho_b", ctypes.c_double),
         ("precision", ctypes.c_int32),
         ("stress_method", ctypes.c_int32),
+        ("node_order", ctypes.c_int32),
     ]
 
 
@@ -150,7 +152,7 @@ class ModelDesc:
     def __init__(self, elem_type, coords, conn, materials, elem_mat=None, v_init=None,
                  bc_code=None, bc_value=None, bc_func=None, functions=(), t_start=0.0, t_end=1.0,
                  ts_method=TS_COURANT, ts_freq=10, ts_safety=0.9, rho_b=0.8182, precision=PREC_FP64,
-                 stress_method=STRESS_NEWTON):
+                 stress_method=STRESS_NEWTON, node_order=None):
         self.elem_type = int(elem_type)
         npe = NODES_PER_ELEMENT[self.elem_type]
         self.coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
@@ -169,6 +171,7 @@ class ModelDesc:
         self.ts_safety, self.rho_b = float(ts_safety), float(rho_b)
         self.precision = int(precision)
         self.stress_method = int(stress_method)
+        self.node_order = ORDER_GIVEN if node_order is None else int(node_order)
         self._c = None
 
     @property
@@ -193,7 +196,8 @@ class ModelDesc:
                   bc_code=self.bc_code, bc_value=self.bc_value, bc_func=self.bc_func,
                   functions=self.functions, t_start=self.t_start, t_end=self.t_end,
                   ts_method=self.ts_method, ts_freq=self.ts_freq, ts_safety=self.ts_safety,
-                  rho_b=self.rho_b, precision=self.precision, stress_method=self.stress_method)
+                  rho_b=self.rho_b, precision=self.precision, stress_method=self.stress_method,
+                  node_order=self.node_order)
         kw.update(changes)
         return ModelDesc(**kw)
 
@@ -224,6 +228,7 @@ class ModelDesc:
         c.ts_safety, c.rho_b = self.ts_safety, self.rho_b
         c.precision = self.precision
         c.stress_method = self.stress_method
+        c.node_order = self.node_order
         self._c = c
         return c
 
@@ -299,6 +304,7 @@ def load_library():
         "dnl_engine_sizes": (ctypes.c_int, [vp] + [ctypes.POINTER(i32)] * 4),
         "dnl_engine_instance_offsets": (ctypes.c_int, [vp, i32] + [ctypes.POINTER(i32)] * 3),
         "dnl_engine_control": (ctypes.c_int, [vp, i32, ctypes.POINTER(Control)]),
+        "dnl_engine_node_order": (ctypes.c_int, [vp, i32, ctypes.POINTER(i32)]),
         "dnl_engine_get_nodes": (ctypes.c_int, [vp, i32, pd]),
         "dnl_engine_set_nodes": (ctypes.c_int, [vp, i32, pd]),
         "dnl_engine_get_ips": (ctypes.c_int, [vp, pd]),
@@ -326,6 +332,8 @@ def load_library():
         "dnl_engine_harvest_count": (ctypes.c_int, [vp, ctypes.POINTER(i64)]),
         "dnl_engine_newton_stats": (ctypes.c_int, [vp, ctypes.POINTER(i64), i32]),
         "dnl_engine_set_guess_scope": (ctypes.c_int, [vp, i32]),
+        "dnl_mesh_order_rcm": (ctypes.c_int, [i32, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+        "dnl_mesh_span": (ctypes.c_int, [i32, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), pd]),
         "dnl_mlp_forward": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, i64, vp, vp]),
         "dnl_mlp_gradients": (ctypes.c_int, [ctypes.POINTER(Mlp), vp, vp, i64, ctypes.POINTER(Mlp),
                                              ctypes.POINTER(ctypes.c_float), vp]),
@@ -347,3 +355,31 @@ def exported_symbols():
     with open(hdr) as f:
         text = f.read()
     return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*\*?(dnl_\w+)\s*\(", text, re.M)))
+
+
+def mesh_order_rcm(conn, n_nodes):
+    """Reverse Cuthill-McKee numbering of a mesh's nodes (dnl_mesh_order_rcm,
+    host code): order[k] is the node numbered k."""
+    lib = load_library()
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    order = np.empty(int(n_nodes), dtype=np.int32)
+    rc = lib.dnl_mesh_order_rcm(int(n_nodes), conn.shape[0], conn.shape[1], _ptr(conn, ctypes.c_int32),
+                                _ptr(order, ctypes.c_int32))
+    if rc != 0:
+        raise EngineError(rc, "dnl_mesh_order_rcm: invalid mesh")
+    return order
+
+
+def mesh_span(conn, n_nodes, order=None):
+    """Mean over the elements of (largest - smallest node number) under the
+    numbering `order` (dnl_mesh_span; None: the given numbering)."""
+    lib = load_library()
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    if order is not None:
+        order = np.ascontiguousarray(order, dtype=np.int32)
+    out = ctypes.c_double()
+    rc = lib.dnl_mesh_span(int(n_nodes), conn.shape[0], conn.shape[1], _ptr(conn, ctypes.c_int32),
+                           _ptr(order, ctypes.c_int32), ctypes.byref(out))
+    if rc != 0:
+        raise EngineError(rc, "dnl_mesh_span: invalid mesh or numbering")
+    return out.value

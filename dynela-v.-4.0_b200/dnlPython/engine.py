@@ -70,6 +70,14 @@ class Engine:
                                                           ctypes.byref(e0), ctypes.byref(q0)))
         return n0.value, e0.value, q0.value
 
+    def node_order(self, instance=0):
+        """The engine's numbering of an instance's nodes: _abi.ORDER_GIVEN or
+        _abi.ORDER_RCM (every node array of this handle stays in the
+        description's numbering either way)."""
+        o = ctypes.c_int32()
+        self._check(self._lib.dnl_engine_node_order(self.h, int(instance), ctypes.byref(o)))
+        return o.value
+
     @staticmethod
     def _out(out, shape):
         """A caller's output array (C-contiguous float64 of `shape`, for

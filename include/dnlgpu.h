@@ -130,7 +130,26 @@ typedef struct dnl_model_desc {
   double rho_b;                /* Explicit::setDissipation (default 0.8182) */
   int32_t precision;           /* DNL_PREC_* */
   int32_t stress_method;       /* DNL_STRESS_*: DynELA::setStressComputation (DynELA.C:1407-1431) */
+  int32_t node_order;          /* DNL_ORDER_*: how the engine numbers its copy of the nodes */
 } dnl_model_desc;
+
+/* Node numbering inside the engine.  The element pass gathers each element's
+ * nodes, so nodes that share elements should be close in memory.  GIVEN keeps
+ * the caller's numbering; RCM renumbers by reverse Cuthill-McKee
+ * (dnl_mesh_order_rcm); AUTO takes RCM when it at least halves the mean
+ * element span (dnl_mesh_span) of the given numbering.  Whatever the choice,
+ * every node index and node array of this interface stays in the caller's
+ * numbering; the results are the same bits up to the order of the sums over
+ * nodes (energies, the power-iteration time step's norms). */
+enum { DNL_ORDER_GIVEN = 0, DNL_ORDER_RCM = 1, DNL_ORDER_AUTO = 2 };
+
+/* Reverse Cuthill-McKee ordering of a mesh's nodes (host code, no device
+ * needed): order[k] is the node numbered k.  conn: [n_elems*npe], npe 4 or 8. */
+int dnl_mesh_order_rcm(int32_t n_nodes, int32_t n_elems, int32_t npe, const int32_t *conn, int32_t *order);
+/* Mean over the elements of (largest - smallest node number) under the
+ * numbering order[k] = node numbered k (NULL: the given numbering). */
+int dnl_mesh_span(int32_t n_nodes, int32_t n_elems, int32_t npe, const int32_t *conn, const int32_t *order,
+                  double *mean_span);
 
 /* Radial return of Model::computeStress (Model.C:840-851): the
  * Newton-Raphson iteration of Element::computeStress (Element.C:407-622) or
@@ -200,6 +219,9 @@ int dnl_engine_sizes(const dnl_engine *h, int32_t *n_instances, int32_t *n_nodes
 /* First node / element / integration point of instance i in the concatenated arrays. */
 int dnl_engine_instance_offsets(const dnl_engine *h, int32_t i, int32_t *node0,
                                 int32_t *elem0, int32_t *ip0);
+/* The numbering the engine chose for instance i's nodes: DNL_ORDER_GIVEN or
+ * DNL_ORDER_RCM. */
+int dnl_engine_node_order(const dnl_engine *h, int32_t instance, int32_t *order);
 
 int dnl_engine_control(const dnl_engine *h, int32_t instance, dnl_control *out);
 

@@ -211,19 +211,22 @@ def full_size_errors(m, z, prefix, source=""):
     return out
 
 
-def check_full_size(m, z, prefix, what, noise=True, source=""):
+def check_full_size(m, z, prefix, what, noise="o", source=""):
     """full_size_errors within their bounds, per component: FULL_ENTRY_RTOL
-    and FULL_SUMS_RTOL, or FULL_NOISE_FACTOR times the C oracle's own
-    distance to the reference measured the same way and stored in the
-    fixture (`*_onoise`, `*_osums`) where that is larger and `noise` is set.
+    and FULL_SUMS_RTOL, or FULL_NOISE_FACTOR times a distance measured the
+    same way and stored in the fixture, where that is larger: noise "o", the
+    C oracle's own distance to the reference (`*_onoise`, `*_osums`); "p",
+    the C oracle's distance to itself run from coordinates moved by one unit
+    in the last place (`*_pnoise`, `*_psums`: how far rounding alone carries
+    two FP64 runs of the same algorithm apart); None, the fixed bounds only.
     Returns per field (largest entry error, largest sums error, largest
     entry error over its bound)."""
     worst = {}
     for name, (err, serr) in full_size_errors(m, z, prefix, source).items():
         eb, sb = np.full(err.size, FULL_ENTRY_RTOL), np.full(serr.size, FULL_SUMS_RTOL)
-        if noise and prefix + name + "_onoise" in z:
-            eb = np.maximum(eb, FULL_NOISE_FACTOR * z[prefix + name + "_onoise"])
-            sb = np.maximum(sb, FULL_NOISE_FACTOR * z[prefix + name + "_osums"])
+        if noise and f"{prefix}{name}_{noise}noise" in z:
+            eb = np.maximum(eb, FULL_NOISE_FACTOR * z[f"{prefix}{name}_{noise}noise"])
+            sb = np.maximum(sb, FULL_NOISE_FACTOR * z[f"{prefix}{name}_{noise}sums"])
         worst[name] = (float(err.max()), float(serr.max()), float((err / eb).max()))
         assert np.all(err <= eb), (what, name, err, eb)
         assert np.all(serr <= sb), (what, name, serr, sb)

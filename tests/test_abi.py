@@ -55,6 +55,8 @@ def test_invalid_descriptions_are_rejected():
     assert rc == -6
     rc, h, msg = _create(d.copy(stress_method=5))
     assert rc == -6 and "stress computation" in msg
+    rc, h, msg = _create(d.copy(node_order=9))
+    assert rc == -1 and "node order" in msg
 
 
 def test_no_device_means_no_engine():

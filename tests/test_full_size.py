@@ -31,9 +31,17 @@ eigenvectors that are not orthonormal and R = F U^-1 is off by up to 2e-3
 which moves a few points' stresses by up to 0.2 % per increment and, through
 the dynamics, the run.  So each checkpoint of a run is held twice: to the C
 restatement's values (same algorithm, accurate rotations; stored in the
-fixture, `*_orc`) with the bounds above, and to the reference's values within
-the bounds above or 4 times the restatement's own distance to them
-(`*_onoise`, helpers.check_full_size), where that is larger.  Mixed path
+fixture, `*_orc`) within the bounds above or 4 times the distance that
+rounding alone makes between two runs of the restatement (the same run from
+coordinates one unit in the last place apart, `*_pnoise`), and to the
+reference's values within the bounds above or 4 times the restatement's own
+distance to them (`*_onoise`, helpers.check_full_size), where that is
+larger.  The engine sums in other orders than the restatement (butterflies
+over an element's lanes, fixed-order tree sums), so its rounding differs by
+about that much: after 10 increments of the 153,600-element bar the engine
+is 2e-10 from the restatement on the displacements where the perturbed
+restatement is 9e-11 from it, and in the first increments of the necking
+pulls both reach 1e-6 on the lateral displacements.  Mixed path
 (FP32 element math and point state, FP64 coordinates, displacements, time and
 energy sums): coordinates within 1e-5 of the bar's span, stresses within
 5e-3 and plastic strain within 1e-3 of their tensor's largest component after
@@ -74,11 +82,12 @@ def rebuild(z, precision):
 
 
 def check_fp64(e, z, prefix, what):
-    # the C restatement's values (same algorithm, accurate rotations): strict bounds
-    if prefix + "ips_orc" in z:
-        worst = helpers.check_full_size(e, z, prefix, what + " vs restatement", noise=False, source="_orc")
-        print(what, "vs restatement", {k: f"{v[0]:.1e}/{v[1]:.1e}" for k, v in worst.items()})
-    # the reference: within its bounds, or 4x the restatement's distance to it
+    # the C restatement's values (same algorithm, accurate rotations): the
+    # fixed bounds, or 4x the distance rounding alone makes between two runs
+    # of the restatement (from coordinates one unit in the last place apart)
+    worst = helpers.check_full_size(e, z, prefix, what + " vs restatement", noise="p", source="_orc")
+    print(what, "vs restatement", {k: f"{v[0]:.1e}/{v[1]:.1e}/{v[2]:.2f}" for k, v in worst.items()})
+    # the reference: within the fixed bounds, or 4x the restatement's distance to it
     worst = helpers.check_full_size(e, z, prefix, what)
     # entry error / sums error / entry error over its bound
     print(what, "vs reference", {k: f"{v[0]:.1e}/{v[1]:.1e}/{v[2]:.2f}" for k, v in worst.items()})
@@ -99,13 +108,20 @@ def test_full_size_fp64_runs_match_reference(path):
         for k in z["checkpoints"]:
             n = e.run(max_incs=int(k) - done)
             done += n
-            ck = z[f"inc{k}_control"]
+            ck, co, cp = z[f"inc{k}_control"], z[f"inc{k}_control_orc"], z[f"inc{k}_control_pnoise"]
             c = e.control()
-            assert c["increment"] == int(ck[2]) == done
-            # the time step is recomputed every 10 increments from a minimum
-            # over elements that rounds differently; the time sums it
-            assert abs(c["time"] - ck[0]) <= 1e-11 * ck[0]
-            assert abs(c["time_step"] - ck[1]) <= 1e-11 * ck[1]
+            assert c["increment"] == int(ck[2]) == int(co[2]) == done
+            # the time step is recomputed every 10 increments as a minimum over
+            # the elements of the current configuration, and the time sums it:
+            # against the restatement within 1e-12 or 4x the time's rounding
+            # sensitivity; against the reference within 1e-11 or 4x the
+            # restatement's own distance to it (the reference's rotation moves
+            # its configuration, see the module's docstring)
+            assert abs(c["time"] - co[0]) <= max(1e-12, 4 * cp[0]) * co[0]
+            assert abs(c["time_step"] - co[1]) <= max(1e-12, 4 * cp[1]) * co[1]
+            for j in (0, 1):
+                bound = max(1e-11, 4 * abs(co[j] - ck[j]) / ck[j]) * ck[j]
+                assert abs([c["time"], c["time_step"]][j] - ck[j]) <= bound, (j, c, ck, co)
             check_fp64(e, z, f"inc{k}_", f"{os.path.basename(path)} increment {k}")
 
 

@@ -257,7 +257,12 @@ def test_oracle_matches_full_size_bar():
         for k in z["checkpoints"][:2]:
             done += o.run(max_incs=int(k) - done)
             assert o.control()["increment"] == int(z[f"inc{k}_control"][2])
-            helpers.check_full_size(o, z, f"inc{k}_", f"oracle increment {k}", noise=False)
+            helpers.check_full_size(o, z, f"inc{k}_", f"oracle increment {k}", noise=None)
+            # and to its own stored values, which the engine's test uses (deterministic: same bits)
+            worst = helpers.check_full_size(o, z, f"inc{k}_", f"oracle increment {k}", noise=None, source="_orc")
+            assert max(v[0] for v in worst.values()) == 0.0, worst
+            c = o.control()
+            assert c["time"] == z[f"inc{k}_control_orc"][0] and c["time_step"] == z[f"inc{k}_control_orc"][1]
     z = np.load(os.path.join(helpers.GOLDEN, "fullsize_taylor3d_153600_elempass.npz"))
     seed = int(z["seed"])
     with oracle.OracleModel(desc) as o:
