@@ -52,6 +52,8 @@ def parse():
                    help="also run the learned Newton initial guess block (harvest, training, comparison; ~1 min)")
     p.add_argument("--no-necking", action="store_true", help="skip the necking workloads block")
     p.add_argument("--no-config0", action="store_true", help="skip the axisymmetric Taylor bar block")
+    p.add_argument("--necking-whole", action="store_true",
+                   help="also run the 1,198,080-element round bar to its 7 mm elongation, mixed and FP64 (~7 min)")
     p.add_argument("--batch-fp64-sample", type=int, default=256,
                    help="instances of the batch timed one by one on the FP64 path (default: all 256)")
     p.add_argument("--axial", type=int, default=160,
@@ -60,6 +62,15 @@ def parse():
 
 
 AXIAL = 160
+
+
+def variant_names(precision):
+    """Names of the element-pass variants the autotuner chooses from
+    (dnl_variant_name): staging scheme / blocks of 128 threads per SM that
+    the register budget allows."""
+    from dnlPython import _abi
+    lib = _abi.load_library()
+    return [lib.dnl_variant_name(int(precision), v).decode() for v in range(8)]
 
 
 def workload(precision):
@@ -355,6 +366,46 @@ def necking_run(incs=300):
     return out
 
 
+def necking_whole_run():
+    """The round bar of 1,198,080 ElHex8N3D pulled to its 7 mm elongation (end
+    speed ramped to 5 m/s over the first 10 % of the run) on the mixed and the
+    FP64 path: increments, device time, and the results the mixed path is held
+    to against the FP64 one (the FP64 GPU path stands in for the FP64 oracle,
+    which is held to the reference on the first increments of this mesh): the
+    elongation, the radius of the neck (the smallest distance to the axis in
+    the symmetry plane y = 0) and the largest equivalent plastic strain."""
+    import numpy as np
+    from dnlPython import _abi, meshes
+    from dnlPython.engine import Engine
+    out = {}
+    for prec, pname in ((_abi.PREC_MIXED, "mixed"), (_abi.PREC_FP64, "fp64")):
+        d = meshes.bar_necking(precision=prec)
+        plane = np.abs(d.coords[:, 1]) < 1e-12
+        with Engine(d) as e:
+            e.init()
+            v, _ = e.autotune(steps=4)
+            e.set_timing(False)
+            t0 = time.perf_counter()
+            n = e.run()
+            wall = time.perf_counter() - t0
+            c = e.control()
+            x = e.nodes(_abi.NODE_COORDS)
+            disp = e.nodes(_abi.NODE_DISP)
+            ep = e.ips()[_abi.IP_EPSP]
+        out[pname] = {"increments": int(n), "run_s": wall, "elem_steps_per_s": d.n_elems * n / wall,
+                      "time": c["time"], "elongation_mm": float(disp[:, 1].max()),
+                      "neck_radius_mm": float(np.hypot(x[plane, 0], x[plane, 2]).max()),
+                      "max_epsp": float(ep.max()), "fp64_resolves": c["fp64_resolves"], "variant": int(v)}
+    m, f = out["mixed"], out["fp64"]
+    out["mixed_over_fp64"] = f["run_s"] / m["run_s"]
+    out["mixed_vs_fp64"] = {k: abs(m[k] - f[k]) / abs(f[k]) for k in ("elongation_mm", "neck_radius_mm", "max_epsp")}
+    out["elements"] = 1198080
+    out["how"] = ("whole run to the end time, host wall time around dnl_engine_run (graph replays polled every 64 "
+                  "increments); neck radius: largest distance to the axis of the nodes of the plane y = 0 (the "
+                  "O-grid's outer ring) after the pull")
+    return out
+
+
 def config0_run():
     """The reference's own CPU-scale case: the axisymmetric copper Taylor bar
     (10 x 80 ElQua4NAx, 227 m/s, 80 us), run whole on the GPU with the Courant
@@ -598,7 +649,10 @@ def run_engine_arm(args, rank, world, dist):
         "step_roofline": step_roofline,
         "gpu_launches": launches,
         "fp64_resolves": ctl["fp64_resolves"],
-        "element_variant": {"chosen": int(variant), "autotune_ms": [round(float(x), 5) for x in variant_ms]},
+        "element_variant": {"chosen": int(variant), "autotune_ms": [round(float(x), 5) for x in variant_ms],
+                            "names": variant_names(desc.precision), "how": (
+                                "the autotuner times every variant (staging scheme x register budget) over "
+                                "increments run from a saved copy of the state and keeps the fastest")},
     }
     if fp64:
         out["fp64_path"] = fp64
@@ -622,6 +676,8 @@ def run_engine_arm(args, rank, world, dist):
         out["necking"] = necking_run()
     if world == 1 and not args.no_config0:
         out["taylor_axi_800"] = config0_run()
+    if world == 1 and args.necking_whole:
+        out["necking_whole_run"] = necking_whole_run()
     if world == 1 and AXIAL == 160 and args.guess:
         out["learned_guess"] = guess_run()
     print(json.dumps(out))

@@ -151,8 +151,16 @@ template <typename R> __device__ __forceinline__ void sym_eigen3(const R a6[6], 
 
 // Spectral functions of the small symmetric A = C - I (C = F^T F) by cyclic
 // Jacobi: lnU = sum log1p(mu_k)/2 n_k n_k, Wm = U^-1 - I = sum ((1+mu_k)^-1/2 - 1) n_k n_k.
-template <typename R> __device__ __noinline__ void spectral_jacobi(const R A[6], R lnU[6], R Wm[6])
+template <typename R> struct Spectral
 {
+  R lnU[6], Wm[6];
+};
+template <typename R>
+__device__ __noinline__ Spectral<R> spectral_jacobi(R a0, R a1, R a2, R a3, R a4, R a5)
+{
+  const R A[6] = {a0, a1, a2, a3, a4, a5};
+  Spectral<R> out;
+  R *lnU = out.lnU, *Wm = out.Wm;
   R mu[3], V[3][3];
   sym_eigen3<R>(A, mu, V);
   R hl[3], g[3];
@@ -178,6 +186,7 @@ template <typename R> __device__ __noinline__ void spectral_jacobi(const R A[6],
       lnU[sym_index(i, j)] = a;
       Wm[sym_index(i, j)] = b;
     }
+  return out;
 }
 
 // The same two functions as power series, without eigenvectors.  By
@@ -280,7 +289,17 @@ template <typename R> __device__ __forceinline__ void polar_lnU(const R H[9], R 
       A[sym_index(i, j)] = H[3 * i + j] + H[3 * j + i] + H[i] * H[j] + H[3 + i] * H[3 + j] + H[6 + i] * H[6 + j];
   R Wm[6]; // U^-1 - I
   if (!spectral_series<R>(A, lnU, Wm))
-    spectral_jacobi<R>(A, lnU, Wm);
+  {
+    // arguments and result by value: no array of this function's has its
+    // address taken, so A, lnU and Wm stay in registers on the series path
+    const Spectral<R> sp = spectral_jacobi<R>(A[0], A[1], A[2], A[3], A[4], A[5]);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+    {
+      lnU[c] = sp.lnU[c];
+      Wm[c] = sp.Wm[c];
+    }
+  }
   // R = (I + H)(I + Wm) = I + H + Wm + H Wm
 #pragma unroll
   for (int i = 0; i < 3; i++)

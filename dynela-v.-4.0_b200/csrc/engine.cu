@@ -2091,6 +2091,13 @@ int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[DNL_NUM_
   return DNL_OK;
 }
 
+const char *dnl_variant_name(int32_t precision, int32_t variant)
+{
+  if (variant < 0 || variant >= kNumVariants || (precision != DNL_PREC_FP64 && precision != DNL_PREC_MIXED))
+    return nullptr;
+  return precision == DNL_PREC_MIXED ? kVariantsF32[variant].name : kVariantsF64[variant].name;
+}
+
 int dnl_engine_set_variant(dnl_engine *h, int32_t variant)
 {
   if (!h || variant < 0 || variant >= kNumVariants)

@@ -324,6 +324,7 @@ def load_library():
         "dnl_engine_autotune": (ctypes.c_int, [vp, i32]),
         "dnl_engine_variant": (ctypes.c_int, [vp, ctypes.POINTER(i32), pd]),
         "dnl_engine_set_variant": (ctypes.c_int, [vp, i32]),
+        "dnl_variant_name": (ctypes.c_char_p, [i32, i32]),
         "dnl_element_pass_static": (ctypes.c_int, [i32, i32, i32, vp, vp, vp, ctypes.POINTER(Material),
                                                    dbl, vp, vp, vp]),
         "dnl_engine_set_mode": (ctypes.c_int, [vp, i32]),

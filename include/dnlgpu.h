@@ -356,6 +356,9 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps);
 int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[DNL_NUM_VARIANTS]);
 /* Force an element-pass variant (0 .. DNL_NUM_VARIANTS-1). */
 int dnl_engine_set_variant(dnl_engine *h, int32_t variant);
+/* Name of a variant of the precision's list ("stage/4": staged tiles, a
+ * register budget of 4 blocks of 128 threads per SM), or NULL. */
+const char *dnl_variant_name(int32_t precision, int32_t variant);
 
 /* Element pass that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc (a host application

@@ -62,6 +62,7 @@ struct orc_model
   int ts_method, ts_freq, stress_method;
   double safety, alphaM, beta, gamma, omegaS;
   int status, bad;
+  int polar_route;     /* 0: the reference's C = F^T F route, 1: from H = F - I (orc_set_polar_route) */
   double *pv;          /* power-iteration vector [nN*dim] (Model::_powerIterationEV) */
   double pfmax;        /* Model::_powerIterationFreqMax */
   long piters;         /* total power iterations run */
@@ -371,6 +372,61 @@ void orc_polar_lnU(const double F[9], double lnU[6], double R[9])
     lnU[c] = hl[0] * P[0][c] + hl[1] * P[1][c] + hl[2] * P[2][c];
 }
 
+/* The same decomposition from H = F - I without forming C = F^T F: the
+ * eigenpairs of A = C - I = H + H^T + H^T H, ln U = sum log1p(mu)/2 n n,
+ * U^-1 = I + sum ((1 + mu)^-1/2 - 1) n n, R = F U^-1.  Mathematically the
+ * reference's route; numerically the entries of C are 1 + O(strain) and
+ * their rounding (about 1e-16 absolute) is a relative error of
+ * 1e-16 / strain increment in ln U, which this route does not make (the
+ * engine's polar_lnU works on A too).  Test infrastructure: the yardstick of
+ * the engine where the strain increments are small (first increments of the
+ * quasi-static necking pulls, about 1e-7 per increment). */
+void orc_polar_lnU_h(const double H[9], double lnU[6], double R[9])
+{
+  double A[6];
+  A[0] = 2 * H[0] + H[0] * H[0] + H[3] * H[3] + H[6] * H[6];
+  A[1] = H[1] + H[3] + H[0] * H[1] + H[3] * H[4] + H[6] * H[7];
+  A[2] = H[2] + H[6] + H[0] * H[2] + H[3] * H[5] + H[6] * H[8];
+  A[3] = 2 * H[4] + H[1] * H[1] + H[4] * H[4] + H[7] * H[7];
+  A[4] = H[5] + H[7] + H[1] * H[2] + H[4] * H[5] + H[7] * H[8];
+  A[5] = 2 * H[8] + H[2] * H[2] + H[5] * H[5] + H[8] * H[8];
+  double mu[3], V[3][3];
+  orc_sym_eigen3(A, mu, V);
+  double P[3][6];
+  for (int k = 0; k < 3; k++)
+  {
+    P[k][0] = V[0][k] * V[0][k];
+    P[k][1] = V[0][k] * V[1][k];
+    P[k][2] = V[0][k] * V[2][k];
+    P[k][3] = V[1][k] * V[1][k];
+    P[k][4] = V[1][k] * V[2][k];
+    P[k][5] = V[2][k] * V[2][k];
+  }
+  double hl[3], g[3];
+  for (int k = 0; k < 3; k++)
+  {
+    hl[k] = log1p(mu[k]) / 2;
+    g[k] = 1.0 / sqrt(1.0 + mu[k]) - 1.0;
+  }
+  double Wm[6];
+  for (int c = 0; c < 6; c++)
+  {
+    lnU[c] = hl[0] * P[0][c] + hl[1] * P[1][c] + hl[2] * P[2][c];
+    Wm[c] = g[0] * P[0][c] + g[1] * P[1][c] + g[2] * P[2][c];
+  }
+  /* R = (I + H)(I + Wm) = I + H + Wm + H Wm */
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+    {
+      double s = H[3 * i + j] + Wm[SYM[i][j]];
+      for (int k = 0; k < 3; k++)
+        s += H[3 * i + k] * Wm[SYM[k][j]];
+      R[3 * i + j] = s + (i == j ? 1.0 : 0.0);
+    }
+}
+
+void orc_set_polar_route(orc_model *m, int route) { m->polar_route = route; }
+
 /* SymTensor2::dotRxRT (SymTensor2.C:512-523): R S R^T. */
 static void rot_sym(const double R[9], double S[6])
 {
@@ -658,21 +714,24 @@ static void strains(orc_model *m)
     {
       long q = e * npe + g;
       const double *dn = m->dNdx + q * npe * 3;
-      double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+      /* the reference sums the gradient into F = I; the H route sums it from
+         zero (H = F - I without the rounding of the identity's 1) */
+      const double one = m->polar_route ? 0.0 : 1.0;
+      double H[9] = {one, 0, 0, 0, one, 0, 0, 0, one};
       if (m->dim == 2)
       {
         double Vr = 0.0;
         for (int n = 0; n < npe; n++)
         {
           const double *un = u + 3 * cn[n];
-          F[0] += dn[3 * n] * un[0];
-          F[1] += dn[3 * n + 1] * un[0];
-          F[3] += dn[3 * n] * un[1];
-          F[4] += dn[3 * n + 1] * un[1];
+          H[0] += dn[3 * n] * un[0];
+          H[1] += dn[3 * n + 1] * un[0];
+          H[3] += dn[3 * n] * un[1];
+          H[4] += dn[3 * n + 1] * un[1];
           Vr += m->N[g][n] * un[0];
         }
         if (m->axi)
-          F[8] += Vr / m->radius[q];
+          H[8] += Vr / m->radius[q];
       }
       else
       {
@@ -681,11 +740,14 @@ static void strains(orc_model *m)
           const double *un = u + 3 * cn[n];
           for (int i = 0; i < 3; i++)
             for (int j = 0; j < 3; j++)
-              F[3 * i + j] += dn[3 * n + j] * un[i];
+              H[3 * i + j] += dn[3 * n + j] * un[i];
         }
       }
       double *de = m->dE + q * 6, *R = m->rot + q * 9;
-      orc_polar_lnU(F, de, R);
+      if (m->polar_route)
+        orc_polar_lnU_h(H, de, R);
+      else
+        orc_polar_lnU(H, de, R); /* H holds F here */
       for (int c = 0; c < 6; c++)
         IPV(m, DNL_IP_STRAIN + c, q) += de[c];
     }

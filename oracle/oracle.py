@@ -44,6 +44,8 @@ def lib():
         L.orc_energies.argtypes = [vp, pd]
         L.orc_sym_eigen3.argtypes = [pd, pd, pd]
         L.orc_polar_lnU.argtypes = [pd, pd, pd]
+        L.orc_polar_lnU_h.argtypes = [pd, pd, pd]
+        L.orc_set_polar_route.argtypes = [vp, ctypes.c_int]
         L.orc_radial_return.argtypes = [ctypes.POINTER(_abi.Material), pd, ctypes.c_double, pd]
         L.orc_jc_yield.restype = ctypes.c_double
         L.orc_jc_yield.argtypes = [ctypes.POINTER(_abi.Material)] + [ctypes.c_double] * 3
@@ -68,6 +70,12 @@ class OracleModel:
         self.h = lib().orc_create(ctypes.byref(self._c))
         if not self.h:
             raise RuntimeError("orc_create failed: " + lib().orc_last_error().decode())
+
+    def set_polar_route(self, route):
+        """0: the reference's polar decomposition of C = F^T F; 1: the same
+        from H = F - I (A = C - I), free of the cancellation in C's entries
+        (orc_polar_lnU_h)."""
+        lib().orc_set_polar_route(self.h, int(route))
 
     def init(self):
         rc = lib().orc_init(self.h)
@@ -164,6 +172,15 @@ def polar_lnU(F):
     lnU = np.zeros(6)
     R = np.zeros(9)
     lib().orc_polar_lnU(_pd(F), _pd(lnU), _pd(R))
+    return lnU, R.reshape(3, 3)
+
+
+def polar_lnU_h(H):
+    """The same decomposition of F = I + H from H (orc_polar_lnU_h)."""
+    H = np.ascontiguousarray(H, dtype=np.float64).reshape(9)
+    lnU = np.zeros(6)
+    R = np.zeros(9)
+    lib().orc_polar_lnU_h(_pd(H), _pd(lnU), _pd(R))
     return lnU, R.reshape(3, 3)
 
 

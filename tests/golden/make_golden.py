@@ -150,70 +150,72 @@ def full_run_case(mesh, checkpoints, threads=None):
 
 def oracle_values(mesh):
     """The C restatement (oracle/dnl_oracle.c, FP64) on a full-size run
-    fixture's model, stored in the fixture at every checkpoint: its values at
-    the sampled nodes and points and its whole-field sums (`*_orc`,
-    `*_orc_sums`), and its distance to the reference measured as the tests
-    measure the engine's (`*_onoise`, `*_osums`, helpers.full_size_errors).
-    The reference's rotation is inaccurate where two principal stretches
-    nearly coincide (polar_defect_case), which moves its runs away from any
-    accurate polar decomposition; the restatement's values are the strict
-    yardstick of the engine's runs, its distance the bound against the
-    reference."""
+    fixture's model, stored in the fixture at every checkpoint, in three runs:
+
+    * the reference's route (C = F^T F): its values at the sampled nodes and
+      points and whole-field sums (`*_orc`, `*_orc_sums`), time and time step
+      (`*_control_orc`), and its distance to the reference measured as the
+      tests measure the engine's (`*_onoise`, `*_osums`).  The reference's
+      rotation is inaccurate where two principal stretches nearly coincide
+      (polar_defect_case), which moves its runs away from any accurate polar
+      decomposition;
+    * the same from H = F - I (orc_polar_lnU_h, the engine's route: no
+      rounding of C's entries near 1, which is a relative error of 1e-16 over
+      the strain increment in ln U, 1e-9 in the first increments of the
+      quasi-static necking pulls): `*_orh`, `*_orh_sums`, `*_control_orh`,
+      and its distance to the reference (`*_hnoise`, `*_hsums`);
+    * the H route again from coordinates moved by one unit in the last place
+      (seeded signs), measured against `*_orh` (`*_pnoise`, `*_psums`,
+      `*_control_pnoise`): how far rounding alone carries two FP64 runs of
+      the same algorithm apart.  The engine sums in other orders than the
+      restatement, so its rounding differs by about as much.
+
+    The H-route values are the strict yardstick of the engine's runs."""
     import oracle
     path = os.path.join(HERE, f"fullsize_{mesh}_incs.npz")
-    derived = ("_onoise", "_osums", "_orc", "_orc_sums", "_pnoise", "_psums", "_control_orc", "_control_pnoise")
+    derived = ("_onoise", "_osums", "_orc", "_orc_sums", "_pnoise", "_psums", "_control_orc", "_control_pnoise",
+               "_orh", "_orh_sums", "_control_orh", "_hnoise", "_hsums")
     data = {k: v for k, v in np.load(path).items() if not k.endswith(derived)}
     desc = full_desc(mesh)
     nodes, ips = data["sample_nodes"], data["sample_ips"]
-    with oracle.OracleModel(desc) as o:
-        o.init()
-        done = 0
-        for k in data["checkpoints"]:
-            done += o.run(max_incs=int(k) - done)
-            clean = dict(data)
-            for name, (err, serr) in helpers.full_size_errors(o, clean, f"inc{k}_").items():
-                data[f"inc{k}_{name}_onoise"] = err
-                data[f"inc{k}_{name}_osums"] = serr
-            for name, f in helpers.FULL_NODE_FIELDS:
-                a = o.nodes(f)
-                data[f"inc{k}_{name}_orc"] = a[nodes]
-                data[f"inc{k}_{name}_orc_sums"] = helpers.field_sums(a)
-            ip = o.ips()
-            data[f"inc{k}_ips_orc"] = ip[:, ips]
-            data[f"inc{k}_ips_orc_sums"] = helpers.field_sums(ip.T)
-            c = o.control()
-            data[f"inc{k}_control_orc"] = np.array([c["time"], c["time_step"], c["increment"]], dtype=np.float64)
-            print(f"oracle {mesh} increment {k}: distance to the reference " +
-                  " ".join(f"{n} {data[f'inc{k}_{n}_onoise'].max():.1e}" for n in ("disp", "speed", "force", "ips")),
-                  flush=True)
-    # The restatement's own sensitivity to rounding: the same run from
-    # coordinates moved by one unit in the last place (seeded signs), measured
-    # against the restatement as the tests measure the engine.  Two FP64
-    # implementations of the same algorithm that sum in different orders
-    # differ by about as much; where a problem is ill-conditioned (the lateral
-    # fields of the first increments of a necking pull) that is well above
-    # the fixed bounds.
+    names = [m for m, _ in helpers.FULL_NODE_FIELDS] + ["ips"]
+    ref_only = dict(data)
+
+    def run(model_desc, route, tag, noise_tag, against):
+        with oracle.OracleModel(model_desc) as o:
+            o.set_polar_route(route)
+            o.init()
+            done = 0
+            for k in data["checkpoints"]:
+                done += o.run(max_incs=int(k) - done)
+                for name, (err, serr) in helpers.full_size_errors(o, against, f"inc{k}_").items():
+                    data[f"inc{k}_{name}_{noise_tag}noise"] = err
+                    data[f"inc{k}_{name}_{noise_tag}sums"] = serr
+                c = o.control()
+                ctl = np.array([c["time"], c["time_step"], c["increment"]], dtype=np.float64)
+                if tag:
+                    for name, f in helpers.FULL_NODE_FIELDS:
+                        a = o.nodes(f)
+                        data[f"inc{k}_{name}_{tag}"] = a[nodes]
+                        data[f"inc{k}_{name}_{tag}_sums"] = helpers.field_sums(a)
+                    ip = o.ips()
+                    data[f"inc{k}_ips_{tag}"] = ip[:, ips]
+                    data[f"inc{k}_ips_{tag}_sums"] = helpers.field_sums(ip.T)
+                    data[f"inc{k}_control_{tag}"] = ctl
+                else:
+                    co = data[f"inc{k}_control_orh"]
+                    data[f"inc{k}_control_pnoise"] = np.abs(ctl[:2] - co[:2]) / co[:2]
+                print(f"oracle {mesh} route {route} {tag or 'perturbed'} increment {k}: distance ({noise_tag}) " +
+                      " ".join(f"{n} {data[f'inc{k}_{n}_{noise_tag}noise'].max():.1e}" for n in names), flush=True)
+
+    run(desc, 0, "orc", "o", ref_only)
+    run(desc, 1, "orh", "h", ref_only)
+    # the perturbed H-route run against the H-route values
+    orh = {f"inc{k}_{n}": data[f"inc{k}_{n}_orh"] for k in data["checkpoints"] for n in names}
+    orh.update({f"inc{k}_{n}_sums": data[f"inc{k}_{n}_orh_sums"] for k in data["checkpoints"] for n in names})
+    orh.update(sample_nodes=nodes, sample_ips=ips)
     signs = np.random.default_rng(20261204).integers(-1, 2, size=desc.coords.shape)
-    pdesc = desc.copy(coords=desc.coords * (1.0 + 2.0 ** -52 * signs))
-    orc = {f"inc{k}_{n}": data[f"inc{k}_{n}_orc"] for k in data["checkpoints"]
-           for n in [m for m, _ in helpers.FULL_NODE_FIELDS] + ["ips"]}
-    orc.update({f"inc{k}_{n}_sums": data[f"inc{k}_{n}_orc_sums"] for k in data["checkpoints"]
-                for n in [m for m, _ in helpers.FULL_NODE_FIELDS] + ["ips"]})
-    orc.update(sample_nodes=nodes, sample_ips=ips)
-    with oracle.OracleModel(pdesc) as o:
-        o.init()
-        done = 0
-        for k in data["checkpoints"]:
-            done += o.run(max_incs=int(k) - done)
-            for name, (err, serr) in helpers.full_size_errors(o, orc, f"inc{k}_").items():
-                data[f"inc{k}_{name}_pnoise"] = err
-                data[f"inc{k}_{name}_psums"] = serr
-            c, co = o.control(), data[f"inc{k}_control_orc"]
-            data[f"inc{k}_control_pnoise"] = np.array([abs(c["time"] - co[0]) / co[0],
-                                                       abs(c["time_step"] - co[1]) / co[1]])
-            print(f"perturbed oracle {mesh} increment {k}: distance " +
-                  " ".join(f"{n} {data[f'inc{k}_{n}_pnoise'].max():.1e}" for n in ("disp", "speed", "force", "ips")) +
-                  f" time {data[f'inc{k}_control_pnoise'][0]:.1e}", flush=True)
+    run(desc.copy(coords=desc.coords * (1.0 + 2.0 ** -52 * signs)), 1, None, "p", orh)
     np.savez_compressed(path, **data)
 
 

@@ -194,7 +194,9 @@ def full_size_errors(m, z, prefix, source=""):
     entries per component (entry_errors, the floor against its group's
     largest magnitude) and the errors of its whole-field sums (sums_errors,
     by group).  source "" compares with the reference's values, "_orc" with
-    the C restatement's stored beside them."""
+    the C restatement's stored beside them (its polar decomposition on
+    C = F^T F, as the reference's), "_orh" with the restatement's whose
+    polar decomposition is formed from H = F - I (as the engine's)."""
     nodes, ips = z["sample_nodes"], z["sample_ips"]
     out = {}
     for name, f in FULL_NODE_FIELDS:
@@ -215,10 +217,12 @@ def check_full_size(m, z, prefix, what, noise="o", source=""):
     """full_size_errors within their bounds, per component: FULL_ENTRY_RTOL
     and FULL_SUMS_RTOL, or FULL_NOISE_FACTOR times a distance measured the
     same way and stored in the fixture, where that is larger: noise "o", the
-    C oracle's own distance to the reference (`*_onoise`, `*_osums`); "p",
-    the C oracle's distance to itself run from coordinates moved by one unit
-    in the last place (`*_pnoise`, `*_psums`: how far rounding alone carries
-    two FP64 runs of the same algorithm apart); None, the fixed bounds only.
+    C oracle's own distance to the reference (`*_onoise`, `*_osums`); "h",
+    the same for the C oracle with its polar decomposition formed from
+    H = F - I (`*_hnoise`, `*_hsums`); "p", that oracle's distance to itself
+    run from coordinates moved by one unit in the last place (`*_pnoise`,
+    `*_psums`: how far rounding alone carries two FP64 runs of the same
+    algorithm apart); None, the fixed bounds only.
     Returns per field (largest entry error, largest sums error, largest
     entry error over its bound)."""
     worst = {}

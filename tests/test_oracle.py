@@ -18,10 +18,16 @@ PASSES = sorted(glob.glob(os.path.join(helpers.GOLDEN, "*_pass.npz")))
 
 
 @pytest.mark.parametrize("path", RUNS, ids=[os.path.basename(p) for p in RUNS])
-def test_oracle_matches_reference_runs(path):
+@pytest.mark.parametrize("route", [0, 1], ids=["C=FtF", "from-H"])
+def test_oracle_matches_reference_runs(path, route):
+    """The restatement on the reference's run fixtures, with its polar
+    decomposition on C = F^T F as the reference forms it (route 0) and on
+    A = C - I from H = F - I as the engine forms it (route 1): both within
+    the same bounds."""
     z = np.load(path)
     desc = helpers.desc_from_npz(z)
     with oracle.OracleModel(desc) as o:
+        o.set_polar_route(route)
         o.init()
         assert helpers.rel_err(o.nodes(_abi.NODE_MASS), z["init_mass"]) < 1e-13
         assert helpers.field_errors(o.ips(), z["init_ips"]).max() < 1e-12
@@ -107,6 +113,43 @@ def test_oracle_courant_lengths_match_reference():
         lo, wo = o.element_lengths()
         assert helpers.rel_err(lo, lr) < 1e-12 and helpers.rel_err(wo, wr) < 1e-14
         assert abs(o.courant() - cr) < 1e-12 * cr
+
+
+def _lnU_extended(H):
+    """ln U of F = I + H for a small H in extended precision (numpy
+    longdouble): log(I + A)/2 with A = H + H^T + H^T H as its power series."""
+    H = np.asarray(H, dtype=np.longdouble)
+    A = H + H.T + H.T @ H
+    out, P = np.zeros((3, 3), dtype=np.longdouble), np.eye(3, dtype=np.longdouble)
+    for k in range(1, 12):
+        P = P @ A
+        out += P * ((1 if k % 2 else -1) / np.longdouble(2 * k))
+    return out
+
+
+def test_polar_routes_small_increments():
+    """For strain increments of 1e-7 (the first increments of the
+    quasi-static necking pulls) the reference's route, C = F^T F, loses about
+    1e-16 / 1e-7 of ln U to the rounding of C's entries near 1; the route from
+    H = F - I (the engine's) keeps it.  For 1e-3 increments (impacts) both
+    are accurate."""
+    rng = np.random.default_rng(17)
+    for scale, f_route_tol in ((1e-7, 1e-7), (1e-3, 1e-11)):
+        worst_f, worst_h = 0.0, 0.0
+        for _ in range(50):
+            H = scale * rng.normal(size=(3, 3))
+            ref = _lnU_extended(H)
+            ref6 = np.array([ref[0, 0], ref[0, 1], ref[0, 2], ref[1, 1], ref[1, 2], ref[2, 2]], dtype=np.float64)
+            lf, _ = oracle.polar_lnU(np.eye(3) + H)
+            lh, Rh = oracle.polar_lnU_h(H)
+            n = np.abs(ref6).max()
+            worst_f = max(worst_f, np.abs(lf - ref6).max() / n)
+            worst_h = max(worst_h, np.abs(lh - ref6).max() / n)
+            assert np.abs(Rh @ Rh.T - np.eye(3)).max() < 1e-14
+        assert worst_h < 1e-13, worst_h
+        assert worst_f < f_route_tol, worst_f
+        if scale == 1e-7:
+            assert worst_f > 1e3 * worst_h  # the cancellation the H route avoids
 
 
 def test_polar_decomposition_properties():
