@@ -213,7 +213,7 @@ template <typename R> __host__ __device__ constexpr SeriesCoef<R> series_coef()
   }
   return c;
 }
-// read with the loop counter, the same on every active lane (one broadcast load)
+// indexed by the unrolled loop counter: compile-time offsets into the constant bank
 static __constant__ SeriesCoef<float> c_series_f = series_coef<float>();
 static __constant__ SeriesCoef<double> c_series_d = series_coef<double>();
 
@@ -238,7 +238,11 @@ template <typename R> __device__ __forceinline__ bool spectral_series(const R A[
   R l0 = R(0), l1 = R(0), l2 = R(0);      // log(I + A)
   R w0 = R(0), w1 = R(0), w2 = R(0);      // (I + A)^-1/2 - I
   R rk = r;
-  for (int k = 1; k < 64; k++)
+  // r < rmax bounds the terms the series needs (r^k < tol by k = 17 in FP32,
+  // 28 in FP64): unrolled, the coefficients are constant-bank operands
+  constexpr int KMAX = sizeof(R) == 4 ? 20 : 32;
+#pragma unroll
+  for (int k = 1; k < KMAX; k++)
   {
     const R cl = co.log1p[k], cw = co.invsqrt[k];
     l0 += cl * al;
