@@ -419,10 +419,66 @@ __device__ __forceinline__ void first_node_by_shuffle(unsigned amask, int base, 
 // every lane needs W_1..W_7 of each: they go through the element's shared
 // memory (grp, the rows of its 8 lanes, 16-byte aligned: 48 values written,
 // then read as vectors), or, without it, by register shuffles.
+// The FP32 form of hex_jacobians with the element's shared rows: component i
+// of the coordinates and of the increment as one packed pair (o[i], o[i+3]),
+// so that the butterfly and the Jacobian rows run as paired FP32 operations
+// (fma.rn.f32x2); the rows hold the pairs of Walsh index w at grp[16 i + 2 w].
+__device__ __forceinline__ void hex_jacobians_paired(unsigned amask, int g, float xi0, float xi1, float xi2,
+                                                     const float (&o)[6], float (&J)[3][3], float (&G)[3][3],
+                                                     float *grp)
+{
+  float2 p[3] = {make_float2(o[0], o[3]), make_float2(o[1], o[4]), make_float2(o[2], o[5])};
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+  {
+    const float sg = ((g >> k) & 1) ? -1.f : 1.f; // bit 0: v + p, bit 1: p - v
+    const float2 SG = make_float2(sg, sg);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+    {
+      const float2 q = make_float2(__shfl_xor_sync(amask, p[i].x, 1 << k), __shfl_xor_sync(amask, p[i].y, 1 << k));
+      p[i] = __ffma2_rn(SG, p[i], q);
+    }
+  }
+  __syncwarp(amask); // the element's lanes are done with their rows (previous tile)
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+    reinterpret_cast<float2 *>(grp)[8 * i + g] = __fmul2_rn(p[i], make_float2(0.125f, 0.125f));
+  __syncwarp(amask);
+  const float2 XI0 = make_float2(xi0, xi0), XI1 = make_float2(xi1, xi1), XI2 = make_float2(xi2, xi2);
+  const float2 NX01 = make_float2(-xi0 * xi1, -xi0 * xi1), NX02 = make_float2(-xi0 * xi2, -xi0 * xi2),
+               NX12 = make_float2(-xi1 * xi2, -xi1 * xi2), M1 = make_float2(-1.f, -1.f);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+  {
+    const float4 *row = reinterpret_cast<const float4 *>(grp + 16 * i);
+    const float4 a = row[0], b = row[1], c = row[2], d = row[3];
+    const float2 w1 = make_float2(a.z, a.w), w2 = make_float2(b.x, b.y), w3 = make_float2(b.z, b.w);
+    const float2 w4 = make_float2(c.x, c.y), w5 = make_float2(c.z, c.w), w6 = make_float2(d.x, d.y);
+    const float2 w7 = make_float2(d.z, d.w);
+    const float2 t0 = __ffma2_rn(w1, XI1, __ffma2_rn(w7, XI2, __ffma2_rn(w5, NX12, __fmul2_rn(w3, M1))));
+    const float2 t1 = __ffma2_rn(w1, XI0, __ffma2_rn(w6, XI2, __ffma2_rn(w5, NX02, __fmul2_rn(w2, M1))));
+    const float2 t2 = __ffma2_rn(w7, XI0, __ffma2_rn(w6, XI1, __ffma2_rn(w5, NX01, __fmul2_rn(w4, M1))));
+    J[i][0] = t0.x;
+    G[i][0] = t0.y;
+    J[i][1] = t1.x;
+    G[i][1] = t1.y;
+    J[i][2] = t2.x;
+    G[i][2] = t2.y;
+  }
+  __syncwarp(amask); // the rows are the lanes' own again from here on
+}
+
 template <typename R>
 __device__ __forceinline__ void hex_jacobians(unsigned amask, int g, int base, R xi0, R xi1, R xi2, R (&o)[6],
                                               R (&J)[3][3], R (&G)[3][3], R *grp)
 {
+  if constexpr (sizeof(R) == 4)
+    if (grp)
+    {
+      hex_jacobians_paired(amask, g, xi0, xi1, xi2, o, J, G, grp);
+      return;
+    }
   walsh8<R, 6>(amask, g, o);
 #pragma unroll
   for (int c = 0; c < 6; c++)
@@ -476,9 +532,60 @@ __device__ __forceinline__ void hex_jacobians(unsigned amask, int g, int base, R
 // returned on lane n: the per-point modal terms Z_w, then a reduction over the
 // eight lanes fused with the Walsh transform (at each lane bit the pair of
 // lanes exchanges the half of the terms the partner keeps).
+// hex_forces for components 0 and 1 as one packed FP32 pair (fma.rn.f32x2),
+// the same operations as the scalar form on each.
+__device__ __forceinline__ float2 hex_forces_pair(unsigned amask, int g, float xi0, float xi1, float xi2,
+                                                  float2 p0, float2 p1, float2 p2)
+{
+  const float2 XI0 = make_float2(xi0, xi0), XI1 = make_float2(xi1, xi1), XI2 = make_float2(xi2, xi2);
+  const float x01 = xi0 * xi1, x02 = xi0 * xi2, x12 = xi1 * xi2;
+  const float s0 = (g & 1) ? -1.f : 1.f, s1 = (g & 2) ? -1.f : 1.f, s2 = (g & 4) ? -1.f : 1.f;
+  const float2 S0 = make_float2(s0, s0), S1 = make_float2(s1, s1), S2 = make_float2(s2, s2);
+  const float2 NS0 = make_float2(-s0, -s0), NS1 = make_float2(-s1, -s1), NS2 = make_float2(-s2, -s2);
+  const float2 M1 = make_float2(-1.f, -1.f);
+  auto shfl2 = [&](float2 v, int m) {
+    return make_float2(__shfl_xor_sync(amask, v.x, m), __shfl_xor_sync(amask, v.y, m));
+  };
+  const float2 z1 = __ffma2_rn(XI1, p0, __fmul2_rn(XI0, p1));
+  const float2 z2 = __fmul2_rn(p1, M1), z3 = __fmul2_rn(p0, M1), z4 = __fmul2_rn(p2, M1);
+  const float2 z5 = __fmul2_rn(M1, __ffma2_rn(make_float2(x12, x12), p0,
+                                              __ffma2_rn(make_float2(x02, x02), p1, __fmul2_rn(make_float2(x01, x01), p2))));
+  const float2 z6 = __ffma2_rn(XI2, p1, __fmul2_rn(XI1, p2)), z7 = __ffma2_rn(XI2, p0, __fmul2_rn(XI0, p2));
+  const float2 s0z1 = __fmul2_rn(S0, z1);
+  const float2 a0 = __fadd2_rn(s0z1, __fmul2_rn(M1, shfl2(s0z1, 1)));
+  const float2 a1 = __fadd2_rn(__ffma2_rn(S0, z3, z2), shfl2(__ffma2_rn(NS0, z3, z2), 1));
+  const float2 a2 = __fadd2_rn(__ffma2_rn(S0, z5, z4), shfl2(__ffma2_rn(NS0, z5, z4), 1));
+  const float2 a3 = __fadd2_rn(__ffma2_rn(S0, z7, z6), shfl2(__ffma2_rn(NS0, z7, z6), 1));
+  const float2 b0 = __fadd2_rn(__ffma2_rn(S1, a1, a0), shfl2(__ffma2_rn(NS1, a1, a0), 2));
+  const float2 b1 = __fadd2_rn(__ffma2_rn(S1, a3, a2), shfl2(__ffma2_rn(NS1, a3, a2), 2));
+  return __fmul2_rn(make_float2(0.125f, 0.125f),
+                    __fadd2_rn(__ffma2_rn(S2, b1, b0), shfl2(__ffma2_rn(NS2, b1, b0), 4)));
+}
+
 template <typename R>
 __device__ __forceinline__ void hex_forces(unsigned amask, int g, R xi0, R xi1, R xi2, const R (&P)[3][3], R (&f)[3])
 {
+  if constexpr (sizeof(R) == 4)
+  {
+    const float2 fxy = hex_forces_pair(amask, g, xi0, xi1, xi2, make_float2(P[0][0], P[0][1]),
+                                       make_float2(P[1][0], P[1][1]), make_float2(P[2][0], P[2][1]));
+    f[0] = fxy.x;
+    f[1] = fxy.y;
+    const R x01 = xi0 * xi1, x02 = xi0 * xi2, x12 = xi1 * xi2;
+    const R s0 = (g & 1) ? R(-1) : R(1), s1 = (g & 2) ? R(-1) : R(1), s2 = (g & 4) ? R(-1) : R(1);
+    const R p0 = P[0][2], p1 = P[1][2], p2 = P[2][2];
+    const R z1 = xi1 * p0 + xi0 * p1, z2 = -p1, z3 = -p0, z4 = -p2;
+    const R z5 = -(x12 * p0 + x02 * p1 + x01 * p2);
+    const R z6 = xi2 * p1 + xi1 * p2, z7 = xi2 * p0 + xi0 * p2;
+    const R a0 = s0 * z1 - __shfl_xor_sync(amask, s0 * z1, 1);
+    const R a1 = (z2 + s0 * z3) + __shfl_xor_sync(amask, z2 - s0 * z3, 1);
+    const R a2 = (z4 + s0 * z5) + __shfl_xor_sync(amask, z4 - s0 * z5, 1);
+    const R a3 = (z6 + s0 * z7) + __shfl_xor_sync(amask, z6 - s0 * z7, 1);
+    const R b0 = (a0 + s1 * a1) + __shfl_xor_sync(amask, a0 - s1 * a1, 2);
+    const R b1 = (a2 + s1 * a3) + __shfl_xor_sync(amask, a2 - s1 * a3, 2);
+    f[2] = R(0.125) * ((b0 + s2 * b1) + __shfl_xor_sync(amask, b0 - s2 * b1, 4));
+    return;
+  }
   const R x01 = xi0 * xi1, x02 = xi0 * xi2, x12 = xi1 * xi2;
   const R s0 = (g & 1) ? R(-1) : R(1), s1 = (g & 2) ? R(-1) : R(1), s2 = (g & 4) ? R(-1) : R(1);
 #pragma unroll
@@ -801,12 +908,11 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
 #pragma unroll
     for (int c = 0; c < 6; c++)
       ep[c] = old(DNL_IP_PLASTIC_STRAIN + c) + st.kplast * (st.s[c] - ((c == 0 || c == 3 || c == 5) ? pn : R(0)));
-    rotate_sym<R>(Rot, ep);
+    rotate_sym2<R>(Rot, ep, st.s);
 #pragma unroll
     for (int c = 0; c < 6; c++)
       io.put(DNL_IP_PLASTIC_STRAIN + c, ep[c]);
   }
-  rotate_sym<R>(Rot, st.s);
   R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
   if (AXI)
     rho /= radius;
@@ -978,12 +1084,11 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
 #pragma unroll
     for (int c = 0; c < 6; c++)
       ep[c] = old(DNL_IP_PLASTIC_STRAIN + c) + st.kplast * (st.s[c] - ((c == 0 || c == 3 || c == 5) ? pn : R(0)));
-    rotate_sym<R>(Rot, ep);
+    rotate_sym2<R>(Rot, ep, st.s);
 #pragma unroll
     for (int c = 0; c < 6; c++)
       io.put(DNL_IP_PLASTIC_STRAIN + c, ep[c]);
   }
-  rotate_sym<R>(Rot, st.s);
   R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / f.detJ; // Element::computeDensity (Element.C:1243-1256)
   if (AXI)
     rho /= f.radius;

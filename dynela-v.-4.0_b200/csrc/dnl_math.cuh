@@ -77,6 +77,44 @@ template <typename R> __device__ __forceinline__ void rotate_sym(const R Q[9], R
     S[k] = out[k];
 }
 
+// Q S Q^T of two symmetric tensors at once; in FP32 as packed pairs
+// (fma.rn.f32x2), the same arithmetic as rotate_sym on each.
+template <typename R> __device__ __forceinline__ void rotate_sym2(const R Q[9], R S1[6], R S2[6])
+{
+  if constexpr (sizeof(R) == 4)
+  {
+    float2 S[6], QB[9];
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      S[k] = make_float2(S1[k], S2[k]);
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+      QB[k] = make_float2(Q[k], Q[k]);
+    float2 T[9];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+        T[3 * i + j] = __ffma2_rn(QB[3 * i + 2], S[sym_index(2, j)],
+                                  __ffma2_rn(QB[3 * i + 1], S[sym_index(1, j)], __fmul2_rn(QB[3 * i], S[sym_index(0, j)])));
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = i; j < 3; j++)
+      {
+        const float2 o = __ffma2_rn(T[3 * i + 2], QB[3 * j + 2],
+                                    __ffma2_rn(T[3 * i + 1], QB[3 * j + 1], __fmul2_rn(T[3 * i], QB[3 * j])));
+        S1[sym_index(i, j)] = o.x;
+        S2[sym_index(i, j)] = o.y;
+      }
+  }
+  else
+  {
+    rotate_sym<R>(Q, S1);
+    rotate_sym<R>(Q, S2);
+  }
+}
+
 // One Jacobi rotation zeroing A(p, q) of the symmetric matrix held in A6,
 // accumulated into the eigenvector matrix V (columns).
 template <typename R, int P, int Q>

@@ -51,7 +51,8 @@ struct dnl_engine
   bool timing = false;
   double times[4] = {0, 0, 0, 0};
   long long launches = 0;
-  int launchesPerStep = 0;
+  int launchesPerStep = 0; // kernels of one graph replay
+  int graphIncs = 1;        // increments per graph replay (dnl_engine_set_graph_increments)
   bool initialized = false;
   int nTiles = 0;
   int variant = 0;          // element-pass kernel variant (see kVariants)
@@ -596,11 +597,13 @@ int enqueue_step(dnl_engine *h)
   return DNL_OK;
 }
 
-// Increments a run replays between two looks at the device: every replay can
-// add a history record, so no more than the ring holds.
+// Graph replays a run issues between two looks at the device (about dflt
+// increments): every increment can add a history record, so no more than the
+// ring holds.
 int poll_chunk(const dnl_engine *h, int dflt)
 {
-  return h->histOn ? std::min(dflt, h->hist.cap) : dflt;
+  const int incs = h->histOn ? std::min(dflt, h->hist.cap) : dflt;
+  return std::max(1, incs / h->graphIncs);
 }
 
 // Records written on the device since the last look, appended on the host.
@@ -631,7 +634,11 @@ int build_graph(dnl_engine *h)
     return DNL_OK;
   long long before = h->launches;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_step(h);
+  // graphIncs increments, each kernel after the first waiting for the previous
+  // one by programmatic serialization, also across the increments' boundaries;
+  // increments past an instance's stop find it inactive and do nothing
+  for (int k = 0; k < h->graphIncs; k++)
+    enqueue_step(h);
   cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
   if (e != cudaSuccess)
     return fail(h, DNL_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
@@ -1231,7 +1238,7 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
   else if (max_incs > 0 && !h->histOn)
   {
     // known number of increments: replay the graph without polling
-    for (int64_t s = 0; s < max_incs; s++)
+    for (int64_t s = 0; s < (max_incs + h->graphIncs - 1) / h->graphIncs; s++)
     {
       CK(cudaGraphLaunch(h->graphExec, h->stream));
       h->launches += h->launchesPerStep;
@@ -2145,6 +2152,15 @@ void drop_graph(dnl_engine *h)
   }
 }
 } // namespace
+
+int dnl_engine_set_graph_increments(dnl_engine *h, int32_t n)
+{
+  if (!h || n < 1 || n > 64)
+    return DNL_ERR_ARG;
+  h->graphIncs = n;
+  drop_graph(h);
+  return DNL_OK;
+}
 
 int dnl_engine_set_mode(dnl_engine *h, int32_t mode)
 {

@@ -321,6 +321,7 @@ def load_library():
         "dnl_engine_set_timing": (ctypes.c_int, [vp, i32]),
         "dnl_engine_timings": (ctypes.c_int, [vp, pd]),
         "dnl_engine_launch_count": (ctypes.c_int64, [vp]),
+        "dnl_engine_set_graph_increments": (ctypes.c_int, [vp, i32]),
         "dnl_engine_autotune": (ctypes.c_int, [vp, i32]),
         "dnl_engine_variant": (ctypes.c_int, [vp, ctypes.POINTER(i32), pd]),
         "dnl_engine_set_variant": (ctypes.c_int, [vp, i32]),

@@ -200,6 +200,10 @@ class Engine:
     def set_variant(self, v):
         self._check(self._lib.dnl_engine_set_variant(self.h, int(v)))
 
+    def set_graph_increments(self, n):
+        """Increments captured in one graph replay (dnl_engine_set_graph_increments)."""
+        self._check(self._lib.dnl_engine_set_graph_increments(self.h, int(n)))
+
     def launch_count(self):
         return int(self._lib.dnl_engine_launch_count(self.h))
 

@@ -337,6 +337,13 @@ int dnl_engine_energies(dnl_engine *h, int32_t instance, double out[3]);
 int dnl_engine_set_timing(dnl_engine *h, int32_t on);
 int dnl_engine_timings(const dnl_engine *h, double out[4]);
 
+/* Increments captured in one CUDA graph replay (1..64, default 1): with
+ * more, the first kernel of an increment is scheduled while the previous
+ * increment's last kernel ends (programmatic serialization inside the graph)
+ * instead of after a replay boundary.  A run stops on the same increment
+ * either way (the increments past an instance's stop do nothing). */
+int dnl_engine_set_graph_increments(dnl_engine *h, int32_t n);
+
 /* Number of kernel launches issued on the device by the last run call. */
 int64_t dnl_engine_launch_count(const dnl_engine *h);
 
