@@ -70,7 +70,7 @@ def variant_names(precision):
     the register budget allows."""
     from dnlPython import _abi
     lib = _abi.load_library()
-    return [lib.dnl_variant_name(int(precision), v).decode() for v in range(8)]
+    return [lib.dnl_variant_name(int(precision), v).decode() for v in range(_abi.NUM_VARIANTS)]
 
 
 def workload(precision):

@@ -1322,21 +1322,26 @@ template <int NPE> struct TileMap
 // same binary serves both, so that a model gives the same bits alone and in a
 // batch; the persistent variants below are the ones that suit the tail of a
 // batch, where few instances still run.
-template <typename R, int NPE, int MINB>
-__global__ void __launch_bounds__(TILE, MINB) k_element(DevModel M, int nTiles)
+// PTS points per block: TILE (a block per work slot), 2 TILE (two slots per
+// block) or TILE / 2 (two blocks per slot); MINB blocks of PTS threads per SM.
+template <typename R, int NPE, int MINB, int PTS = TILE>
+__global__ void __launch_bounds__(PTS, MINB) k_element(DevModel M, int nTiles)
 {
+  static_assert(PTS == TILE || PTS == 2 * TILE || 2 * PTS == TILE, "PTS: half, one or two tiles");
   pdl_wait();
   constexpr int ROW = ElemShape<NPE>::PASS_ROW;
-  __shared__ __align__(16) R sh[TILE * ROW];
+  __shared__ __align__(16) R sh[PTS * ROW];
   const int lane = threadIdx.x & 31;
   const int g = lane & (NPE - 1);
   const int base = lane & ~(NPE - 1);
   const TileMap<NPE> map{M, nTiles};
-  if ((int)blockIdx.x >= map.count())
+  const int slot = PTS >= TILE ? (int)(blockIdx.x * (PTS / TILE) + threadIdx.x / TILE) : (int)(blockIdx.x / 2);
+  if (slot >= map.count())
     return;
   int tile, inst;
-  map.get(blockIdx.x, tile, inst);
-  const int q = tile * TILE + threadIdx.x;
+  map.get(slot, tile, inst);
+  const int t = PTS >= TILE ? (int)(threadIdx.x % TILE) : (int)((blockIdx.x % 2) * PTS + threadIdx.x);
+  const int q = tile * TILE + t;
   const int e = q / NPE;
   Ctl *C = M.ctl + inst;
   const bool act = e >= C->elem_begin && e < C->elem_end && C->active;

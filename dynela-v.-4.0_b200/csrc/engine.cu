@@ -52,12 +52,12 @@ struct dnl_engine
   double times[4] = {0, 0, 0, 0};
   long long launches = 0;
   int launchesPerStep = 0; // kernels of one graph replay
-  int graphIncs = 1;        // increments per graph replay (dnl_engine_set_graph_increments)
+  int graphIncs = 8;        // increments per graph replay (dnl_engine_set_graph_increments)
   bool initialized = false;
   int nTiles = 0;
   int variant = 0;          // element-pass kernel variant (see kVariants)
   bool tuned = false;
-  double variantMs[8] = {0};
+  double variantMs[DNL_NUM_VARIANTS] = {0};
   int *derr = nullptr;      // bulk-copy wait failure flag
   int numSMs = 0;
   bool powerIteration = false;
@@ -237,16 +237,25 @@ std::vector<int> node_order_of(const dnl_model_desc *d, int npe)
 struct Variant
 {
   const char *name;
-  int tma;
-  int minb;
+  int tma;  // 0 plain, 1 bulk-copy state, 2 fully staged
+  int minb; // blocks per SM of the register budget
+  int pts;  // points (threads) per block
 };
 // each precision: two plain budgets, then persistent staged tiles from the most
 // blocks per SM (fewest registers, most spilled) to the fewest (no spills)
 // then the fully staged kernel (node gathers one tile ahead as well)
-const Variant kVariantsF32[] = {{"plain/6", 0, 6}, {"plain/8", 0, 8}, {"tma/4", 1, 4}, {"tma/5", 1, 5},
-                                {"tma/3", 1, 3},   {"stage/4", 2, 4}, {"stage/3", 2, 3}, {"stage/2", 2, 2}};
-const Variant kVariantsF64[] = {{"plain/4", 0, 4}, {"plain/3", 0, 3}, {"tma/2", 1, 2},  {"tma/3", 1, 3},
-                                {"plain/2", 0, 2}, {"tma/1", 1, 1},   {"stage/2", 2, 2}, {"stage/1", 2, 1}};
+// then plain blocks of half a tile (8 hexahedra) and of two tiles (32) at
+// the register budgets of the 128-point ones
+const Variant kVariantsF32[] = {{"plain/6", 0, 6, 128},     {"plain/8", 0, 8, 128},    {"tma/4", 1, 4, 128},
+                                {"tma/5", 1, 5, 128},       {"tma/3", 1, 3, 128},      {"stage/4", 2, 4, 128},
+                                {"stage/3", 2, 3, 128},     {"stage/2", 2, 2, 128},    {"plain64/12", 0, 12, 64},
+                                {"plain64/16", 0, 16, 64},  {"plain256/3", 0, 3, 256}, {"plain256/4", 0, 4, 256}};
+const Variant kVariantsF64[] = {{"plain/4", 0, 4, 128},     {"plain/3", 0, 3, 128},    {"tma/2", 1, 2, 128},
+                                {"tma/3", 1, 3, 128},       {"plain/2", 0, 2, 128},    {"tma/1", 1, 1, 128},
+                                {"stage/2", 2, 2, 128},     {"stage/1", 2, 1, 128},    {"plain64/8", 0, 8, 64},
+                                {"plain64/6", 0, 6, 64},    {"plain256/2", 0, 2, 256}, {"plain256/1", 0, 1, 256}};
+static_assert(sizeof(kVariantsF32) / sizeof(Variant) == DNL_NUM_VARIANTS, "variant list");
+static_assert(sizeof(kVariantsF64) / sizeof(Variant) == DNL_NUM_VARIANTS, "variant list");
 constexpr int kNumVariants = DNL_NUM_VARIANTS;
 
 const Variant &variant_of(const dnl_engine *h, int v)
@@ -273,11 +282,14 @@ void launch_pdl(dnl_engine *h, void (*k)(P...), int grid, int block, size_t smem
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
-template <typename R, int NPE, int MINB> int launch_plain(dnl_engine *h)
+template <typename R, int NPE, int MINB, int PTS = TILE> int launch_plain(dnl_engine *h)
 {
-  // one block per work slot: a batch has up to nInst - 1 more slots than tiles
-  // (a tile shared by two running instances is a slot of each)
-  launch_pdl(h, k_element<R, NPE, MINB>, h->nTiles + h->nInst - 1, TILE, 0, h->M, h->nTiles);
+  // work slots: a batch has up to nInst - 1 more slots than tiles (a tile
+  // shared by two running instances is a slot of each); PTS / TILE slots per
+  // block, or two blocks per slot
+  const int slots = h->nTiles + h->nInst - 1;
+  const int grid = PTS >= TILE ? (slots + PTS / TILE - 1) / (PTS / TILE) : 2 * slots;
+  launch_pdl(h, k_element<R, NPE, MINB, PTS>, grid, PTS, 0, h->M, h->nTiles);
   return DNL_OK;
 }
 
@@ -356,7 +368,11 @@ template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
     case 4: return launch_tma<R, NPE, 3>(h);
     case 5: return launch_stage<R, NPE, 4>(h);
     case 6: return launch_stage<R, NPE, 3>(h);
-    default: return launch_stage<R, NPE, 2>(h);
+    case 7: return launch_stage<R, NPE, 2>(h);
+    case 8: return launch_plain<R, NPE, 12, TILE / 2>(h);
+    case 9: return launch_plain<R, NPE, 16, TILE / 2>(h);
+    case 10: return launch_plain<R, NPE, 3, 2 * TILE>(h);
+    default: return launch_plain<R, NPE, 4, 2 * TILE>(h);
     }
   }
   switch (v)
@@ -368,7 +384,11 @@ template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
   case 4: return launch_plain<R, NPE, 2>(h);
   case 5: return launch_tma<R, NPE, 1>(h);
   case 6: return launch_stage<R, NPE, 2>(h);
-  default: return launch_stage<R, NPE, 1>(h);
+  case 7: return launch_stage<R, NPE, 1>(h);
+  case 8: return launch_plain<R, NPE, 8, TILE / 2>(h);
+  case 9: return launch_plain<R, NPE, 6, TILE / 2>(h);
+  case 10: return launch_plain<R, NPE, 2, 2 * TILE>(h);
+  default: return launch_plain<R, NPE, 1, 2 * TILE>(h);
   }
 }
 

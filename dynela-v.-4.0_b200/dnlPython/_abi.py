@@ -22,7 +22,7 @@ DIMS = {ELQUA4NAX: 2, ELHEX8N3D: 3, ELQUA4N2D: 2}
 
 STRESS_NEWTON, STRESS_DIRECT = 0, 1
 ORDER_GIVEN, ORDER_RCM, ORDER_AUTO = 0, 1, 2
-NUM_VARIANTS = 8  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)
+NUM_VARIANTS = 12  # element-pass variants of the autotuner (DNL_NUM_VARIANTS)
 TS_COURANT = 0
 TS_POWER_ITERATION = 1
 PREC_FP64 = 0

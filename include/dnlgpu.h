@@ -337,18 +337,21 @@ int dnl_engine_energies(dnl_engine *h, int32_t instance, double out[3]);
 int dnl_engine_set_timing(dnl_engine *h, int32_t on);
 int dnl_engine_timings(const dnl_engine *h, double out[4]);
 
-/* Increments captured in one CUDA graph replay (1..64, default 1): with
+/* Increments captured in one CUDA graph replay (1..64, default 8): with
  * more, the first kernel of an increment is scheduled while the previous
  * increment's last kernel ends (programmatic serialization inside the graph)
- * instead of after a replay boundary.  A run stops on the same increment
- * either way (the increments past an instance's stop do nothing). */
+ * instead of after a replay boundary (1.2 % per increment on the
+ * 153,600-element bar from 1 to 8).  A run stops on the same increment
+ * either way: the increments past an instance's stop do nothing. */
 int dnl_engine_set_graph_increments(dnl_engine *h, int32_t n);
 
 /* Number of kernel launches issued on the device by the last run call. */
 int64_t dnl_engine_launch_count(const dnl_engine *h);
 
-/* Element-pass autotuner (hex8 models): times each kernel variant (register
- * budget, plain or bulk-copy-staged persistent tiles) over `steps` increments
+/* Element-pass autotuner (hex8 models): times each kernel variant (staging
+ * scheme: plain, bulk-copied point state, or every input staged; register
+ * budget; points per block for the plain kernel: 64, 128 or 256, i.e. 8, 16
+ * or 32 hexahedra; names from dnl_variant_name) over `steps` increments
  * run from a saved copy of the state, keeps the fastest for the following runs
  * (on the mixed path the staged 4-blocks-per-SM variant, 5, when it is within
  * 1 % of the fastest: it holds up best later in an impact) and restores the
@@ -358,7 +361,7 @@ int64_t dnl_engine_launch_count(const dnl_engine *h);
  * increment, even when few instances still run.  No counterpart in the
  * reference (its element loop has one implementation). */
 int dnl_engine_autotune(dnl_engine *h, int32_t steps);
-#define DNL_NUM_VARIANTS 8
+#define DNL_NUM_VARIANTS 12
 /* Variant in use and the element-pass time (ms) the autotuner measured for each. */
 int dnl_engine_variant(const dnl_engine *h, int32_t *variant, double ms[DNL_NUM_VARIANTS]);
 /* Force an element-pass variant (0 .. DNL_NUM_VARIANTS-1). */
