@@ -111,7 +111,20 @@ struct DevModel
   int *act_list;           // [nInst]
   int *act_tile_pre, *act_node_pre, *act_elem_pre; // [nInst + 1]
   int *due_count, *due_list, *due_elem_pre;         // the same for the running instances whose time step is due
+  // a model with one material: its Johnson-Cook block and density, read by the
+  // element pass from the kernel parameters (JC<R, true>)
+  JCParams<float> one32;
+  JCParams<double> one64;
+  double one_rho0;
 };
+
+template <typename R> __device__ __forceinline__ const JCParams<R> *one_params(const DevModel &M)
+{
+  if constexpr (sizeof(R) == 4)
+    return &M.one32;
+  else
+    return &M.one64;
+}
 
 // Node i's first force slot: a fixed stride of slotW slots per node when every
 // node has at most that many (the padding slots hold zeros, which leave the
@@ -223,13 +236,17 @@ __host__ __device__ __forceinline__ size_t ip_index(int c, int q)
   return (size_t)(q / TILE) * (DNL_IP_NCOMP * TILE) + (size_t)ip_slot(c) * TILE + (q % TILE);
 }
 
+// The point state streams through the L2 once per increment (143 MB on the
+// mixed path, 285 MB in FP64, more than the 126 MB L2): its loads and stores
+// are marked evict-first (ld/st.global.cs), so that the force slots, node
+// vectors and connectivity that the next passes read stay in the L2.
 template <typename R> __device__ __forceinline__ R ipv(const DevModel &M, int c, int q)
 {
-  return reinterpret_cast<const R *>(M.ip)[ip_index(c, q)];
+  return __ldcs(reinterpret_cast<const R *>(M.ip) + ip_index(c, q));
 }
 template <typename R> __device__ __forceinline__ void ipw(const DevModel &M, int c, int q, R v)
 {
-  reinterpret_cast<R *>(M.ip)[ip_index(c, q)] = v;
+  __stcs(reinterpret_cast<R *>(M.ip) + ip_index(c, q), v);
 }
 
 __device__ __forceinline__ void raise_status(Ctl *c, int code, int index)
@@ -670,7 +687,8 @@ template <typename R, int NPE, int N> struct MassToShared
 
 // How the element update reaches nodes, materials and its outputs in the
 // engine's own arrays (tile-major point state, node-ordered force slots).
-template <typename R> struct EngineIo
+// ONE: the model has one material, read from the kernel parameters.
+template <typename R, bool ONE = false> struct EngineIo
 {
   using R4 = typename V4<R>::type;
   const DevModel &M;
@@ -679,6 +697,22 @@ template <typename R> struct EngineIo
   __device__ __forceinline__ double4 u(int n) const { return M.u[f0][n]; }
   __device__ __forceinline__ const MatDev &mat(int e) const { return M.mat[M.emat[e]]; }
   __device__ __forceinline__ const MatDev *matp(int e) const { return M.mat + M.emat[e]; }
+  __device__ __forceinline__ JC<R, ONE> law(int e) const
+  {
+    JC<R, ONE> j;
+    if constexpr (ONE)
+      j.q = one_params<R>(M);
+    else
+      j.load(mat(e));
+    return j;
+  }
+  __device__ __forceinline__ double rho0(int e) const
+  {
+    if constexpr (ONE)
+      return M.one_rho0;
+    else
+      return mat(e).rho0;
+  }
   __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
   __device__ __forceinline__ void slot(const R4 &v) const { reinterpret_cast<R4 *>(M.slot)[M.slot_pos[q]] = v; }
   __device__ __forceinline__ const float *ip32() const { return reinterpret_cast<const float *>(M.ip); }
@@ -810,7 +844,6 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   const bool AXI = ElemShape<NPE>::AXI && !(C->plane);
   using R4 = typename V4<R>::type;
   const double dt = C->dt_eff;
-  const MatDev &mp = io.mat(e);
   const double4 X = io.x(node);
   const double4 U = io.u(node);
   double4 X0, U0;
@@ -864,8 +897,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   st.T = old(DNL_IP_T);
   st.eint = old(DNL_IP_EINT);
   st.einel = old(DNL_IP_EINEL);
-  JC<R> jc;
-  jc.load(mp);
+  const auto jc = io.law(e);
   st.pressure = (st.s[0] + st.s[3] + st.s[5]) / R(3) + jc.K() * (trSum / R(NPE));
   {
     bool ok;
@@ -913,7 +945,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
     for (int c = 0; c < 6; c++)
       io.put(DNL_IP_PLASTIC_STRAIN + c, ep[c]);
   }
-  R rho = R(mp.rho0) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
+  R rho = R(io.rho0(e)) * old(DNL_IP_DETJ0) / detJ; // Element::computeDensity (Element.C:1243-1256)
   if (AXI)
     rho /= radius;
 #pragma unroll
@@ -1324,7 +1356,7 @@ template <int NPE> struct TileMap
 // batch, where few instances still run.
 // PTS points per block: TILE (a block per work slot), 2 TILE (two slots per
 // block) or TILE / 2 (two blocks per slot); MINB blocks of PTS threads per SM.
-template <typename R, int NPE, int MINB, int PTS = TILE>
+template <typename R, int NPE, int MINB, int PTS = TILE, bool ONE = false>
 __global__ void __launch_bounds__(PTS, MINB) k_element(DevModel M, int nTiles)
 {
   static_assert(PTS == TILE || PTS == 2 * TILE || 2 * PTS == TILE, "PTS: half, one or two tiles");
@@ -1349,7 +1381,7 @@ __global__ void __launch_bounds__(PTS, MINB) k_element(DevModel M, int nTiles)
   if (!act)
     return;
   GlobalState<R> old{M, q};
-  EngineIo<R> io{M, q, C->f0};
+  EngineIo<R, ONE> io{M, q, C->f0};
   element_update<R, NPE>(io, C, q, e, g, base, amask, M.conn[q], old, sh + threadIdx.x * ROW,
                          sh + (threadIdx.x - g) * ROW);
 }
@@ -1375,6 +1407,18 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// the same with an evict-first L2 policy: for the point state, which is read
+// once per increment (see ipv)
+__device__ __forceinline__ void bulk_g2s_ef(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
                : "memory");
 }
 
@@ -1406,7 +1450,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 // block computes one tile, the bulk-copy engine brings the next tile's point
 // state (one contiguous block in the tile-major layout) and connectivity into
 // the other shared-memory buffer.  Results go straight to global memory.
-template <typename R, int NPE, int MINB>
+template <typename R, int NPE, int MINB, bool ONE = false>
 __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTiles, int *err)
 {
   pdl_wait();
@@ -1433,7 +1477,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
   auto issue = [&](int tile, int b) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&bar[b], STATE_BYTES + CONN_BYTES);
-    bulk_g2s(state[b], reinterpret_cast<const R *>(M.ip) + (size_t)tile * DNL_IP_NCOMP * TILE, STATE_BYTES, &bar[b]);
+    bulk_g2s_ef(state[b], reinterpret_cast<const R *>(M.ip) + (size_t)tile * DNL_IP_NCOMP * TILE, STATE_BYTES, &bar[b]);
     bulk_g2s(conn[b], M.conn + (size_t)tile * TILE, CONN_BYTES, &bar[b]);
   };
   // Work slots (TileMap): the tiles of the running instances only.  The
@@ -1469,7 +1513,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTil
     if (act)
     {
       SharedTile<R> old{state[b], t};
-      EngineIo<R> io{M, q, C->f0};
+      EngineIo<R, ONE> io{M, q, C->f0};
       element_update<R, NPE>(io, C, q, e, g, base, amask, conn[b][t], old, rows + t * ROW, rows + (t - g) * ROW);
     }
     __syncthreads(); // the buffer is refilled two tiles later
@@ -1505,7 +1549,7 @@ struct StagedVec
   }
 };
 
-template <typename R> struct StagedIo
+template <typename R, bool ONE = false> struct StagedIo
 {
   using R4 = typename V4<R>::type;
   const DevModel &M;
@@ -1518,6 +1562,22 @@ template <typename R> struct StagedIo
   __device__ __forceinline__ double4 u(int) const { return nu.get(); }
   __device__ __forceinline__ const MatDev &mat(int) const { return *mp; }
   __device__ __forceinline__ const MatDev *matp(int) const { return mp; }
+  __device__ __forceinline__ JC<R, ONE> law(int) const
+  {
+    JC<R, ONE> j;
+    if constexpr (ONE)
+      j.q = one_params<R>(M);
+    else
+      j.load(*mp);
+    return j;
+  }
+  __device__ __forceinline__ double rho0(int) const
+  {
+    if constexpr (ONE)
+      return M.one_rho0;
+    else
+      return mp->rho0;
+  }
   __device__ __forceinline__ void put(int c, R v) const { ipw<R>(M, c, q, v); }
   __device__ __forceinline__ void slot(const R4 &v) const { reinterpret_cast<R4 *>(M.slot)[spos] = v; }
   __device__ __forceinline__ const float *ip32() const { return reinterpret_cast<const float *>(M.ip); }
@@ -1554,7 +1614,7 @@ template <typename R, int NPE> struct StageLayout
   static constexpr uint32_t BYTES = OFF_ROWS + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
 };
 
-template <typename R, int NPE, int MINB>
+template <typename R, int NPE, int MINB, bool ONE = false>
 __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nTiles, int *err)
 {
   pdl_wait();
@@ -1593,7 +1653,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
   auto issue_state = [&](int tl, int b) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&sbar[b], STATE_BYTES + IDX_BYTES + EMAT_BYTES);
-    bulk_g2s(state(b), reinterpret_cast<const R *>(M.ip) + (size_t)tl * DNL_IP_NCOMP * TILE, STATE_BYTES, &sbar[b]);
+    bulk_g2s_ef(state(b), reinterpret_cast<const R *>(M.ip) + (size_t)tl * DNL_IP_NCOMP * TILE, STATE_BYTES, &sbar[b]);
     bulk_g2s(spos(b), M.slot_pos + (size_t)tl * TILE, IDX_BYTES, &sbar[b]);
     bulk_g2s(emat(b), M.emat + (size_t)tl * EPT, EMAT_BYTES, &sbar[b]);
   };
@@ -1681,7 +1741,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
     if (act)
     {
       SharedTile<R> old{state(b), t};
-      StagedIo<R> io{M, q, {nxy(b, 0) + t, nz(b, 0) + t}, {nxy(b, 1) + t, nz(b, 1) + t}, spos(b)[t],
+      StagedIo<R, ONE> io{M, q, {nxy(b, 0) + t, nz(b, 0) + t}, {nxy(b, 1) + t, nz(b, 1) + t}, spos(b)[t],
                      M.mat + emat(b)[t / NPE], g};
       element_update<R, NPE>(io, C, q, e, g, base, amask, 0, old, rows + t * ROW, rows + (t - g) * ROW);
     }

@@ -405,12 +405,22 @@ inline MatDev make_mat(const dnl_material &m)
 }
 
 // The Johnson-Cook law as the return calls it.  The parameters are read from
-// the material (global memory, read-only loads) at each use instead of being
-// held in registers through the return: the element pass is limited by
-// registers, and the material is one cached line that every thread shares.
-template <typename R> struct JC
+// the material at each use instead of being held in registers through the
+// return (the element pass is limited by registers).  PARAM false: q points to
+// the material in global memory (read-only loads of one cached line that every
+// thread shares); PARAM true: q points into the kernel's parameter block (a
+// model with one material: DevModel::one32 / one64), whose values the
+// arithmetic takes as constant-bank operands, without a load.
+template <typename R, bool PARAM = false> struct JC
 {
   const JCParams<R> *q;
+  __device__ __forceinline__ R ld(const R &v) const
+  {
+    if constexpr (PARAM)
+      return v;
+    else
+      return __ldg(&v);
+  }
   __device__ __forceinline__ void load(const MatDev &p)
   {
     if constexpr (sizeof(R) == 4)
@@ -418,25 +428,25 @@ template <typename R> struct JC
     else
       q = &p.jc64;
   }
-  __device__ __forceinline__ R twoG() const { return __ldg(&q->twoG); }
-  __device__ __forceinline__ R heatFrac() const { return __ldg(&q->thermal); }
-  __device__ __forceinline__ R invRho0() const { return __ldg(&q->invRho0); }
-  __device__ __forceinline__ R K() const { return __ldg(&q->K); }
+  __device__ __forceinline__ R twoG() const { return ld(q->twoG); }
+  __device__ __forceinline__ R heatFrac() const { return ld(q->thermal); }
+  __device__ __forceinline__ R invRho0() const { return ld(q->invRho0); }
+  __device__ __forceinline__ R K() const { return ld(q->K); }
   // JohnsonCookLaw::getYieldStress (JohnsonCookLaw.C:146-170) and the analytic
   // total derivative getDerivateYieldStress (JohnsonCookLaw.C:298-339), in one pass.
   __device__ __forceinline__ void eval(R epsp, R depsp, R T, R dt, R &yield, R &hard, bool wantHard) const
   {
-    R pn = Num<R>::pow_(epsp, __ldg(&q->n)); // epsp^n
-    R hard0 = __ldg(&q->A) + __ldg(&q->B) * pn;
-    bool rate = depsp > __ldg(&q->depsp0);
-    R visc0 = rate ? R(1) + __ldg(&q->C) * Num<R>::log_(depsp / __ldg(&q->depsp0)) : R(1);
+    R pn = Num<R>::pow_(epsp, ld(q->n)); // epsp^n
+    R hard0 = ld(q->A) + ld(q->B) * pn;
+    bool rate = depsp > ld(q->depsp0);
+    R visc0 = rate ? R(1) + ld(q->C) * Num<R>::log_(depsp / ld(q->depsp0)) : R(1);
     R temp0 = R(1), temp1 = R(0);
-    bool hot = T > __ldg(&q->Tref), melt = !(T < __ldg(&q->Tm));
+    bool hot = T > ld(q->Tref), melt = !(T < ld(q->Tm));
     if (hot)
     {
       if (!melt)
       {
-        temp1 = Num<R>::pow_((T - __ldg(&q->Tref)) * __ldg(&q->invTmT), __ldg(&q->m));
+        temp1 = Num<R>::pow_((T - ld(q->Tref)) * ld(q->invTmT), ld(q->m));
         temp0 = R(1) - temp1;
       }
       else
@@ -445,11 +455,11 @@ template <typename R> struct JC
     yield = hard0 * visc0 * temp0;
     if (wantHard)
     {
-      R h = __ldg(&q->n) * __ldg(&q->B) * (epsp > R(0) ? pn / epsp : R(0)) * visc0 * temp0; // n B epsp^(n-1) ...
+      R h = ld(q->n) * ld(q->B) * (epsp > R(0) ? pn / epsp : R(0)) * visc0 * temp0; // n B epsp^(n-1) ...
       if (rate)
-        h += hard0 * __ldg(&q->C) * temp0 / (depsp * dt);
+        h += hard0 * ld(q->C) * temp0 / (depsp * dt);
       if (hot && !melt)
-        h -= __ldg(&q->m) * __ldg(&q->thermal) * hard0 * hard0 * visc0 * visc0 * temp0 * temp1 / (T - __ldg(&q->Tref));
+        h -= ld(q->m) * ld(q->thermal) * hard0 * hard0 * visc0 * visc0 * temp0 * temp1 / (T - ld(q->Tref));
       hard = h;
     }
   }
@@ -468,8 +478,8 @@ template <typename R> struct ReturnState
 // Trial equivalent stress sqrt(3/2)|dev(sigma_old) + 2G dev(dE)| and the yield
 // stress the return starts from (with the reference's lazy first evaluation at
 // gamma = 1e-8, Element.C:458-463): the inputs of the learned initial guess.
-template <typename R>
-__device__ __forceinline__ void trial_state(const JC<R> &jc, R twoG, const R dE[6], const ReturnState<R> &st, R dt,
+template <typename R, class Law>
+__device__ __forceinline__ void trial_state(const Law &jc, R twoG, const R dE[6], const ReturnState<R> &st, R dt,
                                             R &Strial, R &yield0)
 {
   R p0 = (st.s[0] + st.s[3] + st.s[5]) / R(3), pe = (dE[0] + dE[3] + dE[5]) / R(3);
@@ -503,8 +513,8 @@ __device__ __forceinline__ void trial_state(const JC<R> &jc, R twoG, const R dE[
 // gamma = (|s*| - sqrt(2/3) sigma_y) / (2G (1 + h / (3G))) with the slope h at
 // the previous plastic strain (or 1e-8) and rate and the initial temperature,
 // then the yield stress at the new state (1 evaluation).
-template <typename R>
-__device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac, R inv_rho0, const R dE[6], R dt,
+template <typename R, class Law>
+__device__ __forceinline__ int radial_return(const Law &jc, R twoG, R heatFrac, R inv_rho0, const R dE[6], R dt,
                                              ReturnState<R> &st, bool &ok, R gamma0 = R(-1), bool direct = false)
 {
   const R SQ32 = R(1.2247448713915890491), SQ23 = R(0.81649658092772603273);
@@ -579,6 +589,7 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
     R epsp = epsp0 + SQ23 * gamma;
     T = T0 + R(0.5) * gamma * heatFrac * (SQ23 * yield + Snorm0);
     R fun = R(0), dfun = twoG32, tol = R(1e-8);
+    bool bisected = false; // the last step halved the bracket instead of a Newton step
     for (;;)
     {
       R hard;
@@ -591,7 +602,8 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
       dfun = twoG32 + SQ23 * hard;
       R dgamma = fun / dfun;
       gamma += dgamma;
-      if ((gammaMax - gamma) * (gamma - gammaMin) < R(0))
+      bisected = (gammaMax - gamma) * (gamma - gammaMin) < R(0);
+      if (bisected)
       {
         dgamma = R(0.5) * (gammaMax - gammaMin);
         gamma = gammaMin + dgamma;
@@ -610,9 +622,17 @@ __device__ __forceinline__ int radial_return(const JC<R> &jc, R twoG, R heatFrac
         return iterate + 1;
       }
     }
-    // FP32 acceptance: the last residual is the one before the final Newton
-    // step, so it is bounded by dfun times the step tolerance
-    if (!fp64 && !(Num<R>::abs_(fun) <= R(1e-5) * Strial + R(2) * dfun * tol))
+    // FP32 acceptance: after a Newton step the last residual is the one before
+    // that step, so it is bounded by dfun times the step tolerance; a rounding
+    // failure shows there.  An exit by halving the bracket (Element.C:539-547:
+    // the bracket closed to the step tolerance, with a residual that can reach
+    // a few MPa) is the algorithm's own exit: from the reference's start the
+    // FP64 iteration ends those points in the same bracket, after as many
+    // steps, with the same residual, so re-solving them in FP64 changes
+    // nothing but costs time.  Where the bracket closes depends on the start,
+    // so a point started from a guess (gamma0) that ends that way is still
+    // re-solved, from the reference's start.
+    if (!fp64 && !(bisected && gamma0 < R(0)) && !(Num<R>::abs_(fun) <= R(1e-5) * Strial + R(2) * dfun * tol))
     {
       ok = false;
       return iterate + 1;

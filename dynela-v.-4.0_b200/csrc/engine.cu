@@ -48,11 +48,16 @@ struct dnl_engine
   double *denergy = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graphExec = nullptr;
+  // graphs of r < graphIncs increments (remExec[r]), for runs of a known
+  // number of increments that is not a multiple of graphIncs
+  cudaGraphExec_t remExec[64] = {};
+  int remLaunches[64] = {};
   bool timing = false;
   double times[4] = {0, 0, 0, 0};
   long long launches = 0;
   int launchesPerStep = 0; // kernels of one graph replay
   int graphIncs = 8;        // increments per graph replay (dnl_engine_set_graph_increments)
+  bool oneMat = false;      // one material in the whole engine: the element pass reads it from its parameters
   bool initialized = false;
   int nTiles = 0;
   int variant = 0;          // element-pass kernel variant (see kVariants)
@@ -282,46 +287,46 @@ void launch_pdl(dnl_engine *h, void (*k)(P...), int grid, int block, size_t smem
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
-template <typename R, int NPE, int MINB, int PTS = TILE> int launch_plain(dnl_engine *h)
+template <typename R, int NPE, bool ONE, int MINB, int PTS = TILE> int launch_plain(dnl_engine *h)
 {
   // work slots: a batch has up to nInst - 1 more slots than tiles (a tile
   // shared by two running instances is a slot of each); PTS / TILE slots per
   // block, or two blocks per slot
   const int slots = h->nTiles + h->nInst - 1;
   const int grid = PTS >= TILE ? (slots + PTS / TILE - 1) / (PTS / TILE) : 2 * slots;
-  launch_pdl(h, k_element<R, NPE, MINB, PTS>, grid, PTS, 0, h->M, h->nTiles);
+  launch_pdl(h, k_element<R, NPE, MINB, PTS, ONE>, grid, PTS, 0, h->M, h->nTiles);
   return DNL_OK;
 }
 
-template <typename R, int NPE, int MINB> int launch_tma(dnl_engine *h)
+template <typename R, int NPE, bool ONE, int MINB> int launch_tma(dnl_engine *h)
 {
   const size_t smem = 2 * (DNL_IP_NREAD * TILE * sizeof(R) + TILE * sizeof(int)) + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
   static int perSM = -1; // per instantiation
   if (perSM < 0)
   {
-    CK(cudaFuncSetAttribute(k_element_tma<R, NPE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_tma<R, NPE, MINB>, TILE, smem));
+    CK(cudaFuncSetAttribute(k_element_tma<R, NPE, MINB, ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_tma<R, NPE, MINB, ONE>, TILE, smem));
     if (perSM < 1)
       perSM = 1;
   }
   const int grid = std::min(h->nTiles, perSM * h->numSMs);
-  launch_pdl(h, k_element_tma<R, NPE, MINB>, grid, TILE, smem, h->M, h->nTiles, h->derr);
+  launch_pdl(h, k_element_tma<R, NPE, MINB, ONE>, grid, TILE, smem, h->M, h->nTiles, h->derr);
   return DNL_OK;
 }
 
-template <typename R, int NPE, int MINB> int launch_stage(dnl_engine *h)
+template <typename R, int NPE, bool ONE, int MINB> int launch_stage(dnl_engine *h)
 {
   const size_t smem = StageLayout<R, NPE>::BYTES;
   static int perSM = -1; // per instantiation
   if (perSM < 0)
   {
-    CK(cudaFuncSetAttribute(k_element_stage<R, NPE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_stage<R, NPE, MINB>, TILE, smem));
+    CK(cudaFuncSetAttribute(k_element_stage<R, NPE, MINB, ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_element_stage<R, NPE, MINB, ONE>, TILE, smem));
     if (perSM < 1)
       perSM = 1;
   }
   const int grid = std::min(h->nTiles, perSM * h->numSMs);
-  launch_pdl(h, k_element_stage<R, NPE, MINB>, grid, TILE, smem, h->M, h->nTiles, h->derr);
+  launch_pdl(h, k_element_stage<R, NPE, MINB, ONE>, grid, TILE, smem, h->M, h->nTiles, h->derr);
   return DNL_OK;
 }
 
@@ -355,40 +360,40 @@ template <int NPE> int launch_mode_any(dnl_engine *h)
   }
 }
 
-template <typename R, int NPE> int launch_variant(dnl_engine *h, int v)
+template <typename R, int NPE, bool ONE> int launch_variant(dnl_engine *h, int v)
 {
   if (sizeof(R) == 4)
   {
     switch (v)
     {
-    case 0: return launch_plain<R, NPE, 6>(h);
-    case 1: return launch_plain<R, NPE, 8>(h);
-    case 2: return launch_tma<R, NPE, 4>(h);
-    case 3: return launch_tma<R, NPE, 5>(h);
-    case 4: return launch_tma<R, NPE, 3>(h);
-    case 5: return launch_stage<R, NPE, 4>(h);
-    case 6: return launch_stage<R, NPE, 3>(h);
-    case 7: return launch_stage<R, NPE, 2>(h);
-    case 8: return launch_plain<R, NPE, 12, TILE / 2>(h);
-    case 9: return launch_plain<R, NPE, 16, TILE / 2>(h);
-    case 10: return launch_plain<R, NPE, 3, 2 * TILE>(h);
-    default: return launch_plain<R, NPE, 4, 2 * TILE>(h);
+    case 0: return launch_plain<R, NPE, ONE, 6>(h);
+    case 1: return launch_plain<R, NPE, ONE, 8>(h);
+    case 2: return launch_tma<R, NPE, ONE, 4>(h);
+    case 3: return launch_tma<R, NPE, ONE, 5>(h);
+    case 4: return launch_tma<R, NPE, ONE, 3>(h);
+    case 5: return launch_stage<R, NPE, ONE, 4>(h);
+    case 6: return launch_stage<R, NPE, ONE, 3>(h);
+    case 7: return launch_stage<R, NPE, ONE, 2>(h);
+    case 8: return launch_plain<R, NPE, ONE, 12, TILE / 2>(h);
+    case 9: return launch_plain<R, NPE, ONE, 16, TILE / 2>(h);
+    case 10: return launch_plain<R, NPE, ONE, 3, 2 * TILE>(h);
+    default: return launch_plain<R, NPE, ONE, 4, 2 * TILE>(h);
     }
   }
   switch (v)
   {
-  case 0: return launch_plain<R, NPE, 4>(h);
-  case 1: return launch_plain<R, NPE, 3>(h);
-  case 2: return launch_tma<R, NPE, 2>(h);
-  case 3: return launch_tma<R, NPE, 3>(h);
-  case 4: return launch_plain<R, NPE, 2>(h);
-  case 5: return launch_tma<R, NPE, 1>(h);
-  case 6: return launch_stage<R, NPE, 2>(h);
-  case 7: return launch_stage<R, NPE, 1>(h);
-  case 8: return launch_plain<R, NPE, 8, TILE / 2>(h);
-  case 9: return launch_plain<R, NPE, 6, TILE / 2>(h);
-  case 10: return launch_plain<R, NPE, 2, 2 * TILE>(h);
-  default: return launch_plain<R, NPE, 1, 2 * TILE>(h);
+  case 0: return launch_plain<R, NPE, ONE, 4>(h);
+  case 1: return launch_plain<R, NPE, ONE, 3>(h);
+  case 2: return launch_tma<R, NPE, ONE, 2>(h);
+  case 3: return launch_tma<R, NPE, ONE, 3>(h);
+  case 4: return launch_plain<R, NPE, ONE, 2>(h);
+  case 5: return launch_tma<R, NPE, ONE, 1>(h);
+  case 6: return launch_stage<R, NPE, ONE, 2>(h);
+  case 7: return launch_stage<R, NPE, ONE, 1>(h);
+  case 8: return launch_plain<R, NPE, ONE, 8, TILE / 2>(h);
+  case 9: return launch_plain<R, NPE, ONE, 6, TILE / 2>(h);
+  case 10: return launch_plain<R, NPE, ONE, 2, 2 * TILE>(h);
+  default: return launch_plain<R, NPE, ONE, 1, 2 * TILE>(h);
   }
 }
 
@@ -427,13 +432,16 @@ int launch_element_any(dnl_engine *h, int mode)
     {
       // the axisymmetric models are small: one plain variant
       if (h->precision == DNL_PREC_MIXED)
-        rc = launch_plain<float, 4, 6>(h);
+        rc = h->oneMat ? launch_plain<float, 4, true, 6>(h) : launch_plain<float, 4, false, 6>(h);
       else
-        rc = launch_plain<double, 4, 4>(h);
+        rc = h->oneMat ? launch_plain<double, 4, true, 4>(h) : launch_plain<double, 4, false, 4>(h);
     }
+    else if (h->oneMat)
+      rc = h->precision == DNL_PREC_MIXED ? launch_variant<float, 8, true>(h, h->variant)
+                                          : launch_variant<double, 8, true>(h, h->variant);
     else
-      rc = h->precision == DNL_PREC_MIXED ? launch_variant<float, 8>(h, h->variant)
-                                          : launch_variant<double, 8>(h, h->variant);
+      rc = h->precision == DNL_PREC_MIXED ? launch_variant<float, 8, false>(h, h->variant)
+                                          : launch_variant<double, 8, false>(h, h->variant);
   }
   h->launches++;
   return rc;
@@ -648,24 +656,60 @@ int drain_history(dnl_engine *h)
   return DNL_OK;
 }
 
+void drop_graph(dnl_engine *h)
+{
+  if (h->graphExec)
+  {
+    cudaGraphExecDestroy(h->graphExec);
+    cudaGraphDestroy(h->graph);
+    h->graphExec = nullptr;
+    h->graph = nullptr;
+  }
+  for (auto &g : h->remExec)
+    if (g)
+    {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// A graph of n increments, each kernel after the first waiting for the
+// previous one by programmatic serialization, also across the increments'
+// boundaries; increments past an instance's stop find it inactive and do
+// nothing.  *launches: the kernels of one replay.
+int capture_steps(dnl_engine *h, int n, cudaGraph_t *graph, cudaGraphExec_t *exec, int *launches)
+{
+  long long before = h->launches;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < n; k++)
+    enqueue_step(h);
+  cudaError_t e = cudaStreamEndCapture(h->stream, graph);
+  if (e != cudaSuccess)
+    return fail(h, DNL_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  CK(cudaGraphInstantiate(exec, *graph, 0));
+  *launches = (int)(h->launches - before);
+  h->launches = before;
+  return DNL_OK;
+}
+
 int build_graph(dnl_engine *h)
 {
   if (h->graphExec)
     return DNL_OK;
-  long long before = h->launches;
-  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  // graphIncs increments, each kernel after the first waiting for the previous
-  // one by programmatic serialization, also across the increments' boundaries;
-  // increments past an instance's stop find it inactive and do nothing
-  for (int k = 0; k < h->graphIncs; k++)
-    enqueue_step(h);
-  cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
-  if (e != cudaSuccess)
-    return fail(h, DNL_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-  CK(cudaGraphInstantiate(&h->graphExec, h->graph, 0));
-  h->launchesPerStep = (int)(h->launches - before);
-  h->launches = before;
-  return DNL_OK;
+  return capture_steps(h, h->graphIncs, &h->graph, &h->graphExec, &h->launchesPerStep);
+}
+
+// The graph of r (1 <= r < graphIncs) increments: the end of a run of a known
+// number of increments, so that no replay runs increments past it.
+int build_rem_graph(dnl_engine *h, int r)
+{
+  if (h->remExec[r])
+    return DNL_OK;
+  cudaGraph_t g = nullptr;
+  int rc = capture_steps(h, r, &g, &h->remExec[r], &h->remLaunches[r]);
+  if (g)
+    cudaGraphDestroy(g);
+  return rc;
 }
 
 int sync_ctl(dnl_engine *h)
@@ -895,6 +939,10 @@ int dnl_engine_batch_create(const dnl_model_desc *const *descs, int32_t n, dnl_e
   M.conn = (const int *)(A + o_conn);
   M.emat = (const int *)(A + o_emat);
   M.mat = (const MatDev *)(A + o_mat);
+  h->oneMat = mats.size() == 1;
+  M.one32 = mats[0].jc32;
+  M.one64 = mats[0].jc64;
+  M.one_rho0 = mats[0].rho0;
   M.csr_off = (const int *)(A + o_off);
   M.slot_pos = (const int *)(A + o_pos);
   M.bc = (const uint8_t *)(A + o_bc);
@@ -1133,7 +1181,6 @@ int dnl_engine_create(const dnl_model_desc *desc, dnl_engine **out)
 namespace
 {
 void free_items(dnl_engine *h);
-void drop_graph(dnl_engine *h);
 }
 
 int dnl_engine_destroy(dnl_engine *h)
@@ -1142,10 +1189,7 @@ int dnl_engine_destroy(dnl_engine *h)
     return DNL_OK;
   if (h->stream)
     cudaStreamSynchronize(h->stream);
-  if (h->graphExec)
-    cudaGraphExecDestroy(h->graphExec);
-  if (h->graph)
-    cudaGraphDestroy(h->graph);
+  drop_graph(h);
   for (void *p : h->allocs)
     cudaFree(p);
   if (h->dstage)
@@ -1192,6 +1236,10 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
     return fail(h, DNL_ERR_ARG, "dnl_engine_init must be called first");
   int rc = build_graph(h);
   if (rc)
+    return rc;
+  const bool counted = !h->timing && max_incs > 0 && !h->histOn; // replays without polling
+  const int rem = counted ? (int)(max_incs % h->graphIncs) : 0;
+  if (rem && (rc = build_rem_graph(h, rem)))
     return rc;
   std::vector<long long> inc0(h->nInst);
   if ((rc = sync_ctl(h)))
@@ -1255,13 +1303,19 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
     h->times[1] = acc[1];
     h->times[2] = acc[2];
   }
-  else if (max_incs > 0 && !h->histOn)
+  else if (counted)
   {
-    // known number of increments: replay the graph without polling
-    for (int64_t s = 0; s < (max_incs + h->graphIncs - 1) / h->graphIncs; s++)
+    // known number of increments: replay the graph without polling, the last
+    // rem increments by their own graph
+    for (int64_t s = 0; s < max_incs / h->graphIncs; s++)
     {
       CK(cudaGraphLaunch(h->graphExec, h->stream));
       h->launches += h->launchesPerStep;
+    }
+    if (rem)
+    {
+      CK(cudaGraphLaunch(h->remExec[rem], h->stream));
+      h->launches += h->remLaunches[rem];
     }
   }
   else
@@ -2096,13 +2150,7 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps)
   cudaEventDestroy(e1);
   h->variant = best;
   h->tuned = true;
-  if (h->graphExec)
-  {
-    cudaGraphExecDestroy(h->graphExec);
-    cudaGraphDestroy(h->graph);
-    h->graphExec = nullptr;
-    h->graph = nullptr;
-  }
+  drop_graph(h);
   return check_status(h);
 }
 
@@ -2130,13 +2178,7 @@ int dnl_engine_set_variant(dnl_engine *h, int32_t variant)
   if (!h || variant < 0 || variant >= kNumVariants)
     return DNL_ERR_ARG;
   h->variant = variant;
-  if (h->graphExec)
-  {
-    cudaGraphExecDestroy(h->graphExec);
-    cudaGraphDestroy(h->graph);
-    h->graphExec = nullptr;
-    h->graph = nullptr;
-  }
+  drop_graph(h);
   return DNL_OK;
 }
 
@@ -2158,20 +2200,6 @@ int dnl_engine_timings(const dnl_engine *h, double out[4])
 }
 
 int64_t dnl_engine_launch_count(const dnl_engine *h) { return h ? h->launches : 0; }
-
-namespace
-{
-void drop_graph(dnl_engine *h)
-{
-  if (h->graphExec)
-  {
-    cudaGraphExecDestroy(h->graphExec);
-    cudaGraphDestroy(h->graph);
-    h->graphExec = nullptr;
-    h->graph = nullptr;
-  }
-}
-} // namespace
 
 int dnl_engine_set_graph_increments(dnl_engine *h, int32_t n)
 {

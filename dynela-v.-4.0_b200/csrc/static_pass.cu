@@ -74,6 +74,13 @@ struct StaticIo
   }
   __device__ __forceinline__ const MatDev &mat(int) const { return *mat_; }
   __device__ __forceinline__ const MatDev *matp(int) const { return mat_; }
+  __device__ __forceinline__ JC<double> law(int) const
+  {
+    JC<double> j;
+    j.load(*mat_);
+    return j;
+  }
+  __device__ __forceinline__ double rho0(int) const { return mat_->rho0; }
   __device__ __forceinline__ void put(int c, double v) const { ip[(size_t)c * nIP + q] = v; }
   __device__ __forceinline__ void slot(const double4 &v) const { slots[q] = v; }
   __device__ __forceinline__ const float *ip32() const { return nullptr; }

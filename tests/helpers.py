@@ -275,3 +275,12 @@ def case_plane_small(precision=_abi.PREC_FP64):
     initial speed field."""
     return meshes.quad_block(4, 6, size=(1.2, 1.8), speed=60000.0, seed=13, distort=0.12, t_end=5e-6,
                              precision=precision, ts_freq=3)
+
+
+def with_spare_material(desc):
+    """The same model with a second, unused copy of its material.  An engine
+    with one material reads it from the kernel parameters, one with several
+    from global memory as a batch does; the two kernel families round the
+    same arithmetic differently in the last bits, so a run that a batch must
+    reproduce bit for bit is made on the several-materials family."""
+    return desc.copy(materials=list(desc.materials) + [dict(desc.materials[0])])

@@ -50,7 +50,7 @@ def test_batch_failed_instance_stops_alone(variant):
     instances of the batch run to their end exactly as they do alone."""
     good = meshes.hex_block(2, 3, 2, speed=90000.0, seed=4, distort=0.05, t_end=6e-6)
     bad = helpers.case_hex_small()
-    with engine(good) as e:
+    with engine(helpers.with_spare_material(good)) as e:
         e.init()
         e.set_variant(variant)
         e.run()
@@ -77,8 +77,10 @@ def test_batch_failed_instance_stops_alone(variant):
 @pytest.mark.parametrize("variant", [0, 2, 6], ids=["plain", "bulk-copy", "staged"])
 def test_batch_of_taylor_bars_matches_single_runs(variant):
     """Bars of uneven size, speed and material in one batch: every instance
-    ends bit-identical to its own run (the bars finish at different
-    increments, after which their tiles are skipped)."""
+    ends bit-identical to its own run on the same kernels (the bars finish at
+    different increments, after which their tiles are skipped), and within
+    the last bits of the point math of its run on the one-material kernels
+    (material constants as kernel parameters)."""
     descs = meshes.taylor_batch(n=5, seed=11, elems=(300, 1500), t_end=6e-6)
     with engine(descs) as b:
         b.init()
@@ -87,15 +89,26 @@ def test_batch_of_taylor_bars_matches_single_runs(variant):
         X, IP = b.nodes(_abi.NODE_COORDS), b.ips()
         incs = []
         for i, d in enumerate(descs):
-            with engine(d) as e:
+            n0, _, q0 = b.offsets(i)
+            with engine(helpers.with_spare_material(d)) as e:
                 e.init()
                 e.set_variant(variant)
                 e.run()
-                n0, _, q0 = b.offsets(i)
                 assert np.array_equal(X[n0:n0 + d.n_nodes], e.nodes(_abi.NODE_COORDS))
                 assert np.array_equal(IP[:, q0:q0 + d.n_ips], e.ips())
                 assert b.control(i)["increment"] == e.control()["increment"]
                 incs.append(e.control()["increment"])
+            with engine(d) as e:
+                e.init()
+                e.set_variant(variant)
+                e.run()
+                x1, ip1 = e.nodes(_abi.NODE_COORDS), e.ips()
+                dx = np.abs(x1 - X[n0:n0 + d.n_nodes]).max() / np.abs(x1).max()
+                ds = np.abs(ip1 - IP[:, q0:q0 + d.n_ips]).max(axis=1) / np.maximum(np.abs(ip1).max(axis=1), 1e-300)
+                print(f"instance {i}: one-material kernels against the batch: coordinates {dx:.2e}, "
+                      f"point state {ds.max():.2e} of the field's largest value")
+                assert b.control(i)["increment"] == e.control()["increment"]
+                assert dx <= 1e-9 and ds.max() <= 1e-4
     assert len(set(incs)) > 1
 
 
