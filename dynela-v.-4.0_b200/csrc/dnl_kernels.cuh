@@ -388,10 +388,75 @@ template <int NPE> struct ElemShape
   // shared-memory row per point (padded for bank spread): the element forces
   // of the transpose, or the rotation and inverse Jacobian parked across the return
   static constexpr int ROW = (NPE * DIM > 18 ? NPE * DIM : 18) + 1;
-  // the element pass's row: the rotation and J^-1 parked across the return
-  // (the hexahedron's forces need no transpose, the quadrilaterals' 8 fit)
-  static constexpr int PASS_ROW = 19;
+  // the element pass's row: the rotation and J^-1 parked across the return as
+  // 16-byte vectors (the hexahedron's forces need no transpose, the
+  // quadrilaterals' 8 fit).  A row of 20 floats (80 B) or 22 doubles (176 B)
+  // is an odd number of 16-byte units, so the 8 lanes of each phase of a
+  // 16-byte access reach 8 different bank groups
+  template <typename R> static constexpr int pass_row = sizeof(R) == 4 ? 20 : 22;
 };
+
+// The rotation and J^-1 of this lane's point parked in its row across the
+// return: 18 values as 16-byte stores and loads (row 16-byte aligned).
+template <typename R>
+__device__ __forceinline__ void park_rot_inv(R *row, const R (&Rot)[9], const R (&inv)[3][3])
+{
+  const R v[18] = {Rot[0], Rot[1], Rot[2], Rot[3], Rot[4], Rot[5], Rot[6], Rot[7], Rot[8],
+                   inv[0][0], inv[0][1], inv[0][2], inv[1][0], inv[1][1], inv[1][2], inv[2][0], inv[2][1], inv[2][2]};
+  if constexpr (sizeof(R) == 4)
+  {
+    float4 *r4 = reinterpret_cast<float4 *>(row);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      r4[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    reinterpret_cast<float2 *>(row)[8] = make_float2(v[16], v[17]);
+  }
+  else
+  {
+    double2 *r2 = reinterpret_cast<double2 *>(row);
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+      r2[k] = make_double2(v[2 * k], v[2 * k + 1]);
+  }
+}
+
+template <typename R> __device__ __forceinline__ void unpark_rot_inv(const R *row, R (&Rot)[9], R (&inv)[9])
+{
+  R v[18];
+  if constexpr (sizeof(R) == 4)
+  {
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+    {
+      const float4 a = r4[k];
+      v[4 * k] = a.x;
+      v[4 * k + 1] = a.y;
+      v[4 * k + 2] = a.z;
+      v[4 * k + 3] = a.w;
+    }
+    const float2 b = reinterpret_cast<const float2 *>(row)[8];
+    v[16] = b.x;
+    v[17] = b.y;
+  }
+  else
+  {
+    const double2 *r2 = reinterpret_cast<const double2 *>(row);
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+    {
+      const double2 a = r2[k];
+      v[2 * k] = a.x;
+      v[2 * k + 1] = a.y;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+  {
+    Rot[k] = v[k];
+    inv[k] = v[9 + k];
+  }
+}
 
 // Hexahedron in modal form.  With the node signs of node_sign(),
 // s0 = -chi_3(n), s1 = -chi_2(n), s2 = -chi_4(n), s0 s1 = chi_1(n),
@@ -633,7 +698,7 @@ __device__ __forceinline__ typename V4<R>::type element_forces(unsigned amask, i
                                                                R *row, R *grp)
 {
   constexpr int DIM = ElemShape<NPE>::DIM;
-  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int ROW = ElemShape<NPE>::template pass_row<R>;
   static_assert(ROW >= NPE * DIM || NPE == 8, "the transpose needs NPE * DIM values per row");
   const R a = R(0.57735026918962576451);
   const R xi0 = R(node_sign(g, 0)) * a, xi1 = R(node_sign(g, 1)) * a, xi2 = R(node_sign(g, 2)) * a;
@@ -877,12 +942,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
   }
 
   // the rotation and J^-1 wait in shared memory while the return holds its registers
-#pragma unroll
-  for (int k = 0; k < 9; k++)
-  {
-    row[k] = Rot[k];
-    row[9 + k] = inv[k / 3][k % 3];
-  }
+  park_rot_inv<R>(row, Rot, inv);
 
   // J2 radial return with Johnson-Cook hardening (Element.C:407-622)
   ReturnState<R> st;
@@ -931,9 +991,8 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
 
   // final rotation of the plastic strain (PlasticStrain += gamma s*/|s*|,
   // Element.C:587) and of the stress, state write-back
-#pragma unroll
-  for (int k = 0; k < 9; k++)
-    Rot[k] = row[k];
+  R iv[9]; // J^-1, row-major
+  unpark_rot_inv<R>(row, Rot, iv);
   {
     R ep[6];
     const R pn = (st.s[0] + st.s[3] + st.s[5]) / R(3);
@@ -973,7 +1032,7 @@ __device__ __forceinline__ void element_update(const Io &io, Ctl *C, int q, int 
       R s = R(0);
 #pragma unroll
       for (int j = 0; j < DIM; j++)
-        s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
+        s += iv[3 * k + j] * st.s[sym_index(j, i)];
       P[k][i] = -WxdJ * s;
     }
   const R hoop = AXI ? st.s[5] / radius * WxdJ : R(0);
@@ -1033,12 +1092,7 @@ __device__ __forceinline__ void element_front(const Io &io, Ctl *C, int e, int g
   }
 
   // the rotation and J^-1 wait in shared memory while the return holds its registers
-#pragma unroll
-  for (int k = 0; k < 9; k++)
-  {
-    row[k] = Rot[k];
-    row[9 + k] = inv[k / 3][k % 3];
-  }
+  park_rot_inv<R>(row, Rot, inv);
 
   ReturnState<R> &st = f.st;
 #pragma unroll
@@ -1106,10 +1160,8 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
 
   // final rotation of the plastic strain (PlasticStrain += gamma s*/|s*|,
   // Element.C:587) and of the stress, state write-back
-  R Rot[9];
-#pragma unroll
-  for (int k = 0; k < 9; k++)
-    Rot[k] = row[k];
+  R Rot[9], iv[9]; // iv: J^-1, row-major
+  unpark_rot_inv<R>(row, Rot, iv);
   {
     R ep[6];
     const R pn = (st.s[0] + st.s[3] + st.s[5]) / R(3);
@@ -1149,7 +1201,7 @@ __device__ __forceinline__ int element_back(const Io &io, Ctl *C, int q, int e, 
       R s = R(0);
 #pragma unroll
       for (int j = 0; j < DIM; j++)
-        s += row[9 + 3 * k + j] * st.s[sym_index(j, i)];
+        s += iv[3 * k + j] * st.s[sym_index(j, i)];
       P[k][i] = -f.WxdJ * s;
     }
   const R hoop = AXI ? st.s[5] / f.radius * f.WxdJ : R(0);
@@ -1361,7 +1413,7 @@ __global__ void __launch_bounds__(PTS, MINB) k_element(DevModel M, int nTiles)
 {
   static_assert(PTS == TILE || PTS == 2 * TILE || 2 * PTS == TILE, "PTS: half, one or two tiles");
   pdl_wait();
-  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int ROW = ElemShape<NPE>::template pass_row<R>;
   __shared__ __align__(16) R sh[PTS * ROW];
   const int lane = threadIdx.x & 31;
   const int g = lane & (NPE - 1);
@@ -1454,7 +1506,7 @@ template <typename R, int NPE, int MINB, bool ONE = false>
 __global__ void __launch_bounds__(TILE, MINB) k_element_tma(DevModel M, int nTiles, int *err)
 {
   pdl_wait();
-  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int ROW = ElemShape<NPE>::template pass_row<R>;
   constexpr uint32_t STATE_BYTES = DNL_IP_NREAD * TILE * sizeof(R); // the runs the pass reads
   constexpr uint32_t CONN_BYTES = TILE * sizeof(int);
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1611,7 +1663,7 @@ template <typename R, int NPE> struct StageLayout
   static constexpr uint32_t IDX_STRIDE = IDX_BYTES + EMAT_BYTES;
   static constexpr uint32_t OFF_CONN = OFF_IDX + 2 * IDX_STRIDE;
   static constexpr uint32_t OFF_ROWS = OFF_CONN + 3 * IDX_BYTES;
-  static constexpr uint32_t BYTES = OFF_ROWS + TILE * ElemShape<NPE>::PASS_ROW * sizeof(R);
+  static constexpr uint32_t BYTES = OFF_ROWS + TILE * ElemShape<NPE>::template pass_row<R> * sizeof(R);
 };
 
 template <typename R, int NPE, int MINB, bool ONE = false>
@@ -1619,7 +1671,7 @@ __global__ void __launch_bounds__(TILE, MINB) k_element_stage(DevModel M, int nT
 {
   pdl_wait();
   using L = StageLayout<R, NPE>;
-  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int ROW = ElemShape<NPE>::template pass_row<R>;
   constexpr int EPT = L::EPT;
   constexpr uint32_t STATE_BYTES = L::STATE_BYTES, NODE_BYTES = L::NODE_BYTES, IDX_BYTES = L::IDX_BYTES,
                      EMAT_BYTES = L::EMAT_BYTES, OFF_NODES = L::OFF_NODES, OFF_IDX = L::OFF_IDX,
@@ -1769,7 +1821,7 @@ template <int NPE, int MODE>
 __global__ void __launch_bounds__(TILE, 4) k_element_mode(DevModel M, int nTiles, int *err)
 {
   using R = float;
-  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int ROW = ElemShape<NPE>::template pass_row<R>;
   __shared__ __align__(16) R sh[TILE * ROW];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tslot;

@@ -221,7 +221,7 @@ __global__ void k_sp_sort(Args a)
 
 template <int NPE> __global__ void __launch_bounds__(TILE) k_sp_element(Args a)
 {
-  constexpr int ROW = ElemShape<NPE>::PASS_ROW;
+  constexpr int ROW = ElemShape<NPE>::template pass_row<double>;
   __shared__ double sh[TILE * ROW];
   Scratch s = carve(a.scratch);
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
