@@ -362,7 +362,7 @@ template <int NPE> int launch_mode_any(dnl_engine *h)
 
 template <typename R, int NPE, bool ONE> int launch_variant(dnl_engine *h, int v)
 {
-  if (sizeof(R) == 4)
+  if constexpr (sizeof(R) == 4)
   {
     switch (v)
     {
@@ -380,20 +380,23 @@ template <typename R, int NPE, bool ONE> int launch_variant(dnl_engine *h, int v
     default: return launch_plain<R, NPE, ONE, 4, 2 * TILE>(h);
     }
   }
-  switch (v)
+  else
   {
-  case 0: return launch_plain<R, NPE, ONE, 4>(h);
-  case 1: return launch_plain<R, NPE, ONE, 3>(h);
-  case 2: return launch_tma<R, NPE, ONE, 2>(h);
-  case 3: return launch_tma<R, NPE, ONE, 3>(h);
-  case 4: return launch_plain<R, NPE, ONE, 2>(h);
-  case 5: return launch_tma<R, NPE, ONE, 1>(h);
-  case 6: return launch_stage<R, NPE, ONE, 2>(h);
-  case 7: return launch_stage<R, NPE, ONE, 1>(h);
-  case 8: return launch_plain<R, NPE, ONE, 8, TILE / 2>(h);
-  case 9: return launch_plain<R, NPE, ONE, 6, TILE / 2>(h);
-  case 10: return launch_plain<R, NPE, ONE, 2, 2 * TILE>(h);
-  default: return launch_plain<R, NPE, ONE, 1, 2 * TILE>(h);
+    switch (v)
+    {
+    case 0: return launch_plain<R, NPE, ONE, 4>(h);
+    case 1: return launch_plain<R, NPE, ONE, 3>(h);
+    case 2: return launch_tma<R, NPE, ONE, 2>(h);
+    case 3: return launch_tma<R, NPE, ONE, 3>(h);
+    case 4: return launch_plain<R, NPE, ONE, 2>(h);
+    case 5: return launch_tma<R, NPE, ONE, 1>(h);
+    case 6: return launch_stage<R, NPE, ONE, 2>(h);
+    case 7: return launch_stage<R, NPE, ONE, 1>(h);
+    case 8: return launch_plain<R, NPE, ONE, 8, TILE / 2>(h);
+    case 9: return launch_plain<R, NPE, ONE, 6, TILE / 2>(h);
+    case 10: return launch_plain<R, NPE, ONE, 2, 2 * TILE>(h);
+    default: return launch_plain<R, NPE, ONE, 1, 2 * TILE>(h);
+    }
   }
 }
 

@@ -353,9 +353,10 @@ int64_t dnl_engine_launch_count(const dnl_engine *h);
  * budget; points per block for the plain kernel: 64, 128 or 256, i.e. 8, 16
  * or 32 hexahedra; names from dnl_variant_name) over `steps` increments
  * run from a saved copy of the state, keeps the fastest for the following runs
- * (on the mixed path the staged 4-blocks-per-SM variant, 5, when it is within
- * 1 % of the fastest: it holds up best later in an impact) and restores the
- * state.  A batch (several instances) is offered the
+ * (on the mixed path a preferred variant when it is within 1 % of the fastest,
+ * as it holds up best later in an impact: the plain pass on 64-point blocks,
+ * 9, for a single model, the staged 4-blocks-per-SM pass, 5, for a batch) and
+ * restores the state.  A batch (several instances) is offered the
  * persistent variants only (its ms entries for the plain ones are -1): the
  * plain variants launch a block per tile of the whole batch at every
  * increment, even when few instances still run.  No counterpart in the
