@@ -679,7 +679,8 @@ void drop_graph(dnl_engine *h)
 // A graph of n increments, each kernel after the first waiting for the
 // previous one by programmatic serialization, also across the increments'
 // boundaries; increments past an instance's stop find it inactive and do
-// nothing.  *launches: the kernels of one replay.
+// nothing.  *launches: the kernels of one replay.  The graph is uploaded
+// after instantiation, so that its first replay does not carry the upload.
 int capture_steps(dnl_engine *h, int n, cudaGraph_t *graph, cudaGraphExec_t *exec, int *launches)
 {
   long long before = h->launches;
@@ -690,6 +691,8 @@ int capture_steps(dnl_engine *h, int n, cudaGraph_t *graph, cudaGraphExec_t *exe
   if (e != cudaSuccess)
     return fail(h, DNL_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
   CK(cudaGraphInstantiate(exec, *graph, 0));
+  // the executable graph goes to the device now, not at its first replay
+  CK(cudaGraphUpload(*exec, h->stream));
   *launches = (int)(h->launches - before);
   h->launches = before;
   return DNL_OK;
