@@ -57,6 +57,20 @@ def test_invalid_descriptions_are_rejected():
     assert rc == -6 and "stress computation" in msg
     rc, h, msg = _create(d.copy(node_order=9))
     assert rc == -1 and "node order" in msg
+    # empty and ragged inputs: no elements, no nodes, no material, a material
+    # index past the list, an unknown precision; each is refused on the host
+    # before any device call and leaves no handle
+    for field, value, text in (("n_elems", 0, "empty mesh"), ("n_nodes", 0, "empty mesh"),
+                               ("n_materials", 0, "no material"), ("precision", 9, "unknown precision")):
+        c = d.cstruct()
+        setattr(c, field, value)
+        h = ctypes.c_void_p()
+        assert lib.dnl_engine_create(ctypes.byref(c), ctypes.byref(h)) == -1 and not h, field
+        assert text in lib.dnl_engine_last_error(None).decode(), field
+    rc, h, msg = _create(d.copy(elem_mat=np.full(d.n_elems, 1, dtype=np.int32)))
+    assert rc == -1 and "material index of element 0 out of range" in msg and not h
+    rc, h, msg = _create(d.copy(conn=np.where(d.conn == 3, -1, d.conn)))
+    assert rc == -1 and "out of range" in msg and not h
 
 
 def test_no_device_means_no_engine():
