@@ -121,6 +121,28 @@ def profiled_traffic():
 
 # ------------------------------------------------------------------- clocks
 
+def smi_index(fallback, uuid=None, listing=None):
+    """nvidia-smi's index of the GPU this process computes on: its CUDA device
+    0 (the launcher's assignment, through CUDA_VISIBLE_DEVICES), matched by
+    UUID against `nvidia-smi --query-gpu=index,uuid`; `fallback` when either
+    is unavailable.  uuid / listing: given by the tests, queried otherwise."""
+    try:
+        if uuid is None:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(0).uuid)
+        if listing is None:
+            listing = subprocess.run(["nvidia-smi", "--query-gpu=index,uuid", "--format=csv,noheader"],
+                                     capture_output=True, text=True, timeout=30).stdout
+    except Exception:
+        return fallback
+    want = uuid.lower().removeprefix("gpu-")
+    for line in listing.splitlines():
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) == 2 and parts[1].lower().removeprefix("gpu-") == want:
+            return int(parts[0])
+    return fallback
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -538,7 +560,7 @@ def run_engine_arm(args, rank, world, dist):
 
     # ---- timed region: K increments, device time on the engine stream
     barrier()
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0)
+    sampler = ClockSampler(smi_index(int(os.environ.get("LOCAL_RANK", "0")) if world > 1 else 0))
     sampler.start()
     done = eng.run(max_incs=args.steps)
     run_ms = eng.timings()["run_ms"]

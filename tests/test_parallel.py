@@ -73,3 +73,18 @@ def test_two_gloo_ranks_split_a_batch():
         assert sorted(r[4]) == list(range(16))
         assert all(r[4][i]["elements"] == descs[i].n_elems for i in range(16))
         assert all(r[4][i]["rank"] == (0 if i in res[0][1] else 1) for i in range(16))
+
+
+def test_clock_sampler_follows_the_assigned_gpu():
+    """The bench samples the clocks of the GPU its rank computes on: the one
+    whose UUID matches its CUDA device 0, wherever that lies in nvidia-smi's
+    list (a launcher may hand a job GPUs 4 and 5); the rank's index when no
+    match can be made."""
+    import sys
+    sys.path.insert(0, helpers.ROOT)
+    import bench
+    listing = ("0, GPU-aaaa-0000\n1, GPU-bbbb-1111\n4, GPU-cccc-4444\n5, GPU-dddd-5555\n")
+    assert bench.smi_index(1, uuid="dddd-5555", listing=listing) == 5
+    assert bench.smi_index(0, uuid="GPU-CCCC-4444", listing=listing) == 4
+    assert bench.smi_index(1, uuid="eeee-9999", listing=listing) == 1
+    assert bench.smi_index(3, uuid="aaaa-0000", listing="") == 3
