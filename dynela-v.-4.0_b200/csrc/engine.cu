@@ -1263,48 +1263,62 @@ int dnl_engine_run(dnl_engine *h, double t_pause, int64_t max_incs, int64_t *inc
   launch_control(h, CTL_LIMITS, t_pause, max_incs);
   if (h->timing)
   {
-    // kernel-by-kernel with events: per-phase device time
-    cudaEvent_t e[4];
-    for (int k = 0; k < 4; k++)
-      CK(cudaEventCreate(&e[k]));
+    // kernel-by-kernel with events: per-phase device time.  A chunk of
+    // increments is queued with its own events and read after one wait, so
+    // that the kernels are already queued when their opening event completes
+    // and each bracket holds device time only (waiting on every increment
+    // would put the host's launch latency inside the brackets).
+    // (increments, not graph replays: at most what the history ring holds)
+    const int maxChunk = h->histOn ? std::max(1, std::min(64, h->hist.cap)) : 64;
+    std::vector<cudaEvent_t> e(4 * (size_t)maxChunk);
+    for (auto &ev : e)
+      CK(cudaEventCreate(&ev));
     float acc[3] = {0, 0, 0};
     long long steps = 0;
     for (;;)
     {
-      const int chunk = poll_chunk(h, 16);
-      for (int s = 0; s < chunk; s++)
+      int queued = 0;
+      for (int s = 0; s < maxChunk; s++)
       {
+        cudaEvent_t *es = &e[4 * (size_t)s];
         launch_bc_prep(h);
-        CK(cudaEventRecord(e[0], h->stream));
+        CK(cudaEventRecord(es[0], h->stream));
         launch_element_any(h, 0);
-        CK(cudaEventRecord(e[1], h->stream));
+        CK(cudaEventRecord(es[1], h->stream));
         launch_nodal(h);
-        CK(cudaEventRecord(e[2], h->stream));
+        CK(cudaEventRecord(es[2], h->stream));
         launch_step_end(h);
         launch_history(h);
-        CK(cudaEventRecord(e[3], h->stream));
-        CK(cudaEventSynchronize(e[3]));
+        CK(cudaEventRecord(es[3], h->stream));
+        queued++;
+        if (max_incs > 0 && steps + queued >= max_incs)
+          break;
+      }
+      CK(cudaEventSynchronize(e[4 * (size_t)(queued - 1) + 3]));
+      for (int s = 0; s < queued; s++)
+      {
+        const cudaEvent_t *es = &e[4 * (size_t)s];
         float t01, t12, t23;
-        cudaEventElapsedTime(&t01, e[0], e[1]);
-        cudaEventElapsedTime(&t12, e[1], e[2]);
-        cudaEventElapsedTime(&t23, e[2], e[3]);
+        cudaEventElapsedTime(&t01, es[0], es[1]);
+        cudaEventElapsedTime(&t12, es[1], es[2]);
+        cudaEventElapsedTime(&t23, es[2], es[3]);
         acc[0] += t01;
         acc[1] += t12;
         acc[2] += t23;
-        steps++;
-        if (max_incs > 0 && steps >= max_incs)
-          break;
       }
+      steps += queued;
       if ((rc = sync_ctl(h)) || (rc = drain_history(h)))
-        return rc;
+        break;
       bool any = false;
       for (int i = 0; i < h->nInst; i++)
         any = any || h->hctl[i].active;
       if (!any || (max_incs > 0 && steps >= max_incs))
         break;
     }
-    for (int k = 0; k < 4; k++)
-      cudaEventDestroy(e[k]);
+    for (auto &ev : e)
+      cudaEventDestroy(ev);
+    if (rc)
+      return rc;
     h->times[0] = acc[0];
     h->times[1] = acc[1];
     h->times[2] = acc[2];
