@@ -250,11 +250,13 @@ struct Variant
 // blocks per SM (fewest registers, most spilled) to the fewest (no spills)
 // then the fully staged kernel (node gathers one tile ahead as well)
 // then plain blocks of half a tile (8 hexahedra) and of two tiles (32) at
-// the register budgets of the 128-point ones
+// the register budgets of the 128-point ones; in FP32 also the plain passes
+// at 48 registers (plain64/20, plain/10: 40 warps per SM, no more spilled
+// than at 64 registers)
 const Variant kVariantsF32[] = {{"plain/6", 0, 6, 128},     {"plain/8", 0, 8, 128},    {"tma/4", 1, 4, 128},
-                                {"tma/5", 1, 5, 128},       {"tma/3", 1, 3, 128},      {"stage/4", 2, 4, 128},
+                                {"plain64/20", 0, 20, 64},  {"tma/3", 1, 3, 128},      {"stage/4", 2, 4, 128},
                                 {"stage/3", 2, 3, 128},     {"stage/2", 2, 2, 128},    {"plain64/12", 0, 12, 64},
-                                {"plain64/16", 0, 16, 64},  {"plain256/3", 0, 3, 256}, {"plain256/4", 0, 4, 256}};
+                                {"plain64/16", 0, 16, 64},  {"plain/10", 0, 10, 128},  {"plain256/4", 0, 4, 256}};
 const Variant kVariantsF64[] = {{"plain/4", 0, 4, 128},     {"plain/3", 0, 3, 128},    {"tma/2", 1, 2, 128},
                                 {"tma/3", 1, 3, 128},       {"plain/2", 0, 2, 128},    {"tma/1", 1, 1, 128},
                                 {"stage/2", 2, 2, 128},     {"stage/1", 2, 1, 128},    {"plain64/8", 0, 8, 64},
@@ -369,14 +371,14 @@ template <typename R, int NPE, bool ONE> int launch_variant(dnl_engine *h, int v
     case 0: return launch_plain<R, NPE, ONE, 6>(h);
     case 1: return launch_plain<R, NPE, ONE, 8>(h);
     case 2: return launch_tma<R, NPE, ONE, 4>(h);
-    case 3: return launch_tma<R, NPE, ONE, 5>(h);
+    case 3: return launch_plain<R, NPE, ONE, 20, TILE / 2>(h);
     case 4: return launch_tma<R, NPE, ONE, 3>(h);
     case 5: return launch_stage<R, NPE, ONE, 4>(h);
     case 6: return launch_stage<R, NPE, ONE, 3>(h);
     case 7: return launch_stage<R, NPE, ONE, 2>(h);
     case 8: return launch_plain<R, NPE, ONE, 12, TILE / 2>(h);
     case 9: return launch_plain<R, NPE, ONE, 16, TILE / 2>(h);
-    case 10: return launch_plain<R, NPE, ONE, 3, 2 * TILE>(h);
+    case 10: return launch_plain<R, NPE, ONE, 10>(h);
     default: return launch_plain<R, NPE, ONE, 4, 2 * TILE>(h);
     }
   }
@@ -2159,12 +2161,13 @@ int dnl_engine_autotune(dnl_engine *h, int32_t steps)
   }
   // the trial increments are the next few; later in an impact more points
   // yield, and there the variant with the most warps holds up best: the plain
-  // pass on 64-point blocks (16 per SM) for a single model (3-D bar after
-  // 3,000 increments: 0.075 ms against 0.077 for the staged kernel with 4
-  // blocks per SM, which equals it at the start), the staged kernel with 4
-  // blocks per SM for a batch (plain variants are not offered to batches).
-  // The preferred variant is kept when within 1 % of the fastest trial.
-  const int prefer = h->nInst == 1 ? 9 : 5;
+  // pass on 128-point blocks at 48 registers (10 per SM, 40 warps) for a
+  // single model (3-D bar: 0.0714 ms at the start and 0.0743 after 3,000
+  // increments, against 0.0723 and 0.0741-0.0762 for 64-point blocks at 64
+  // registers), the staged kernel with 4 blocks per SM for a batch (plain
+  // variants are not offered to batches).  The preferred variant is kept
+  // when within 1 % of the fastest trial.
+  const int prefer = h->nInst == 1 ? 10 : 5;
   if (h->precision == DNL_PREC_MIXED && h->variantMs[prefer] > 0.0 && h->variantMs[prefer] <= 1.01 * bestMs)
     best = prefer;
   for (auto &p : parts)
