@@ -244,6 +244,33 @@ def test_pause_and_resume_equal_one_run():
         assert np.array_equal(a.nodes(_abi.NODE_COORDS), b.nodes(_abi.NODE_COORDS))
 
 
+@pytest.mark.parametrize("ts_freq,precision", [(10, _abi.PREC_FP64), (3, _abi.PREC_FP64), (2, _abi.PREC_MIXED),
+                                                (1, _abi.PREC_FP64), (10, _abi.PREC_MIXED)])
+def test_graph_replays_equal_kernel_by_kernel(ts_freq, precision):
+    """Graph replays of several lengths, the graphs of the remaining
+    increments of a counted run, and runs cut into uneven pieces (each piece
+    starting at another increment of the time-step cycle) give the same bits
+    as the same increments launched kernel by kernel."""
+    d = helpers.case_hex_speed().copy(ts_freq=ts_freq, precision=precision)
+    with engine(d) as ref:
+        ref.init()
+        ref.set_timing(True)
+        ref.run(max_incs=61)
+        want = (ref.nodes(_abi.NODE_COORDS), ref.ips(), ref.control()["time"])
+    for graph_incs, pieces in ((8, [61]), (8, [1, 2, 3, 7, 9, 10, 11, 18]), (1, [5, 56]), (16, [13, 27, 21]),
+                               (20, [30, 31])):
+        with engine(d) as e:
+            e.init()
+            e.set_graph_increments(graph_incs)
+            for n in pieces:
+                assert e.run(max_incs=n) == n
+            got = (e.nodes(_abi.NODE_COORDS), e.ips(), e.control()["time"])
+            assert e.control()["increment"] == 61 and e.control()["status"] == 0
+        assert np.array_equal(got[0], want[0]), (graph_incs, pieces)
+        assert np.array_equal(got[1], want[1]), (graph_incs, pieces)
+        assert got[2] == want[2]
+
+
 def test_inverted_element_raises_status():
     d = helpers.case_hex_small()
     with engine(d) as e:
