@@ -191,9 +191,19 @@ int check_desc(const dnl_model_desc *d, int idx)
   if (d->precision != DNL_PREC_FP64 && d->precision != DNL_PREC_MIXED)
     return fail(nullptr, DNL_ERR_ARG, "model %d: unknown precision %d", idx, d->precision);
   const int npe = npe_of(d->elem_type);
-  for (long k = 0; k < (long)d->n_elems * npe; k++)
-    if (d->conn[k] < 0 || d->conn[k] >= d->n_nodes)
-      return fail(nullptr, DNL_ERR_ARG, "model %d: connectivity entry %ld = %d out of range", idx, k, d->conn[k]);
+  // the range of the connectivity by a min / max pass (no early exit, so it
+  // vectorises); the first entry out of range is looked for only when there is one
+  const long nConn = (long)d->n_elems * npe;
+  int32_t lo = INT32_MAX, hi = INT32_MIN;
+  for (long k = 0; k < nConn; k++)
+  {
+    lo = std::min(lo, d->conn[k]);
+    hi = std::max(hi, d->conn[k]);
+  }
+  if (lo < 0 || hi >= d->n_nodes)
+    for (long k = 0; k < nConn; k++)
+      if (d->conn[k] < 0 || d->conn[k] >= d->n_nodes)
+        return fail(nullptr, DNL_ERR_ARG, "model %d: connectivity entry %ld = %d out of range", idx, k, d->conn[k]);
   if (d->elem_mat)
     for (int e = 0; e < d->n_elems; e++)
       if (d->elem_mat[e] < 0 || d->elem_mat[e] >= d->n_materials)
