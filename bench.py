@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--variant", type=int, default=-1,
-                   help="element-pass variant (0-7); default: chosen by the autotuner")
+                   help="element-pass variant (0-11, names in dnl_variant_name); default: chosen by the autotuner")
     p.add_argument("--no-accuracy", action="store_true", help="skip the whole-run mixed/FP64 comparison")
     p.add_argument("--no-batch", action="store_true", help="skip the batch of 256 Taylor bars")
     p.add_argument("--guess", action="store_true",
