@@ -717,6 +717,19 @@ def run_engine_arm(args, rank, world, dist):
     print(json.dumps(out))
 
 
+def rank_device(visible, local):
+    """The CUDA_VISIBLE_DEVICES of local rank `local`: the local-th of the
+    devices the launcher gave the job (`visible`, indices or UUIDs), or
+    device `local` when the launcher set none.  ValueError when the list is
+    shorter than the ranks."""
+    if visible is None or not visible.strip():
+        return str(local)
+    ids = [x.strip() for x in visible.split(",") if x.strip()]
+    if local >= len(ids):
+        raise ValueError(f"local rank {local} but CUDA_VISIBLE_DEVICES lists {len(ids)} devices")
+    return ids[local]
+
+
 def spawn_ranks(n):
     """Run this command again as n ranks under torch.distributed.run (local
     rendezvous on 127.0.0.1, a free port, a hard time limit well above the
@@ -751,17 +764,12 @@ def main():
         return
     dist = None
     if world > 1:
-        # one process per GPU: this rank sees only its own device, the
-        # local_rank-th of the devices the launcher gave the job (the engine
+        # one process per GPU: this rank sees only its own device (the engine
         # creates its handles on the current device, device 0 of what it sees)
-        visible = os.environ.get("CUDA_VISIBLE_DEVICES")
-        if visible:
-            ids = [x for x in visible.split(",") if x.strip()]
-            if local >= len(ids):
-                sys.exit(f"bench.py: local rank {local} but CUDA_VISIBLE_DEVICES lists {len(ids)} devices")
-            os.environ["CUDA_VISIBLE_DEVICES"] = ids[local].strip()
-        else:
-            os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+        try:
+            os.environ["CUDA_VISIBLE_DEVICES"] = rank_device(os.environ.get("CUDA_VISIBLE_DEVICES"), local)
+        except ValueError as e:
+            sys.exit(f"bench.py: {e}")
         import datetime
         import torch
         import torch.distributed as tdist

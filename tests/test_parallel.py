@@ -88,3 +88,17 @@ def test_clock_sampler_follows_the_assigned_gpu():
     assert bench.smi_index(0, uuid="GPU-CCCC-4444", listing=listing) == 4
     assert bench.smi_index(1, uuid="eeee-9999", listing=listing) == 1
     assert bench.smi_index(3, uuid="aaaa-0000", listing="") == 3
+
+
+def test_each_rank_takes_its_own_assigned_gpu():
+    """Under a launcher every rank runs on the local-rank-th of the GPUs the
+    job was given, never on a GPU outside that list."""
+    import sys
+    sys.path.insert(0, helpers.ROOT)
+    import bench
+    assert bench.rank_device("4,5", 0) == "4" and bench.rank_device("4,5", 1) == "5"
+    assert bench.rank_device(" 6 , 7 ", 1) == "7"
+    assert bench.rank_device("GPU-aaaa,GPU-bbbb", 1) == "GPU-bbbb"
+    assert bench.rank_device(None, 3) == "3" and bench.rank_device("", 2) == "2"
+    with pytest.raises(ValueError, match="lists 2 devices"):
+        bench.rank_device("4,5", 2)
