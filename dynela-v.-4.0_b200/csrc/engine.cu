@@ -181,6 +181,11 @@ int check_desc(const dnl_model_desc *d, int idx)
     return fail(nullptr, DNL_ERR_ARG, "model %d: unknown element type %d", idx, d->elem_type);
   if (d->n_nodes <= 0 || d->n_elems <= 0 || !d->coords || !d->conn)
     return fail(nullptr, DNL_ERR_ARG, "model %d: empty mesh", idx);
+  // before any of the caller's arrays is read: the engine indexes points and
+  // node components with 32-bit integers
+  if ((long long)d->n_elems * npe_of(d->elem_type) > 0x3fffffffLL || 3LL * d->n_nodes > 0x3fffffffLL)
+    return fail(nullptr, DNL_ERR_ARG, "model %d: too large for 32-bit point indices (%d elements, %d nodes)", idx,
+                d->n_elems, d->n_nodes);
   if (d->n_materials <= 0 || !d->materials)
     return fail(nullptr, DNL_ERR_ARG, "model %d: no material", idx);
   if (d->ts_method != DNL_TS_COURANT && d->ts_method != DNL_TS_POWER_ITERATION)

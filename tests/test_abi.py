@@ -67,6 +67,14 @@ def test_invalid_descriptions_are_rejected():
         h = ctypes.c_void_p()
         assert lib.dnl_engine_create(ctypes.byref(c), ctypes.byref(h)) == -1 and not h, field
         assert text in lib.dnl_engine_last_error(None).decode(), field
+    # beyond the 32-bit point indices (the sizes are refused before the
+    # arrays, which here are far shorter, are read)
+    for field, value in (("n_elems", 200_000_000), ("n_nodes", 400_000_000)):
+        c = d.cstruct()
+        setattr(c, field, value)
+        h = ctypes.c_void_p()
+        assert lib.dnl_engine_create(ctypes.byref(c), ctypes.byref(h)) == -1 and not h, field
+        assert "too large for 32-bit point indices" in lib.dnl_engine_last_error(None).decode(), field
     rc, h, msg = _create(d.copy(elem_mat=np.full(d.n_elems, 1, dtype=np.int32)))
     assert rc == -1 and "material index of element 0 out of range" in msg and not h
     rc, h, msg = _create(d.copy(conn=np.where(d.conn == 3, -1, d.conn)))
