@@ -333,7 +333,12 @@ int dnl_engine_energies(dnl_engine *h, int32_t instance, double out[3]);
 
 /* Device-side time of the kernels of the last dnl_engine_run call, in ms:
  * [0] element pass, [1] nodal pass, [2] time-step pass, [3] whole run. Only
- * filled when timing was enabled with dnl_engine_set_timing(h, 1). */
+ * filled when timing was enabled with dnl_engine_set_timing(h, 1): the
+ * increments then run kernel by kernel (no graph), queued in chunks of up to
+ * 64 with CUDA events around each pass that are read after the chunk, so
+ * that no bracket holds host launch latency; the run stops at the end of
+ * the chunk in which its instances stop (the increments past the stop do
+ * nothing and add a few microseconds each to the sums). */
 int dnl_engine_set_timing(dnl_engine *h, int32_t on);
 int dnl_engine_timings(const dnl_engine *h, double out[4]);
 
