@@ -74,31 +74,3 @@ def test_two_gloo_ranks_split_a_batch():
         assert all(r[4][i]["elements"] == descs[i].n_elems for i in range(16))
         assert all(r[4][i]["rank"] == (0 if i in res[0][1] else 1) for i in range(16))
 
-
-def test_clock_sampler_follows_the_assigned_gpu():
-    """The bench samples the clocks of the GPU its rank computes on: the one
-    whose UUID matches its CUDA device 0, wherever that lies in nvidia-smi's
-    list (a launcher may hand a job GPUs 4 and 5); the rank's index when no
-    match can be made."""
-    import sys
-    sys.path.insert(0, helpers.ROOT)
-    import bench
-    listing = ("0, GPU-aaaa-0000\n1, GPU-bbbb-1111\n4, GPU-cccc-4444\n5, GPU-dddd-5555\n")
-    assert bench.smi_index(1, uuid="dddd-5555", listing=listing) == 5
-    assert bench.smi_index(0, uuid="GPU-CCCC-4444", listing=listing) == 4
-    assert bench.smi_index(1, uuid="eeee-9999", listing=listing) == 1
-    assert bench.smi_index(3, uuid="aaaa-0000", listing="") == 3
-
-
-def test_each_rank_takes_its_own_assigned_gpu():
-    """Under a launcher every rank runs on the local-rank-th of the GPUs the
-    job was given, never on a GPU outside that list."""
-    import sys
-    sys.path.insert(0, helpers.ROOT)
-    import bench
-    assert bench.rank_device("4,5", 0) == "4" and bench.rank_device("4,5", 1) == "5"
-    assert bench.rank_device(" 6 , 7 ", 1) == "7"
-    assert bench.rank_device("GPU-aaaa,GPU-bbbb", 1) == "GPU-bbbb"
-    assert bench.rank_device(None, 3) == "3" and bench.rank_device("", 2) == "2"
-    with pytest.raises(ValueError, match="lists 2 devices"):
-        bench.rank_device("4,5", 2)
